@@ -1,0 +1,349 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 3D ADI time step: cell-steps/s on a synthetic masked domain.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config spheres128]
+                    [--solver fast|exact] [--impl ours|reference]
+
+One "step" is one pass of the reference driver loop (FluidSolver3D.cpp:241-242):
+UpdateBoundaries + TimeStep(dt, num_global, num_local), with the divergence error
+evaluated on every 10th step as the driver does.  The metric counts box cells:
+cell-steps/s = dimx*dimy*dimz * steps / time.
+
+value  : device time of K steps (CUDA events on the solver's stream, L2 flushed
+         by a 256 MiB memset between steps and excluded from the time), max over
+         ranks; inputs are resident in HBM.
+e2e    : the same K steps through the C ABI with host buffers: each step uploads
+         the state from pinned host memory (adi_set_state), steps, and reads the
+         result back (adi_get_state).
+roofline: the sweep kernels (the dominant class), algorithmic bytes per launch /
+         their CUDA-event time, against the measured HBM copy bandwidth.
+cpu_baseline: the reference's own CPU solver (oracle/_ref/libref3d.so, compiled
+         from its sources) on the same workload on this host's cores (rank 0, N=1).
+
+Multi-GPU: the single-domain step does not shard (the reference's slab
+decomposition is out of scope), so N ranks run N independent replicas
+("replicas only"); value = all ranks' cell-steps / max-over-ranks time.
+--impl reference times the reference CPU solver instead (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "cmc-fluid-solver_b200")
+ORACLE = os.path.join(ROOT, "oracle")
+sys.path.insert(0, PKG)
+sys.path.insert(0, ORACLE)
+
+import numpy as np  # noqa: E402
+
+from adi_b200 import geometry as G  # noqa: E402
+
+METRIC = "cell-steps/s"
+
+
+def _spheres128():
+    return G.spheres_channel(n=128, n_spheres=40, rmin=4.0, rmax=12.0, seed=0)
+
+
+def _ellipsoids384():
+    return G.ellipsoids_tube(n=384, n_ellipsoids=300, amin=3.0, amax=20.0, seed=1)
+
+
+def _spheres64():
+    return G.spheres_channel(n=64, n_spheres=10, rmin=3.0, rmax=7.0, seed=0)
+
+
+CONFIGS = {
+    "spheres128": dict(make=_spheres128, Re=200.0, Pr=0.72, lam=1.4, dt=5e-4, ng=4, nl=2,
+                       desc="plain 3D ADI forward: 128^3 FP32 box, 40 solid spheres (radii U[4,12], "
+                            "centres U[0,128)^3, seed 0), inflow u=1 on x=0, Re=200, dt=5e-4, "
+                            "num_global=4, num_local=2"),
+    "ellipsoids384": dict(make=_ellipsoids384, Re=500.0, Pr=0.72, lam=1.4, dt=2e-4, ng=4, nl=2,
+                          desc="large 3D single domain: 384^3 FP32, 300 solid ellipsoids (semi-axes "
+                               "U[3,20], seed 1) plus a thin-walled tube along x, Re=500, dt=2e-4, "
+                               "num_global=4, num_local=2"),
+    "spheres64": dict(make=_spheres64, Re=200.0, Pr=0.72, lam=1.4, dt=5e-4, ng=4, nl=2,
+                      desc="small case for profiling: 64^3 FP32, 10 spheres, Re=200, dt=5e-4, "
+                           "num_global=4, num_local=2"),
+}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(config: str, solver: str):
+    """Per-launch DRAM bytes of the sweep kernel from a committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "sweep_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    return d.get(f"{config}/{solver}")
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms in the background."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_reference_run(cfg, steps: int, budget_s: float, d=None):
+    """Times the reference CPU solver on the workload: up to `steps` steps or until
+    budget_s seconds have passed (at least one).  Returns (cells*steps/s, steps, s)."""
+    import oracle as O
+    if not O.have_ref():
+        O.build()
+    if d is None:
+        d = cfg["make"]()
+    ref = O.RefSolver(d, Re=cfg["Re"], Pr=cfg["Pr"], lam=cfg["lam"])
+    done, t0 = 0, time.perf_counter()
+    while done < steps:
+        ref.step(cfg["dt"], cfg["ng"], cfg["nl"], done % 10 == 0)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    ref.close()
+    return d.cells * done / el, done, el
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup()
+    cfg = CONFIGS[args.config]
+    if rank != 0:
+        return 0
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+    d = cfg["make"]()
+    # warm-up steps are part of the sample budget too (first-touch of the layers)
+    if args.warmup:
+        cpu_reference_run(cfg, min(args.warmup, 1), 60.0, d)
+    value, done, el = cpu_reference_run(cfg, args.steps, args.ref_budget, d)
+    cores = int(os.environ["OMP_NUM_THREADS"])
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+        "steps": done, "warmup": args.warmup, "ms_per_step": 1e3 * el / done, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{args.config}: {cfg['desc']}", "cells": d.cells},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "reference",
+                         "sample": f"{done} full steps of {args.config} ({el:.1f} s), OpenMP {cores} threads"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    import adi_b200
+    cfg = CONFIGS[args.config]
+    d = cfg["make"]()
+    stream = torch.cuda.current_stream()
+    solver_kind = adi_b200.ADI_SOLVER_FAST if args.solver == "fast" else adi_b200.ADI_SOLVER_EXACT
+    s = adi_b200.AdiSolver3D(d, Re=cfg["Re"], Pr=cfg["Pr"], lam=cfg["lam"], precision=adi_b200.ADI_FP32,
+                             solver=solver_kind, stream=stream.cuda_stream)
+    stats = s.CreateSegments()
+    dt, ng, nl = cfg["dt"], cfg["ng"], cfg["nl"]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def one_step(i):
+        rc = s.step(dt, ng, nl, i % 10 == 0)
+        if rc != 0:
+            raise RuntimeError(f"adi_step failed with status {rc}")
+
+    for i in range(args.warmup):
+        one_step(i)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    # ---- timed region: device time of K steps, L2 flushed between steps ----
+    clocks = ClockSampler(local)
+    clocks.start()
+    s.profile(reset=True)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier()
+    for i in range(args.steps):
+        flush.zero_()
+        ev[i][0].record(stream)
+        one_step(i)
+        ev[i][1].record(stream)
+    barrier()
+    prof_plain = s.profile(reset=True)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = float(sum(step_ms))
+    # ---- kernel roofline pass: same steps with per-launch CUDA events ----
+    s.set_profiling(True)
+    for i in range(args.steps):
+        flush.zero_()
+        one_step(i)
+    torch.cuda.synchronize()
+    prof = s.profile(reset=True)
+    s.set_profiling(False)
+    clk = clocks.stop()
+
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * d.cells * args.steps / (total_ms / 1e3)
+
+    # ---- end to end through the C ABI with host buffers ----
+    pinned = [torch.empty(d.shape, dtype=torch.float32, pin_memory=True).numpy() for _ in range(8)]
+    cur = s.fields(0)
+    for a, b in zip(pinned[:4], cur):
+        a[...] = b
+    e2e_steps = max(1, min(args.steps, 20))
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(e2e_steps):
+        s.set_state(*pinned[:4])
+        one_step(i)
+        s._check(s.lib.adi_get_state(s.h, 0, *[p.ctypes.data for p in pinned[4:]]))
+        pinned[:4], pinned[4:] = pinned[4:], pinned[:4]
+    e1.record(stream)
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * d.cells * e2e_steps / (e2e_ms / 1e3)
+    io_bytes = 4 * d.cells * 4
+
+    sweep_keys = ("sweep_x", "sweep_y", "sweep_z")
+    sw_bytes = sum(prof[k]["bytes"] for k in sweep_keys)
+    sw_ms = sum(prof[k]["ms"] for k in sweep_keys)
+    sw_launches = sum(prof[k]["launches"] for k in sweep_keys)
+    peak, peak_kind = measured_peaks()
+    achieved = (sw_bytes / sw_launches) / (sw_ms / sw_launches / 1e3) / 1e9 if sw_ms > 0 else 0.0
+    traffic = ncu_traffic(args.config, args.solver)
+    launches = sum(v["launches"] for v in prof_plain.values())
+    step_bytes = sum(v["bytes"] for v in prof.values()) / args.steps
+
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{args.config}: {cfg['desc']}", "cells": d.cells,
+                   "segments_xyz": stats["num_segments"], "segment_nodes_xyz": stats["num_nodes"],
+                   "solver": args.solver, "parallelism": f"replicas x{world}" if world > 1 else "single domain",
+                   "l2": "flushed between steps (256 MiB memset, excluded from the time)",
+                   "algorithmic_bytes_per_step": step_bytes},
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes,
+                "steps": e2e_steps},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if peak else None, "traffic": traffic,
+                     "kernel": f"sweep_{args.solver} (X, Y, Z)", "peak_source": peak_kind,
+                     "per_class_ms_per_step": {k: v["ms"] / args.steps for k, v in prof.items() if v["launches"]}},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+        v, done, el = cpu_reference_run(cfg, 1000, args.cpu_budget, d)
+        line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": int(os.environ["OMP_NUM_THREADS"]),
+                                "kind": "reference",
+                                "sample": f"{done} full steps of {args.config} ({el:.1f} s) on the reference "
+                                          f"CPU solver, OpenMP {os.environ['OMP_NUM_THREADS']} threads"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    s.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--config", default="spheres128", choices=sorted(CONFIGS))
+    ap.add_argument("--solver", default="fast", choices=["fast", "exact"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of reference CPU time for cpu_baseline")
+    ap.add_argument("--ref-budget", type=float, default=120.0, help="seconds cap for --impl reference")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,149 @@
+"""Python front end of the B200 3D ADI step (ctypes over include/adi_b200.h).
+
+``AdiSolver3D`` mirrors the reference's ``Solver3D``/``AdiSolver3D`` surface
+(``FluidSolver3D/Solver3D.h:24-49``, ``AdiSolver3D.h:49-61``): ``Init``, ``CreateSegments``,
+``UpdateBoundaries``, ``TimeStep``, ``GetLayer``, plus state access.  Every call goes
+through the C ABI of ``libadi_b200.so``; there is no Python or CPU compute path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._abi import ADI_FP32, ADI_FP64, ADI_SOLVER_EXACT, ADI_SOLVER_FAST, AdiError  # noqa: F401
+
+__all__ = ["AdiSolver3D", "AdiError", "fluid_params_normalized", "ADI_FP32", "ADI_FP64",
+           "ADI_SOLVER_EXACT", "ADI_SOLVER_FAST", "library_path"]
+
+
+def library_path() -> str:
+    return _abi.LIB_PATH
+
+
+def fluid_params_normalized(Re: float, Pr: float, lam: float) -> _abi.FluidParams:
+    p = _abi.FluidParams()
+    _abi.check(_abi.load().adi_fluid_params_normalized(Re, Pr, lam, C.byref(p)))
+    return p
+
+
+def fluid_params_dimensional(vis, rho, R, k, cv) -> _abi.FluidParams:
+    p = _abi.FluidParams()
+    _abi.check(_abi.load().adi_fluid_params_dimensional(vis, rho, R, k, cv, C.byref(p)))
+    return p
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+class AdiSolver3D:
+    """One masked 3D domain resident on the current CUDA device."""
+
+    def __init__(self, domain, params=None, Re: float = 200.0, Pr: float = 0.72, lam: float = 1.4,
+                 precision: int = ADI_FP32, solver: int = ADI_SOLVER_FAST, stream=None):
+        self.lib = _abi.load()
+        self.domain = domain
+        self.precision = precision
+        self.dtype = np.float64 if precision == ADI_FP64 else np.float32
+        self.shape = domain.shape
+        self.h = C.c_void_p()
+        self.params = params if params is not None else fluid_params_normalized(Re, Pr, lam)
+        g = _abi.GridDesc(domain.nx, domain.ny, domain.nz, domain.dx, domain.dy, domain.dz, precision)
+        _abi.check(self.lib.adi_create(C.byref(g), C.byref(self.params), C.byref(self.h)))
+        if stream is not None:
+            self.set_stream(stream)
+        self._check(self.lib.adi_set_solver(self.h, solver))
+        arrs = domain.arrays()
+        self._check(self.lib.adi_set_mask(self.h, *[_ptr(a) for a in arrs]))
+        self.stats = None
+
+    # -- plumbing --
+    def _check(self, status):
+        _abi.check(status, self.h)
+
+    def set_stream(self, stream):
+        handle = stream if isinstance(stream, int) else getattr(stream, "cuda_stream", stream)
+        self._check(self.lib.adi_set_stream(self.h, C.c_void_p(handle)))
+
+    def set_solver(self, kind: int):
+        self._check(self.lib.adi_set_solver(self.h, kind))
+
+    def close(self):
+        if self.h:
+            self.lib.adi_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- reference surface --
+    def CreateSegments(self):
+        st = _abi.SegStats()
+        self._check(self.lib.adi_build_segments(self.h, C.byref(st)))
+        self.stats = {
+            "num_segments": list(st.num_segments), "num_nodes": list(st.num_nodes),
+            "max_size": list(st.max_size), "max_per_line": list(st.max_per_line), "num_in": st.num_in,
+        }
+        return self.stats
+
+    def UpdateBoundaries(self):
+        self._check(self.lib.adi_update_boundaries(self.h))
+
+    def TimeStep(self, dt, num_global, num_local, computeError=False):
+        self._check(self.lib.adi_time_step(self.h, dt, num_global, num_local, int(computeError)))
+
+    def step(self, dt, num_global, num_local, compute_error=False) -> int:
+        """UpdateBoundaries + TimeStep; returns the raw status (0 = OK)."""
+        return self.lib.adi_step(self.h, dt, num_global, num_local, int(compute_error))
+
+    def run(self, dt, num_global, num_local, n_steps, err_every=10):
+        self._check(self.lib.adi_run(self.h, dt, num_global, num_local, n_steps, err_every))
+
+    def GetLayer(self, outdimx=0, outdimy=0, outdimz=0):
+        ox, oy, oz = outdimx or self.shape[0], outdimy or self.shape[1], outdimz or self.shape[2]
+        v = np.zeros((ox, oy, oz, 3), self.dtype)
+        T = np.zeros((ox, oy, oz), np.float64)
+        self._check(self.lib.adi_get_layer(self.h, outdimx, outdimy, outdimz, _ptr(v), _ptr(T)))
+        return v, T
+
+    # -- state --
+    def segments(self, direction: int) -> np.ndarray:
+        n = C.c_int64()
+        self._check(self.lib.adi_get_segments(self.h, direction, None, 0, C.byref(n)))
+        out = np.zeros((max(n.value, 1), 7), np.int32)
+        self._check(self.lib.adi_get_segments(self.h, direction, _ptr(out), out.shape[0], C.byref(n)))
+        return out[: n.value]
+
+    def fields(self, which: int = 0):
+        out = [np.zeros(self.shape, self.dtype) for _ in range(4)]
+        self._check(self.lib.adi_get_state(self.h, which, *[_ptr(a) for a in out]))
+        return out
+
+    def set_state(self, u, v, w, T):
+        arrs = [np.ascontiguousarray(a, self.dtype) for a in (u, v, w, T)]
+        self._check(self.lib.adi_set_state(self.h, *[_ptr(a) for a in arrs]))
+
+    def div_error(self) -> float:
+        out = C.c_double()
+        self._check(self.lib.adi_div_error(self.h, C.byref(out)))
+        return out.value
+
+    def set_profiling(self, on: bool = True):
+        self._check(self.lib.adi_set_profiling(self.h, int(on)))
+
+    def profile(self, reset: bool = False) -> dict:
+        """Per kernel class: launches, summed CUDA-event ms, algorithmic bytes."""
+        p = _abi.Profile()
+        self._check(self.lib.adi_get_profile(self.h, C.byref(p), int(reset)))
+        return {name: {"launches": p.launches[c], "ms": p.ms[c], "bytes": p.bytes[c]}
+                for c, name in enumerate(_abi.KERNEL_CLASSES)}
+
+    def device_pointers(self):
+        arr = (C.c_void_p * 8)()
+        self._check(self.lib.adi_device_pointers(self.h, C.byref(arr)))
+        return [arr[i] for i in range(8)]

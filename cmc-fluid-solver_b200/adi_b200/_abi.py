@@ -1,0 +1,112 @@
+"""ctypes binding of libadi_b200.so (include/adi_b200.h).
+
+The shared library is built in-tree by ``cmc-fluid-solver_b200/build_adi.py``.  There is
+no fallback: if the library is missing or fails to load, importing the binding
+raises, so nothing can silently run a CPU path in its place.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libadi_b200.so")
+
+ADI_OK = 0
+STATUS_NAMES = {
+    0: "ADI_OK", 1: "ADI_ERR_BAD_ARG", 2: "ADI_ERR_CAPACITY", 3: "ADI_ERR_NONFINITE",
+    4: "ADI_ERR_NOT_CONVERGED", 5: "ADI_ERR_CUDA", 6: "ADI_ERR_TIMEOUT", 7: "ADI_ERR_DIVERGENCE",
+    8: "ADI_ERR_STATE", 9: "ADI_ERR_NO_DEVICE",
+}
+ADI_FP32, ADI_FP64 = 4, 8
+ADI_SOLVER_EXACT, ADI_SOLVER_FAST = 0, 1
+
+# every entry point include/adi_b200.h declares
+EXPORTED = [
+    "adi_fluid_params_normalized", "adi_fluid_params_dimensional", "adi_create", "adi_destroy",
+    "adi_set_stream", "adi_set_solver", "adi_last_error_string", "adi_set_mask", "adi_build_segments",
+    "adi_get_segments", "adi_update_boundaries", "adi_time_step", "adi_step", "adi_run", "adi_get_state",
+    "adi_set_state", "adi_get_layer", "adi_div_error", "adi_device_pointers", "adi_version",
+    "adi_set_profiling", "adi_get_profile",
+]
+
+K_NUM = 7
+KERNEL_CLASSES = ["step_begin", "sweep_x", "sweep_y", "sweep_z", "merge", "div_error", "other"]
+
+
+class GridDesc(C.Structure):
+    _fields_ = [("dimx", C.c_int), ("dimy", C.c_int), ("dimz", C.c_int),
+                ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double), ("precision", C.c_int)]
+
+
+class FluidParams(C.Structure):
+    _fields_ = [("v_T", C.c_double), ("v_vis", C.c_double), ("t_vis", C.c_double), ("t_phi", C.c_double)]
+
+
+class SegStats(C.Structure):
+    _fields_ = [("num_segments", C.c_int64 * 3), ("num_nodes", C.c_int64 * 3), ("max_size", C.c_int32 * 3),
+                ("max_per_line", C.c_int32 * 3), ("num_in", C.c_int64)]
+
+
+class Profile(C.Structure):
+    _fields_ = [("launches", C.c_int64 * 7), ("ms", C.c_double * 7), ("bytes", C.c_int64 * 7)]
+
+
+class AdiError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing; build it with cmc-fluid-solver_b200/build_adi.py")
+    lib = C.CDLL(LIB_PATH)
+    vp, i, d = C.c_void_p, C.c_int, C.c_double
+    sig = {
+        "adi_fluid_params_normalized": [d, d, d, C.POINTER(FluidParams)],
+        "adi_fluid_params_dimensional": [d, d, d, d, d, C.POINTER(FluidParams)],
+        "adi_create": [C.POINTER(GridDesc), C.POINTER(FluidParams), C.POINTER(vp)],
+        "adi_destroy": [vp],
+        "adi_set_stream": [vp, vp],
+        "adi_set_solver": [vp, i],
+        "adi_set_mask": [vp] + [vp] * 7,
+        "adi_build_segments": [vp, C.POINTER(SegStats)],
+        "adi_get_segments": [vp, i, vp, C.c_int64, C.POINTER(C.c_int64)],
+        "adi_update_boundaries": [vp],
+        "adi_time_step": [vp, d, i, i, i],
+        "adi_step": [vp, d, i, i, i],
+        "adi_run": [vp, d, i, i, i, i],
+        "adi_get_state": [vp, i, vp, vp, vp, vp],
+        "adi_set_state": [vp, vp, vp, vp, vp],
+        "adi_get_layer": [vp, i, i, i, vp, vp],
+        "adi_div_error": [vp, C.POINTER(d)],
+        "adi_device_pointers": [vp, C.POINTER(vp * 8)],
+        "adi_set_profiling": [vp, i],
+        "adi_get_profile": [vp, C.POINTER(Profile), i],
+    }
+    for name, args in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = C.c_int
+    lib.adi_last_error_string.argtypes = [vp]
+    lib.adi_last_error_string.restype = C.c_char_p
+    lib.adi_version.argtypes = []
+    lib.adi_version.restype = C.c_char_p
+    _lib = lib
+    return lib
+
+
+def check(status: int, handle=None) -> None:
+    if status != ADI_OK:
+        msg = ""
+        if handle:
+            raw = load().adi_last_error_string(handle)
+            msg = raw.decode() if raw else ""
+        raise AdiError(status, msg)

@@ -1,0 +1,679 @@
+// C ABI of libadi_b200.so (include/adi_b200.h): handle lifetime, device memory,
+// mask upload and checks, segment building and the time-step schedule.
+//
+// The schedule is the CPU backend's (AdiSolver3D.cpp:306-391 with SolveDirection
+// :564-666): per global iteration Z (cur -> next), Y (next -> half),
+// X (half -> next), each repeated num_local times with the nonlinear merge
+// temp = (temp + result)/2 after every sweep, plus one more merge after X.  The
+// merges are fused into the sweeps; the nonlinear layer is double buffered so that
+// every sweep sees the pre-merge layer, as the reference's separate merge pass
+// guarantees.  Layers are swapped by index, as the reference swaps pointers.
+#include "adi_b200.h"
+#include "adi_internal.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+using namespace adi;
+
+struct adi_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int prec = ADI_FP32;
+    int solver = ADI_SOLVER_FAST;
+    int nx = 0, ny = 0, nz = 0;
+    long long n = 0;
+    double dx = 0, dy = 0, dz = 0;
+    adi_fluid_params params{};
+
+    uint8_t *d_code = nullptr;
+    void *d_nv[4] = {};
+    void *d_L[5][4] = {};  // five layers of four fields
+    int cur = 0, nxt = 1, half = 2, ta = 3, tb = 4;
+
+    int *d_line_lo[3] = {}, *d_line_hi[3] = {};
+    int32_t *d_segs[3] = {};
+    long long nsegs[3] = {0, 0, 0};
+    void *d_scratch = nullptr;
+    size_t scratch_bytes = 0;
+
+    double *d_psum = nullptr, *d_sum = nullptr;
+    unsigned long long *d_pcnt = nullptr, *d_cnt = nullptr;
+
+    // built-in profiler (adi_set_profiling / adi_get_profile)
+    struct Rec {
+        int cls;
+        cudaEvent_t a, b;
+    };
+    bool prof_on = false;
+    std::vector<cudaEvent_t> ev_free;
+    std::vector<Rec> ev_pending;
+    int64_t launches[ADI_K_NUM] = {};
+    double ms[ADI_K_NUM] = {};
+    int64_t bytes[ADI_K_NUM] = {};
+    long long seg_nodes[3] = {0, 0, 0};
+
+    bool mask_set = false, segs_built = false, contract_ok = false;
+    std::string contract_msg;
+    std::string err;
+    double diff_error = 0.0;
+    long long num_in = 0;
+};
+
+namespace {
+
+const char *kVersion = "adi_b200 1.0 (sm_100a)";
+
+adi_status fail(adi_handle *h, adi_status s, const std::string &msg)
+{
+    if (h) h->err = msg;
+    return s;
+}
+
+#define CK(call)                                                                                       \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess)                                                                         \
+            return fail(h, ADI_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));         \
+    } while (0)
+
+size_t esize(const adi_handle *h) { return h->prec == ADI_FP64 ? 8 : 4; }
+
+template <typename R>
+DomainView<R> view(const adi_handle *h)
+{
+    DomainView<R> d;
+    d.nx = h->nx; d.ny = h->ny; d.nz = h->nz; d.n = h->n;
+    d.code = h->d_code;
+    for (int v = 0; v < 4; v++) d.nv[v] = (const R *)h->d_nv[v];
+    return d;
+}
+
+template <typename R>
+Layer<R> layer(const adi_handle *h, int l)
+{
+    Layer<R> x;
+    for (int v = 0; v < 4; v++) x.f[v] = (R *)h->d_L[l][v];
+    return x;
+}
+
+template <typename R>
+CLayer<R> clayer(const adi_handle *h, int l)
+{
+    CLayer<R> x;
+    for (int v = 0; v < 4; v++) x.f[v] = (const R *)h->d_L[l][v];
+    return x;
+}
+
+// Scalar constants of one sweep, in the working precision, with BuildMatrix's
+// operations (AdiSolver3D.cpp:744-752: vis/(h*h); :761,775,789: 3/dt + 2*vis;
+// (2*h) denominators).  Host code is compiled with -ffp-contract=off.
+template <typename R>
+SweepConst<R> sweep_const(const adi_handle *h, int dir, R dt)
+{
+    SweepConst<R> k;
+    const R dx = (R)h->dx, dy = (R)h->dy, dz = (R)h->dz;
+    const R hh = dir == 0 ? dx : (dir == 1 ? dy : dz);
+    const R v_vis = (R)h->params.v_vis, t_vis = (R)h->params.t_vis;
+    k.three = R(3);
+    k.dt = dt;
+    k.two_h = R(2) * hh;
+    k.vis_v = v_vis / (hh * hh);
+    k.vis_t = t_vis / (hh * hh);
+    k.b_v = R(3) / dt + R(2) * k.vis_v;
+    k.b_t = R(3) / dt + R(2) * k.vis_t;
+    k.v_T = (R)h->params.v_T;
+    k.t_phi = (R)h->params.t_phi;
+    k.two_dx = R(2) * dx;
+    k.two_dy = R(2) * dy;
+    k.two_dz = R(2) * dz;
+    return k;
+}
+
+cudaEvent_t take_event(adi_handle *h)
+{
+    if (!h->ev_free.empty()) {
+        cudaEvent_t e = h->ev_free.back();
+        h->ev_free.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    return e;
+}
+
+// Launches through `launch` (which returns a cudaError_t), counting it under the
+// kernel class `cls` with `bytes` algorithmic HBM bytes, and bracketing it with
+// an event pair when profiling is on.
+template <class F>
+cudaError_t timed(adi_handle *h, int cls, int64_t bytes, F launch)
+{
+    h->launches[cls]++;
+    h->bytes[cls] += bytes;
+    if (!h->prof_on) return launch();
+    cudaEvent_t a = take_event(h), b = take_event(h);
+    if (!a || !b) return cudaErrorMemoryAllocation;
+    cudaEventRecord(a, h->stream);
+    cudaError_t e = launch();
+    cudaEventRecord(b, h->stream);
+    h->ev_pending.push_back({cls, a, b});
+    return e;
+}
+
+cudaError_t fold_profile(adi_handle *h)
+{
+    if (h->ev_pending.empty()) return cudaSuccess;
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return e;
+    for (auto &r : h->ev_pending) {
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, r.a, r.b) == cudaSuccess) h->ms[r.cls] += t;
+        h->ev_free.push_back(r.a);
+        h->ev_free.push_back(r.b);
+    }
+    h->ev_pending.clear();
+    return cudaSuccess;
+}
+
+void free_all(adi_handle *h)
+{
+    for (auto &r : h->ev_pending) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (auto e : h->ev_free) cudaEventDestroy(e);
+    h->ev_pending.clear();
+    h->ev_free.clear();
+    cudaFree(h->d_code);
+    for (int v = 0; v < 4; v++) cudaFree(h->d_nv[v]);
+    for (int l = 0; l < 5; l++)
+        for (int v = 0; v < 4; v++) cudaFree(h->d_L[l][v]);
+    for (int d = 0; d < 3; d++) {
+        cudaFree(h->d_line_lo[d]);
+        cudaFree(h->d_line_hi[d]);
+        cudaFree(h->d_segs[d]);
+    }
+    cudaFree(h->d_scratch);
+    cudaFree(h->d_psum);
+    cudaFree(h->d_pcnt);
+    cudaFree(h->d_sum);
+    cudaFree(h->d_cnt);
+}
+
+// The solver contract (the reference relies on it too: stencils read +-1 without
+// bounds checks, TimeLayer3D.h:256-259,338-343).
+std::string check_contract(const adi_handle *h, const uint8_t *t, const uint8_t *bv, const uint8_t *bt)
+{
+    const int nx = h->nx, ny = h->ny, nz = h->nz;
+    const long long sx = (long long)ny * nz, sy = nz;
+    for (int i = 0; i < nx; i++)
+        for (int j = 0; j < ny; j++)
+            for (int k = 0; k < nz; k++) {
+                long long id = i * sx + j * sy + k;
+                bool frame = i == 0 || j == 0 || k == 0 || i == nx - 1 || j == ny - 1 || k == nz - 1;
+                if (t[id] == NODE_IN) {
+                    if (frame) return "NODE_IN cell on the outer frame";
+                    if (t[id - sx] == NODE_OUT || t[id + sx] == NODE_OUT || t[id - sy] == NODE_OUT ||
+                        t[id + sy] == NODE_OUT || t[id - 1] == NODE_OUT || t[id + 1] == NODE_OUT)
+                        return "NODE_IN cell next to a NODE_OUT cell";
+                } else if (!frame && (bv[id] == BC_FREE || bt[id] == BC_FREE)) {
+                    if ((t[id - sx] == NODE_IN && t[id + sx] == NODE_IN) ||
+                        (t[id - sy] == NODE_IN && t[id + sy] == NODE_IN) ||
+                        (t[id - 1] == NODE_IN && t[id + 1] == NODE_IN))
+                        return "BC_FREE cell shared by two segments of one line";
+                }
+            }
+    return "";
+}
+
+template <typename R>
+adi_status run_sweeps(adi_handle *h, R dt, int num_global, int num_local)
+{
+    const DomainView<R> d = view<R>(h);
+    for (int it = 0; it < num_global; it++) {
+        const int order[3] = {2, 1, 0};
+        const int src[3] = {h->cur, h->nxt, h->half};
+        const int dst[3] = {h->nxt, h->half, h->nxt};
+        for (int q = 0; q < 3; q++) {
+            const int dir = order[q];
+            const SweepConst<R> k = sweep_const<R>(h, dir, dt);
+            // algorithmic bytes: IN rows read cur, temp and write next, temp (16
+            // values); end rows write next (4 values)
+            const int64_t bytes = (int64_t)sizeof(R) * (16 * h->num_in + 4 * (h->seg_nodes[dir] - h->num_in));
+            const int cls = dir == 0 ? ADI_K_SWEEP_X : (dir == 1 ? ADI_K_SWEEP_Y : ADI_K_SWEEP_Z);
+            for (int l = 0; l < num_local; l++) {
+                const int merges = (dir == 0 && l == num_local - 1) ? 2 : 1;
+                CK(timed(h, cls, bytes, [&] {
+                    return launch_sweep_exact<R>(dir, d, h->d_line_lo[dir], h->d_line_hi[dir], clayer<R>(h, src[q]),
+                                                 clayer<R>(h, h->ta), layer<R>(h, dst[q]), layer<R>(h, h->tb),
+                                                 (R *)h->d_scratch, k, merges, h->stream);
+                }));
+                std::swap(h->ta, h->tb);
+            }
+        }
+    }
+    return ADI_OK;
+}
+
+template <typename R>
+adi_status div_error_of(adi_handle *h, int l, double *out)
+{
+    CK(timed(h, ADI_K_DIV_ERROR, (int64_t)h->n * (1 + 3 * (int64_t)sizeof(R)), [&] {
+        return launch_div_error<R>(view<R>(h), clayer<R>(h, l), (R)h->dx, (R)h->dy, (R)h->dz, h->d_psum, h->d_pcnt,
+                                   DIV_BLOCKS, h->d_sum, h->d_cnt, h->stream);
+    }));
+    double sum = 0;
+    unsigned long long cnt = 0;
+    CK(cudaMemcpyAsync(&sum, h->d_sum, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(&cnt, h->d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    *out = cnt ? sum / (double)cnt : 0.0;
+    return ADI_OK;
+}
+
+template <typename R>
+adi_status time_step(adi_handle *h, double dt, int num_global, int num_local, int compute_error, bool update_bnd)
+{
+    const R dtr = (R)dt;
+    CK(timed(h, ADI_K_STEP_BEGIN, (int64_t)h->n * (1 + 8 * (int64_t)sizeof(R)), [&] {
+        return launch_step_begin<R>(view<R>(h), layer<R>(h, h->cur), layer<R>(h, h->nxt), layer<R>(h, h->ta),
+                                    layer<R>(h, h->tb), update_bnd, h->stream);
+    }));
+    adi_status s = run_sweeps<R>(h, dtr, num_global, num_local);
+    if (s != ADI_OK) return s;
+    if (compute_error) {
+        s = div_error_of<R>(h, h->nxt, &h->diff_error);
+        if (s != ADI_OK) return s;
+    }
+    if (h->diff_error > 0.01) {
+        char buf[128];
+        snprintf(buf, sizeof buf, "divergence error %.8f above 0.01", h->diff_error);
+        return fail(h, ADI_ERR_DIVERGENCE, buf);
+    }
+    std::swap(h->cur, h->nxt);
+    return ADI_OK;
+}
+
+adi_status check_ready(adi_handle *h)
+{
+    if (!h) return ADI_ERR_BAD_ARG;
+    if (!h->mask_set) return fail(h, ADI_ERR_STATE, "adi_set_mask has not been called");
+    if (!h->segs_built) return fail(h, ADI_ERR_STATE, "adi_build_segments has not been called");
+    if (!h->contract_ok) return fail(h, ADI_ERR_BAD_ARG, "mask breaks the solver contract: " + h->contract_msg);
+    return ADI_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+const char *adi_version(void) { return kVersion; }
+
+adi_status adi_fluid_params_normalized(double Re, double Pr, double lambda, adi_fluid_params *out)
+{
+    if (!out || Re == 0.0 || Pr == 0.0 || lambda == 0.0) return ADI_ERR_BAD_ARG;
+    out->v_T = 1.0;
+    out->v_vis = 1.0 / Re;
+    out->t_vis = 1.0 / (Re * Pr);
+    out->t_phi = (lambda - 1) / (lambda * Re);
+    return ADI_OK;
+}
+
+adi_status adi_fluid_params_dimensional(double vis, double rho, double R, double k, double cv, adi_fluid_params *out)
+{
+    if (!out || rho == 0.0 || cv == 0.0) return ADI_ERR_BAD_ARG;
+    out->v_T = R;
+    out->v_vis = vis / rho;
+    out->t_vis = k / (rho * cv);
+    out->t_phi = vis / (rho * cv);
+    return ADI_OK;
+}
+
+adi_status adi_create(const adi_grid_desc *g, const adi_fluid_params *p, adi_handle **out)
+{
+    if (!g || !p || !out) return ADI_ERR_BAD_ARG;
+    *out = nullptr;
+    if (g->dimx < 3 || g->dimy < 3 || g->dimz < 3) return ADI_ERR_BAD_ARG;
+    if (g->precision != ADI_FP32 && g->precision != ADI_FP64) return ADI_ERR_BAD_ARG;
+    if (!(g->dx > 0) || !(g->dy > 0) || !(g->dz > 0)) return ADI_ERR_BAD_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return ADI_ERR_NO_DEVICE;
+    adi_handle *h = new (std::nothrow) adi_handle();
+    if (!h) return ADI_ERR_CAPACITY;
+    cudaGetDevice(&h->device);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, h->device) != cudaSuccess || prop.major < 10) {
+        delete h;
+        return ADI_ERR_NO_DEVICE;
+    }
+    h->prec = g->precision;
+    h->nx = g->dimx; h->ny = g->dimy; h->nz = g->dimz;
+    h->n = (long long)g->dimx * g->dimy * g->dimz;
+    h->dx = g->dx; h->dy = g->dy; h->dz = g->dz;
+    h->params = *p;
+    const size_t fb = (size_t)h->n * esize(h);
+    auto alloc = [&](void **ptr, size_t bytes) { return cudaMalloc(ptr, bytes); };
+    cudaError_t e = alloc((void **)&h->d_code, h->n);
+    for (int v = 0; v < 4 && e == cudaSuccess; v++) e = alloc(&h->d_nv[v], fb);
+    for (int l = 0; l < 5 && e == cudaSuccess; l++)
+        for (int v = 0; v < 4 && e == cudaSuccess; v++) e = alloc(&h->d_L[l][v], fb);
+    for (int d = 0; d < 3 && e == cudaSuccess; d++) {
+        LineGeom lg = line_geom(d, h->nx, h->ny, h->nz);
+        e = alloc((void **)&h->d_line_lo[d], sizeof(int) * lg.nlines);
+        if (e == cudaSuccess) e = alloc((void **)&h->d_line_hi[d], sizeof(int) * lg.nlines);
+    }
+    h->scratch_bytes = 6 * fb;
+    if (e == cudaSuccess) e = alloc(&h->d_scratch, h->scratch_bytes);
+    if (e == cudaSuccess) e = alloc((void **)&h->d_psum, sizeof(double) * DIV_BLOCKS);
+    if (e == cudaSuccess) e = alloc((void **)&h->d_pcnt, sizeof(unsigned long long) * DIV_BLOCKS);
+    if (e == cudaSuccess) e = alloc((void **)&h->d_sum, sizeof(double));
+    if (e == cudaSuccess) e = alloc((void **)&h->d_cnt, sizeof(unsigned long long));
+    if (e == cudaSuccess)
+        for (int l = 0; l < 5 && e == cudaSuccess; l++)
+            for (int v = 0; v < 4 && e == cudaSuccess; v++) e = cudaMemset(h->d_L[l][v], 0, fb);
+    if (e != cudaSuccess) {
+        free_all(h);
+        delete h;
+        cudaGetLastError();
+        return e == cudaErrorMemoryAllocation ? ADI_ERR_CAPACITY : ADI_ERR_CUDA;
+    }
+    *out = h;
+    return ADI_OK;
+}
+
+adi_status adi_destroy(adi_handle *h)
+{
+    if (!h) return ADI_OK;
+    cudaStreamSynchronize(h->stream);
+    free_all(h);
+    delete h;
+    return ADI_OK;
+}
+
+adi_status adi_set_stream(adi_handle *h, void *stream)
+{
+    if (!h) return ADI_ERR_BAD_ARG;
+    h->stream = (cudaStream_t)stream;
+    return ADI_OK;
+}
+
+adi_status adi_set_solver(adi_handle *h, int kind)
+{
+    if (!h) return ADI_ERR_BAD_ARG;
+    if (kind != ADI_SOLVER_EXACT && kind != ADI_SOLVER_FAST) return fail(h, ADI_ERR_BAD_ARG, "unknown solver kind");
+    h->solver = kind;
+    return ADI_OK;
+}
+
+const char *adi_last_error_string(const adi_handle *h)
+{
+    if (!h) return "null handle";
+    return h->err.c_str();
+}
+
+adi_status adi_set_mask(adi_handle *h, const uint8_t *type, const uint8_t *bc_vel, const uint8_t *bc_temp,
+                        const double *vx, const double *vy, const double *vz, const double *T)
+{
+    if (!h || !type || !bc_vel || !bc_temp || !vx || !vy || !vz || !T) return ADI_ERR_BAD_ARG;
+    const long long n = h->n;
+    std::vector<uint8_t> code(n);
+    long long nin = 0;
+    for (long long i = 0; i < n; i++) {
+        if (type[i] > NODE_VALVE || bc_vel[i] > BC_FREE || bc_temp[i] > BC_FREE)
+            return fail(h, ADI_ERR_BAD_ARG, "node type or BC code out of range at index " + std::to_string(i));
+        code[i] = (uint8_t)(type[i] | (bc_vel[i] == BC_FREE ? CODE_VEL_FREE : 0) |
+                            (bc_temp[i] == BC_FREE ? CODE_TEMP_FREE : 0));
+        nin += type[i] == NODE_IN;
+    }
+    h->contract_msg = check_contract(h, type, bc_vel, bc_temp);
+    h->contract_ok = h->contract_msg.empty();
+    h->num_in = nin;
+    CK(cudaMemcpyAsync(h->d_code, code.data(), n, cudaMemcpyHostToDevice, h->stream));
+    const double *src[4] = {vx, vy, vz, T};
+    const size_t fb = (size_t)n * esize(h);
+    if (h->prec == ADI_FP64) {
+        for (int v = 0; v < 4; v++) {
+            CK(cudaMemcpyAsync(h->d_nv[v], src[v], fb, cudaMemcpyHostToDevice, h->stream));
+            CK(cudaMemcpyAsync(h->d_L[h->cur][v], src[v], fb, cudaMemcpyHostToDevice, h->stream));
+        }
+        CK(cudaStreamSynchronize(h->stream));
+    } else {
+        std::vector<float> tmp(n);
+        for (int v = 0; v < 4; v++) {
+            for (long long i = 0; i < n; i++) tmp[i] = (float)src[v][i];
+            CK(cudaMemcpyAsync(h->d_nv[v], tmp.data(), fb, cudaMemcpyHostToDevice, h->stream));
+            CK(cudaMemcpyAsync(h->d_L[h->cur][v], tmp.data(), fb, cudaMemcpyHostToDevice, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+        }
+    }
+    h->mask_set = true;
+    h->segs_built = false;
+    return ADI_OK;
+}
+
+adi_status adi_build_segments(adi_handle *h, adi_seg_stats *stats)
+{
+    if (!h) return ADI_ERR_BAD_ARG;
+    if (!h->mask_set) return fail(h, ADI_ERR_STATE, "adi_set_mask has not been called");
+    adi_seg_stats st;
+    memset(&st, 0, sizeof st);
+    st.num_in = h->num_in;
+    for (int dir = 0; dir < 3; dir++) {
+        LineGeom lg = line_geom(dir, h->nx, h->ny, h->nz);
+        int *d_cnt = nullptr, *d_max = nullptr;
+        long long *d_nodes = nullptr, *d_off = nullptr;
+        CK(cudaMalloc(&d_cnt, sizeof(int) * lg.nlines));
+        CK(cudaMalloc(&d_max, sizeof(int) * lg.nlines));
+        CK(cudaMalloc(&d_nodes, sizeof(long long) * lg.nlines));
+        CK(cudaMalloc(&d_off, sizeof(long long) * lg.nlines));
+        CK(launch_segment_scan(dir, h->nx, h->ny, h->nz, h->d_code, d_cnt, h->d_line_lo[dir], h->d_line_hi[dir],
+                               d_max, d_nodes, h->stream));
+        std::vector<int> cnt(lg.nlines), mx(lg.nlines);
+        std::vector<long long> nodes(lg.nlines), off(lg.nlines);
+        CK(cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(int) * lg.nlines, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(mx.data(), d_max, sizeof(int) * lg.nlines, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(nodes.data(), d_nodes, sizeof(long long) * lg.nlines, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        long long total = 0, tnodes = 0;
+        int maxlen = 0, maxper = 0;
+        for (int l = 0; l < lg.nlines; l++) {
+            off[l] = total;
+            total += cnt[l];
+            tnodes += nodes[l];
+            maxlen = mx[l] > maxlen ? mx[l] : maxlen;
+            maxper = cnt[l] > maxper ? cnt[l] : maxper;
+        }
+        st.num_segments[dir] = total;
+        st.num_nodes[dir] = tnodes;
+        h->seg_nodes[dir] = tnodes;
+        st.max_size[dir] = maxlen;
+        st.max_per_line[dir] = maxper;
+        cudaFree(h->d_segs[dir]);
+        h->d_segs[dir] = nullptr;
+        h->nsegs[dir] = total;
+        if (total > 0) {
+            CK(cudaMalloc(&h->d_segs[dir], sizeof(int32_t) * 7 * total));
+            CK(cudaMemcpyAsync(d_off, off.data(), sizeof(long long) * lg.nlines, cudaMemcpyHostToDevice, h->stream));
+            CK(launch_segment_write(dir, h->nx, h->ny, h->nz, h->d_code, d_off, h->d_segs[dir], h->stream));
+        }
+        CK(cudaStreamSynchronize(h->stream));
+        cudaFree(d_cnt);
+        cudaFree(d_max);
+        cudaFree(d_nodes);
+        cudaFree(d_off);
+    }
+    h->segs_built = true;
+    if (stats) *stats = st;
+    return ADI_OK;
+}
+
+adi_status adi_get_segments(adi_handle *h, int dir, int32_t *out7, int64_t cap, int64_t *count)
+{
+    if (!h || dir < 0 || dir > 2) return ADI_ERR_BAD_ARG;
+    if (!h->segs_built) return fail(h, ADI_ERR_STATE, "adi_build_segments has not been called");
+    if (count) *count = h->nsegs[dir];
+    if (!out7) return ADI_OK;
+    if (cap < h->nsegs[dir]) return fail(h, ADI_ERR_CAPACITY, "segment buffer too small");
+    if (h->nsegs[dir] > 0) {
+        CK(cudaMemcpyAsync(out7, h->d_segs[dir], sizeof(int32_t) * 7 * h->nsegs[dir], cudaMemcpyDeviceToHost,
+                           h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    return ADI_OK;
+}
+
+adi_status adi_update_boundaries(adi_handle *h)
+{
+    if (!h) return ADI_ERR_BAD_ARG;
+    if (!h->mask_set) return fail(h, ADI_ERR_STATE, "adi_set_mask has not been called");
+    CK(timed(h, ADI_K_OTHER, 0, [&] {
+        if (h->prec == ADI_FP64) return launch_update_boundaries<double>(view<double>(h), layer<double>(h, h->cur), h->stream);
+        return launch_update_boundaries<float>(view<float>(h), layer<float>(h, h->cur), h->stream);
+    }));
+    return ADI_OK;
+}
+
+static adi_status step_impl(adi_handle *h, double dt, int num_global, int num_local, int compute_error, bool bnd)
+{
+    adi_status s = check_ready(h);
+    if (s != ADI_OK) return s;
+    if (num_global < 1 || num_local < 1) return fail(h, ADI_ERR_BAD_ARG, "num_global and num_local must be >= 1");
+    if (!(dt > 0) || !std::isfinite(dt)) return fail(h, ADI_ERR_BAD_ARG, "dt must be positive and finite");
+    if (h->prec == ADI_FP64) return time_step<double>(h, dt, num_global, num_local, compute_error, bnd);
+    return time_step<float>(h, dt, num_global, num_local, compute_error, bnd);
+}
+
+adi_status adi_time_step(adi_handle *h, double dt, int num_global, int num_local, int compute_error)
+{
+    return step_impl(h, dt, num_global, num_local, compute_error, false);
+}
+
+adi_status adi_step(adi_handle *h, double dt, int num_global, int num_local, int compute_error)
+{
+    return step_impl(h, dt, num_global, num_local, compute_error, true);
+}
+
+adi_status adi_run(adi_handle *h, double dt, int num_global, int num_local, int n_steps, int err_every)
+{
+    if (!h || n_steps < 0) return ADI_ERR_BAD_ARG;
+    for (int i = 0; i < n_steps; i++) {
+        int ce = (err_every > 0 && i % err_every == 0) || i == n_steps - 1;
+        adi_status s = adi_step(h, dt, num_global, num_local, ce);
+        if (s != ADI_OK) return s;
+    }
+    return ADI_OK;
+}
+
+adi_status adi_get_state(adi_handle *h, int which, void *u, void *v, void *w, void *T)
+{
+    if (!h || !u || !v || !w || !T || (which != 0 && which != 1)) return ADI_ERR_BAD_ARG;
+    const int l = which == 0 ? h->cur : h->nxt;
+    void *dst[4] = {u, v, w, T};
+    const size_t fb = (size_t)h->n * esize(h);
+    for (int f = 0; f < 4; f++)
+        CK(cudaMemcpyAsync(dst[f], h->d_L[l][f], fb, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return ADI_OK;
+}
+
+adi_status adi_set_state(adi_handle *h, const void *u, const void *v, const void *w, const void *T)
+{
+    if (!h || !u || !v || !w || !T) return ADI_ERR_BAD_ARG;
+    const void *src[4] = {u, v, w, T};
+    const size_t fb = (size_t)h->n * esize(h);
+    for (int f = 0; f < 4; f++)
+        CK(cudaMemcpyAsync(h->d_L[h->cur][f], src[f], fb, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return ADI_OK;
+}
+
+adi_status adi_get_layer(adi_handle *h, int outdimx, int outdimy, int outdimz, void *vout, double *Tout)
+{
+    if (!h || !vout || !Tout || outdimx < 0 || outdimy < 0 || outdimz < 0) return ADI_ERR_BAD_ARG;
+    if (!h->mask_set) return fail(h, ADI_ERR_STATE, "adi_set_mask has not been called");
+    if (outdimx == 0) outdimx = h->nx;
+    if (outdimy == 0) outdimy = h->ny;
+    if (outdimz == 0) outdimz = h->nz;
+    const int l = h->nxt;
+    if (h->prec == ADI_FP64) CK(launch_fill_missing<double>(view<double>(h), layer<double>(h, l), h->stream));
+    else CK(launch_fill_missing<float>(view<float>(h), layer<float>(h, l), h->stream));
+    const size_t es = esize(h), fb = (size_t)h->n * es;
+    std::vector<unsigned char> host(4 * fb);
+    for (int f = 0; f < 4; f++)
+        CK(cudaMemcpyAsync(host.data() + f * fb, h->d_L[l][f], fb, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    // FilterToArrays point sampling (TimeLayer3D.h:869-881)
+    for (int i = 0; i < outdimx; i++)
+        for (int j = 0; j < outdimy; j++)
+            for (int k = 0; k < outdimz; k++) {
+                const long long x = (long long)i * h->nx / outdimx, y = (long long)j * h->ny / outdimy,
+                                z = (long long)k * h->nz / outdimz;
+                const long long src = (x * h->ny + y) * h->nz + z;
+                const long long ind = ((long long)i * outdimy + j) * outdimz + k;
+                if (es == 8) {
+                    const double *H = (const double *)host.data();
+                    double *V = (double *)vout;
+                    V[3 * ind + 0] = H[src];
+                    V[3 * ind + 1] = H[h->n + src];
+                    V[3 * ind + 2] = H[2 * h->n + src];
+                    Tout[ind] = H[3 * h->n + src];
+                } else {
+                    const float *H = (const float *)host.data();
+                    float *V = (float *)vout;
+                    V[3 * ind + 0] = H[src];
+                    V[3 * ind + 1] = H[h->n + src];
+                    V[3 * ind + 2] = H[2 * h->n + src];
+                    Tout[ind] = H[3 * h->n + src];
+                }
+            }
+    return ADI_OK;
+}
+
+adi_status adi_div_error(adi_handle *h, double *out)
+{
+    if (!h || !out) return ADI_ERR_BAD_ARG;
+    if (!h->mask_set) return fail(h, ADI_ERR_STATE, "adi_set_mask has not been called");
+    if (!h->contract_ok) return fail(h, ADI_ERR_BAD_ARG, "mask breaks the solver contract: " + h->contract_msg);
+    if (h->prec == ADI_FP64) return div_error_of<double>(h, h->cur, out);
+    return div_error_of<float>(h, h->cur, out);
+}
+
+adi_status adi_set_profiling(adi_handle *h, int on)
+{
+    if (!h) return ADI_ERR_BAD_ARG;
+    h->prof_on = on != 0;
+    return ADI_OK;
+}
+
+adi_status adi_get_profile(adi_handle *h, adi_profile *out, int reset)
+{
+    if (!h || !out) return ADI_ERR_BAD_ARG;
+    CK(fold_profile(h));
+    for (int c = 0; c < ADI_K_NUM; c++) {
+        out->launches[c] = h->launches[c];
+        out->ms[c] = h->ms[c];
+        out->bytes[c] = h->bytes[c];
+    }
+    if (reset) {
+        memset(h->launches, 0, sizeof h->launches);
+        memset(h->ms, 0, sizeof h->ms);
+        memset(h->bytes, 0, sizeof h->bytes);
+    }
+    return ADI_OK;
+}
+
+adi_status adi_device_pointers(adi_handle *h, void *out8[8])
+{
+    if (!h || !out8) return ADI_ERR_BAD_ARG;
+    for (int f = 0; f < 4; f++) {
+        out8[f] = h->d_L[h->cur][f];
+        out8[4 + f] = h->d_L[h->nxt][f];
+    }
+    return ADI_OK;
+}
+
+} // extern "C"

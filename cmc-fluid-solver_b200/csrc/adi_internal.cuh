@@ -1,0 +1,114 @@
+// Internal declarations shared by the CUDA translation units of libadi_b200.so.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace adi {
+
+// Node types and BC codes of the reference (Common/Geometry.h:31-41).
+enum : uint8_t { NODE_IN = 0, NODE_OUT = 1, NODE_BOUND = 2, NODE_VALVE = 3 };
+enum : uint8_t { BC_NOSLIP = 0, BC_FREE = 1 };
+
+// One byte per node on the device: bits 0-1 node type, bit 2 bc_vel == FREE,
+// bit 3 bc_temp == FREE.  Replaces the 28-byte (FP32) Node AoS (Grid3D.h:73-88)
+// on the sweep's read path; the node values live in four separate arrays.
+constexpr uint8_t CODE_TYPE = 0x3;
+constexpr uint8_t CODE_VEL_FREE = 0x4;
+constexpr uint8_t CODE_TEMP_FREE = 0x8;
+
+__host__ __device__ inline bool code_is_in(uint8_t c) { return (c & CODE_TYPE) == NODE_IN; }
+__host__ __device__ inline bool code_is_bv(uint8_t c)
+{
+    uint8_t t = c & CODE_TYPE;
+    return t == NODE_BOUND || t == NODE_VALVE;
+}
+
+// Four fields U, V, W, T of one time layer; element (i,j,k) at (i*ny + j)*nz + k.
+template <typename R>
+struct Layer {
+    R *f[4];
+};
+template <typename R>
+struct CLayer {
+    const R *f[4];
+};
+
+// Geometry of the lines of one sweep direction.  Lines are numbered in the
+// order Grid3D::GenerateListSegments visits them (Grid3D.cpp:64-65):
+//   X: line = j*nz + k, Y: line = i*nz + k, Z: line = i*ny + j.
+struct LineGeom {
+    int nx, ny, nz;
+    int len;          // nodes per line
+    int nlines;
+    long long stride; // element stride along the line
+};
+
+__host__ __device__ inline LineGeom line_geom(int dir, int nx, int ny, int nz)
+{
+    LineGeom g;
+    g.nx = nx; g.ny = ny; g.nz = nz;
+    if (dir == 0) { g.len = nx; g.nlines = ny * nz; g.stride = (long long)ny * nz; }
+    else if (dir == 1) { g.len = ny; g.nlines = nx * nz; g.stride = nz; }
+    else { g.len = nz; g.nlines = nx * ny; g.stride = 1; }
+    return g;
+}
+
+__host__ __device__ inline long long line_base(int dir, const LineGeom &g, int line)
+{
+    if (dir == 0) return line;                                            // (0, j, k): j*nz + k
+    if (dir == 1) return (long long)(line / g.nz) * g.ny * g.nz + (line % g.nz); // (i, 0, k)
+    return (long long)line * g.nz;                                        // (i, j, 0)
+}
+
+// Per-sweep scalar constants, evaluated in the working precision with the same
+// operations BuildMatrix uses (AdiSolver3D.cpp:744-752,760-797).
+template <typename R>
+struct SweepConst {
+    R three;         // 3
+    R dt;            // dt
+    R two_h;         // 2 * h along the line
+    R vis_v, vis_t;  // v_vis / (h*h), t_vis / (h*h)
+    R b_v, b_t;      // 3/dt + 2*vis
+    R v_T, t_phi;
+    R two_dx, two_dy, two_dz;
+};
+
+// Device-side description of one domain, passed by value to kernels.
+template <typename R>
+struct DomainView {
+    int nx, ny, nz;
+    long long n;
+    const uint8_t *code;
+    const R *nv[4];   // node values v.x v.y v.z T
+};
+
+// ---- launchers (each returns cudaGetLastError()) ----
+template <typename R>
+cudaError_t launch_step_begin(const DomainView<R> &d, Layer<R> cur, Layer<R> next, Layer<R> ta, Layer<R> tb,
+                              bool update_boundaries, cudaStream_t s);
+template <typename R>
+cudaError_t launch_update_boundaries(const DomainView<R> &d, Layer<R> cur, cudaStream_t s);
+template <typename R>
+cudaError_t launch_merge(const DomainView<R> &d, CLayer<R> src, Layer<R> dest, cudaStream_t s);
+template <typename R>
+cudaError_t launch_div_error(const DomainView<R> &d, CLayer<R> l, R dx, R dy, R dz, double *partial_sum,
+                             unsigned long long *partial_cnt, int nblocks, double *out_sum,
+                             unsigned long long *out_cnt, cudaStream_t s);
+template <typename R>
+cudaError_t launch_fill_missing(const DomainView<R> &d, Layer<R> l, cudaStream_t s);
+
+template <typename R>
+cudaError_t launch_sweep_exact(int dir, const DomainView<R> &d, const int *line_lo, const int *line_hi,
+                               CLayer<R> cur, CLayer<R> temp_in, Layer<R> next, Layer<R> temp_out,
+                               R *scratch, const SweepConst<R> &k, int merges, cudaStream_t s);
+
+cudaError_t launch_segment_scan(int dir, int nx, int ny, int nz, const uint8_t *code, int *line_count,
+                                int *line_lo, int *line_hi, int *line_maxlen, long long *line_nodes,
+                                cudaStream_t s);
+cudaError_t launch_segment_write(int dir, int nx, int ny, int nz, const uint8_t *code,
+                                 const long long *line_offset, int32_t *out7, cudaStream_t s);
+
+constexpr int DIV_BLOCKS = 592;  // 4 x 148 SMs
+
+} // namespace adi

@@ -1,0 +1,202 @@
+// Whole-layer kernels around the sweeps: boundary refresh, the per-step layer
+// set-up, the standalone merge, the divergence error and the GetLayer fill.
+// All are streaming HBM kernels: one pass, grid-stride, coalesced.
+#include "adi_internal.cuh"
+
+namespace adi {
+
+__device__ __forceinline__ long long gtid() { return (long long)blockIdx.x * blockDim.x + threadIdx.x; }
+__device__ __forceinline__ long long gstride() { return (long long)gridDim.x * blockDim.x; }
+
+static int grid_for(long long n, int threads)
+{
+    long long b = (n + threads - 1) / threads;
+    long long cap = 148LL * 16;  // 16 resident 256-thread blocks per SM
+    if (b > cap) b = cap;
+    return (int)(b < 1 ? 1 : b);
+}
+
+// cur[BOUND|VALVE] = node values.  CPU semantics of UpdateBoundaries
+// (Solver3D.cpp:27-34 / AdiSolver3D.cpp:290-294: CopyFromGrid for BOUND and VALVE).
+template <typename R>
+__global__ void update_boundaries_kernel(DomainView<R> d, Layer<R> cur)
+{
+    for (long long i = gtid(); i < d.n; i += gstride()) {
+        if (code_is_bv(d.code[i])) {
+#pragma unroll
+            for (int v = 0; v < 4; v++) cur.f[v][i] = d.nv[v][i];
+        }
+    }
+}
+
+// Start of TimeStep (AdiSolver3D.cpp:310-320): next[BOUND|VALVE] = cur and
+// temp = cur.  Both temp buffers of the double-buffered nonlinear layer get the
+// copy, because the sweeps only ever write IN nodes of the buffer they fill.
+// With update_boundaries, cur[BOUND|VALVE] is first refreshed from the node values
+// (the driver calls UpdateBoundaries right before TimeStep, FluidSolver3D.cpp:241-242).
+template <typename R>
+__global__ void step_begin_kernel(DomainView<R> d, Layer<R> cur, Layer<R> next, Layer<R> ta, Layer<R> tb,
+                                  bool update_boundaries)
+{
+    for (long long i = gtid(); i < d.n; i += gstride()) {
+        bool bv = code_is_bv(d.code[i]);
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            R x;
+            if (update_boundaries && bv) {
+                x = d.nv[v][i];
+                cur.f[v][i] = x;
+            } else {
+                x = cur.f[v][i];
+            }
+            if (bv) next.f[v][i] = x;
+            ta.f[v][i] = x;
+            tb.f[v][i] = x;
+        }
+    }
+}
+
+// dest = (dest + src) / 2 where type == IN (TimeLayer3D.h:415-436).
+template <typename R>
+__global__ void merge_kernel(DomainView<R> d, CLayer<R> src, Layer<R> dest)
+{
+    for (long long i = gtid(); i < d.n; i += gstride()) {
+        if (code_is_in(d.code[i])) {
+#pragma unroll
+            for (int v = 0; v < 4; v++) dest.f[v][i] = (dest.f[v][i] + src.f[v][i]) / R(2);
+        }
+    }
+}
+
+// TimeLayer3D::EvalDivError (TimeLayer3D.h:595-641).  The eight-corner sums are
+// formed in the working precision, in the reference's operand order, then scaled
+// and accumulated in double.  Per-block partial sums are reduced in a fixed order
+// by a second single-block kernel, so the result is deterministic; it differs from
+// the reference's sequential double sum only by summation order.
+template <typename R>
+__global__ void div_error_partial_kernel(DomainView<R> d, CLayer<R> l, R dx, R dy, R dz, double *psum,
+                                         unsigned long long *pcnt)
+{
+    const int nx = d.nx, ny = d.ny, nz = d.nz;
+    const long long sx = (long long)ny * nz, sy = nz;
+    double acc = 0.0;
+    unsigned long long cnt = 0;
+    const R *U = l.f[0], *V = l.f[1], *W = l.f[2];
+    for (long long id = gtid(); id < d.n; id += gstride()) {
+        int k = (int)(id % nz);
+        long long r = id / nz;
+        int j = (int)(r % ny);
+        int i = (int)(r / ny);
+        if (i >= nx - 1 || j >= ny - 1 || k >= nz - 1) continue;
+        if (!code_is_in(d.code[id])) continue;
+        // E(i,j,k) with the offsets the reference uses; IN nodes never sit on the
+        // frame (solver contract), so i-1, j-1, k-1 >= 0.
+#define E_(A, di, dj, dk) A[id + (di) * sx + (dj) * sy + (dk)]
+        double err_x = (double)((R)((R)((R)((R)((R)((R)((R)(E_(U, 0, 0, 0) + E_(U, 0, -1, 0)) + E_(U, 0, -1, -1)) + E_(U, 0, 0, -1)) -
+                                E_(U, -1, 0, 0)) - E_(U, -1, -1, 0)) - E_(U, -1, -1, -1)) - E_(U, -1, 0, -1)) * dz * dy) / 4.0;
+        double err_y = (double)((R)((R)((R)((R)((R)((R)((R)(E_(V, 0, 0, 0) + E_(V, -1, 0, 0)) + E_(V, -1, 0, -1)) + E_(V, 0, 0, -1)) -
+                                E_(V, 0, -1, 0)) - E_(V, -1, -1, 0)) - E_(V, -1, -1, -1)) - E_(V, 0, -1, -1)) * dx * dz) / 4.0;
+        double err_z = (double)((R)((R)((R)((R)((R)((R)((R)(E_(W, 0, 0, 0) + E_(W, 0, -1, 0)) + E_(W, -1, -1, 0)) + E_(W, -1, 0, 0)) -
+                                E_(W, 0, 0, -1)) - E_(W, 0, -1, -1)) - E_(W, -1, -1, -1)) - E_(W, -1, 0, -1)) * dx * dy) / 4.0;
+#undef E_
+        acc += fabs(err_x + err_y + err_z);
+        cnt++;
+    }
+    __shared__ double s_sum[256];
+    __shared__ unsigned long long s_cnt[256];
+    s_sum[threadIdx.x] = acc;
+    s_cnt[threadIdx.x] = cnt;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            s_sum[threadIdx.x] += s_sum[threadIdx.x + w];
+            s_cnt[threadIdx.x] += s_cnt[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        psum[blockIdx.x] = s_sum[0];
+        pcnt[blockIdx.x] = s_cnt[0];
+    }
+}
+
+__global__ void div_error_final_kernel(const double *psum, const unsigned long long *pcnt, int nblocks,
+                                       double *out_sum, unsigned long long *out_cnt)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double s = 0.0;
+        unsigned long long c = 0;
+        for (int b = 0; b < nblocks; b++) { s += psum[b]; c += pcnt[b]; }
+        *out_sum = s;
+        *out_cnt = c;
+    }
+}
+
+// Solver3D::GetLayer clears OUT cells of the layer to MISSING_VALUE first
+// (Solver3D.cpp:23, TimeLayer3D.h:974-998).
+template <typename R>
+__global__ void fill_missing_kernel(DomainView<R> d, Layer<R> l)
+{
+    for (long long i = gtid(); i < d.n; i += gstride()) {
+        if ((d.code[i] & CODE_TYPE) == NODE_OUT) {
+#pragma unroll
+            for (int v = 0; v < 4; v++) l.f[v][i] = R(99999.0f);
+        }
+    }
+}
+
+template <typename R>
+cudaError_t launch_update_boundaries(const DomainView<R> &d, Layer<R> cur, cudaStream_t s)
+{
+    update_boundaries_kernel<R><<<grid_for(d.n, 256), 256, 0, s>>>(d, cur);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_step_begin(const DomainView<R> &d, Layer<R> cur, Layer<R> next, Layer<R> ta, Layer<R> tb,
+                              bool update_boundaries, cudaStream_t s)
+{
+    step_begin_kernel<R><<<grid_for(d.n, 256), 256, 0, s>>>(d, cur, next, ta, tb, update_boundaries);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_merge(const DomainView<R> &d, CLayer<R> src, Layer<R> dest, cudaStream_t s)
+{
+    merge_kernel<R><<<grid_for(d.n, 256), 256, 0, s>>>(d, src, dest);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_div_error(const DomainView<R> &d, CLayer<R> l, R dx, R dy, R dz, double *partial_sum,
+                             unsigned long long *partial_cnt, int nblocks, double *out_sum,
+                             unsigned long long *out_cnt, cudaStream_t s)
+{
+    div_error_partial_kernel<R><<<nblocks, 256, 0, s>>>(d, l, dx, dy, dz, partial_sum, partial_cnt);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    div_error_final_kernel<<<1, 32, 0, s>>>(partial_sum, partial_cnt, nblocks, out_sum, out_cnt);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_fill_missing(const DomainView<R> &d, Layer<R> l, cudaStream_t s)
+{
+    fill_missing_kernel<R><<<grid_for(d.n, 256), 256, 0, s>>>(d, l);
+    return cudaGetLastError();
+}
+
+#define INST(R)                                                                                                  \
+    template cudaError_t launch_update_boundaries<R>(const DomainView<R> &, Layer<R>, cudaStream_t);            \
+    template cudaError_t launch_step_begin<R>(const DomainView<R> &, Layer<R>, Layer<R>, Layer<R>, Layer<R>,    \
+                                              bool, cudaStream_t);                                                \
+    template cudaError_t launch_merge<R>(const DomainView<R> &, CLayer<R>, Layer<R>, cudaStream_t);             \
+    template cudaError_t launch_div_error<R>(const DomainView<R> &, CLayer<R>, R, R, R, double *,                \
+                                             unsigned long long *, int, double *, unsigned long long *,          \
+                                             cudaStream_t);                                                        \
+    template cudaError_t launch_fill_missing<R>(const DomainView<R> &, Layer<R>, cudaStream_t);
+INST(float)
+INST(double)
+#undef INST
+
+} // namespace adi

@@ -1,0 +1,265 @@
+// Exact segmented tridiagonal sweep: one thread per grid line, four variables.
+//
+// Replaces the reference's per-direction sweep (CPU: AdiSolver3D::SolveDirection,
+// AdiSolver3D.cpp:587-603 -> SolveSegment/BuildMatrix/ApplyBC0/ApplyBC1/
+// SolveTridiagonal/UpdateSegment, :687-852 and Common/Algorithms.h:21-39;
+// GPU twin: solve_segments / solve_tridiagonal, AdiSolver3D.cu:75-495).
+//
+// Every line of the sweep direction is one tridiagonal system that is block
+// diagonal: each segment of the line is a block, nodes outside segments have no
+// row.  A thread walks its line twice in lock step with the 31 other lines of
+// its warp (lanes = neighbouring lines, so each access of a warp is one
+// contiguous row of the grid for X and Y sweeps):
+//   forward:  builds each row (BC row at a segment end node, BuildMatrix row at
+//             an IN node) and runs the Thomas elimination, writing the modified
+//             coefficients c' (one per matrix: velocity, temperature) and d' (one
+//             per variable) to a line-interleaved scratch area;
+//   backward: back-substitutes, writes x to `next` for every segment node and the
+//             nonlinear merge temp_out = (temp_in + x)/2 at IN nodes (twice when
+//             the time step's extra per-iteration merge falls on this sweep,
+//             AdiSolver3D.cpp:347-357).
+// Velocities share one matrix (a, b, c depend only on the advecting component and
+// v_vis), so their c' is computed once; this is the same arithmetic the reference
+// repeats per variable.
+//
+// Exactness: this file is compiled with --fmad=false and spells out every
+// operation in the reference's order (e.g. cur*3/dt, (-w)/(2h) - vis), divisions
+// are IEEE divisions, so the float results equal the reference CPU solver's bit
+// for bit.  A segment's first row never looks at the previous segment
+// (c'0 = c0/b0, d'0 = d0/b0, as Algorithms.h:25-26), and a segment's last row
+// starts the back-substitution (x = d'), so segments stay independent; a node
+// that ends one segment and starts the next carries the later segment's start row,
+// which is the value the reference writes last.  Nodes outside segments are never
+// written.
+//
+// Scratch: 6 values per line position, layout [q][position][line]; a warp's 32
+// lines are adjacent, so scratch traffic is coalesced.
+#include "adi_internal.cuh"
+
+#include <climits>
+
+namespace adi {
+
+template <typename R>
+struct RowKind {
+    enum : int { NONE = 0, START = 1, INTERIOR = 2, END = 3, SHARED = 4 };
+};
+
+// DissFunc along the sweep direction on temp (TimeLayer3D.h:554-588), operand
+// order of the reference for each direction.
+template <typename R, int DIR>
+__device__ __forceinline__ R diss(const CLayer<R> &t, long long off, long long sl, long long so1, long long so2,
+                                  const SweepConst<R> &k)
+{
+    const R *U = t.f[0], *V = t.f[1], *W = t.f[2];
+    if (DIR == 0) {
+        R u_x = (U[off + sl] - U[off - sl]) / k.two_dx;
+        R v_x = (V[off + sl] - V[off - sl]) / k.two_dx;
+        R w_x = (W[off + sl] - W[off - sl]) / k.two_dx;
+        R u_y = (U[off + so1] - U[off - so1]) / k.two_dy;
+        R u_z = (U[off + so2] - U[off - so2]) / k.two_dz;
+        return R(2) * u_x * u_x + v_x * v_x + w_x * w_x + v_x * u_y + w_x * u_z;
+    } else if (DIR == 1) {
+        R u_y = (U[off + sl] - U[off - sl]) / k.two_dy;
+        R v_y = (V[off + sl] - V[off - sl]) / k.two_dy;
+        R w_y = (W[off + sl] - W[off - sl]) / k.two_dy;
+        R v_x = (V[off + so1] - V[off - so1]) / k.two_dx;
+        R v_z = (V[off + so2] - V[off - so2]) / k.two_dz;
+        return u_y * u_y + R(2) * v_y * v_y + w_y * w_y + u_y * v_x + w_y * v_z;
+    } else {
+        R u_z = (U[off + sl] - U[off - sl]) / k.two_dz;
+        R v_z = (V[off + sl] - V[off - sl]) / k.two_dz;
+        R w_z = (W[off + sl] - W[off - sl]) / k.two_dz;
+        R w_x = (W[off + so1] - W[off - so1]) / k.two_dx;
+        R w_y = (W[off + so2] - W[off - so2]) / k.two_dy;
+        return u_z * u_z + v_z * v_z + R(2) * w_z * w_z + u_z * w_x + v_z * w_y;
+    }
+}
+
+__device__ __forceinline__ int row_kind(uint8_t cm, uint8_t c0, uint8_t cp, bool has_m, bool has_p)
+{
+    if (code_is_in(c0)) return 2;
+    bool inm = has_m && code_is_in(cm);
+    bool inp = has_p && code_is_in(cp);
+    if (inm && inp) return 4;
+    if (inp) return 1;
+    if (inm) return 3;
+    return 0;
+}
+
+template <typename R, int DIR>
+__global__ void __launch_bounds__(128) sweep_exact_kernel(DomainView<R> d, LineGeom g, const int *__restrict__ line_lo,
+                                                          const int *__restrict__ line_hi, CLayer<R> cur, CLayer<R> tin,
+                                                          Layer<R> next, Layer<R> tout, R *__restrict__ scratch,
+                                                          SweepConst<R> k, int merges)
+{
+    const int line = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = line < g.nlines;
+    int lo = INT_MAX, hi = -1;
+    if (valid) {
+        int a = line_lo[line], b = line_hi[line];
+        if (a >= 0) { lo = a; hi = b; }
+    }
+    const unsigned full = 0xffffffffu;
+    const int wlo = __reduce_min_sync(full, lo);
+    const int whi = __reduce_max_sync(full, hi);
+    if (!valid || hi < 0) return;  // after the warp-wide reductions
+
+    const long long sl = g.stride;
+    // off-line strides for DissFunc: X -> (y, z), Y -> (x, z), Z -> (x, y)
+    const long long sx = (long long)g.ny * g.nz, sy = g.nz;
+    const long long so1 = DIR == 0 ? sy : sx;
+    const long long so2 = DIR == 2 ? sy : 1;
+    const long long base = line_base(DIR, g, line);
+    const long long qstride = (long long)g.len * g.nlines;  // between scratch quantities
+    R *scr = scratch + line;
+
+    const R *Fd = tin.f[DIR];  // advecting velocity component along the line
+    const R *Tt = tin.f[3];
+    const R three = k.three, dt = k.dt;
+
+    // ---------------- forward elimination ----------------
+    R cpv = R(0), cpt = R(0), dp0 = R(0), dp1 = R(0), dp2 = R(0), dp3 = R(0);
+    for (int p = wlo; p <= whi; p++) {
+        if (p < lo || p > hi) continue;
+        const long long off = base + (long long)p * sl;
+        const uint8_t c0 = d.code[off];
+        const uint8_t cm = p > 0 ? d.code[off - sl] : uint8_t(NODE_OUT);
+        const uint8_t cp = p + 1 < g.len ? d.code[off + sl] : uint8_t(NODE_OUT);
+        const int kind = row_kind(cm, c0, cp, p > 0, p + 1 < g.len);
+        if (kind == 0) continue;
+        R ncv, nct, n0, n1, n2, n3;
+        if (kind == 2) {
+            // BuildMatrix row (AdiSolver3D.cpp:759-797)
+            const R w = Fd[off];
+            const R av = -w / k.two_h - k.vis_v;
+            const R at = -w / k.two_h - k.vis_t;
+            const R cv = w / k.two_h - k.vis_v;
+            const R ct = w / k.two_h - k.vis_t;
+            R dd[4];
+#pragma unroll
+            for (int v = 0; v < 4; v++) dd[v] = cur.f[v][off] * three / dt;
+            dd[DIR] = dd[DIR] - k.v_T * ((Tt[off + sl] - Tt[off - sl]) / k.two_h);
+            dd[3] = dd[3] + k.t_phi * diss<R, DIR>(tin, off, sl, so1, so2, k);
+            // Thomas step (Algorithms.h:30-31)
+            ncv = cv / (k.b_v - av * cpv);
+            nct = ct / (k.b_t - at * cpt);
+            n0 = (dd[0] - dp0 * av) / (k.b_v - av * cpv);
+            n1 = (dd[1] - dp1 * av) / (k.b_v - av * cpv);
+            n2 = (dd[2] - dp2 * av) / (k.b_v - av * cpv);
+            n3 = (dd[3] - dp3 * at) / (k.b_t - at * cpt);
+        } else if (kind == 1 || kind == 4) {
+            // first row of a segment: ApplyBC0 (AdiSolver3D.cpp:804-827), then
+            // c'0 = c0/b0, d'0 = d0/b0 (Algorithms.h:25-26)
+            const bool vf = (c0 & CODE_VEL_FREE) != 0, tf = (c0 & CODE_TEMP_FREE) != 0;
+            const R bv = vf ? R(2) : R(1), cvv = vf ? R(-1) : R(0);
+            const R bt = tf ? R(2) : R(1), ctt = tf ? R(-1) : R(0);
+            const R d0 = vf ? R(0) : d.nv[0][off];
+            const R d1 = vf ? R(0) : d.nv[1][off];
+            const R d2 = vf ? R(0) : d.nv[2][off];
+            const R d3 = tf ? R(0) : d.nv[3][off];
+            ncv = cvv / bv;
+            nct = ctt / bt;
+            n0 = d0 / bv;
+            n1 = d1 / bv;
+            n2 = d2 / bv;
+            n3 = d3 / bt;
+        } else {
+            // last row of a segment: ApplyBC1 (AdiSolver3D.cpp:829-852), c = 0
+            const bool vf = (c0 & CODE_VEL_FREE) != 0, tf = (c0 & CODE_TEMP_FREE) != 0;
+            const R av = vf ? R(-1) : R(0), bv = vf ? R(2) : R(1);
+            const R at = tf ? R(-1) : R(0), bt = tf ? R(2) : R(1);
+            const R d0 = vf ? R(0) : d.nv[0][off];
+            const R d1 = vf ? R(0) : d.nv[1][off];
+            const R d2 = vf ? R(0) : d.nv[2][off];
+            const R d3 = tf ? R(0) : d.nv[3][off];
+            ncv = R(0);
+            nct = R(0);
+            n0 = (d0 - dp0 * av) / (bv - av * cpv);
+            n1 = (d1 - dp1 * av) / (bv - av * cpv);
+            n2 = (d2 - dp2 * av) / (bv - av * cpv);
+            n3 = (d3 - dp3 * at) / (bt - at * cpt);
+        }
+        cpv = ncv; cpt = nct; dp0 = n0; dp1 = n1; dp2 = n2; dp3 = n3;
+        R *s = scr + (long long)p * g.nlines;
+        s[0 * qstride] = ncv;
+        s[1 * qstride] = nct;
+        s[2 * qstride] = n0;
+        s[3 * qstride] = n1;
+        s[4 * qstride] = n2;
+        s[5 * qstride] = n3;
+    }
+
+    // ---------------- back substitution + write-back + merge ----------------
+    R x0 = R(0), x1 = R(0), x2 = R(0), x3 = R(0);
+    for (int p = whi; p >= wlo; p--) {
+        if (p < lo || p > hi) continue;
+        const long long off = base + (long long)p * sl;
+        const uint8_t c0 = d.code[off];
+        const uint8_t cm = p > 0 ? d.code[off - sl] : uint8_t(NODE_OUT);
+        const uint8_t cp = p + 1 < g.len ? d.code[off + sl] : uint8_t(NODE_OUT);
+        const int kind = row_kind(cm, c0, cp, p > 0, p + 1 < g.len);
+        if (kind == 0) continue;
+        const R *s = scr + (long long)p * g.nlines;
+        const R ncv = s[0 * qstride], nct = s[1 * qstride];
+        const R n0 = s[2 * qstride], n1 = s[3 * qstride], n2 = s[4 * qstride], n3 = s[5 * qstride];
+        if (kind == 3) {
+            x0 = n0; x1 = n1; x2 = n2; x3 = n3;          // x[n-1] = d[n-1]
+        } else {
+            x0 = n0 - ncv * x0;                           // x[i] = d[i] - c[i]*x[i+1]
+            x1 = n1 - ncv * x1;
+            x2 = n2 - ncv * x2;
+            x3 = n3 - nct * x3;
+        }
+        next.f[0][off] = x0;
+        next.f[1][off] = x1;
+        next.f[2][off] = x2;
+        next.f[3][off] = x3;
+        if (kind == 2) {
+            // MergeFieldTo: temp = (temp + next) / 2 (TimeLayer3D.h:430), once or twice
+            R m0 = (tin.f[0][off] + x0) / R(2);
+            R m1 = (tin.f[1][off] + x1) / R(2);
+            R m2 = (tin.f[2][off] + x2) / R(2);
+            R m3 = (tin.f[3][off] + x3) / R(2);
+            if (merges == 2) {
+                m0 = (m0 + x0) / R(2);
+                m1 = (m1 + x1) / R(2);
+                m2 = (m2 + x2) / R(2);
+                m3 = (m3 + x3) / R(2);
+            }
+            tout.f[0][off] = m0;
+            tout.f[1][off] = m1;
+            tout.f[2][off] = m2;
+            tout.f[3][off] = m3;
+        }
+    }
+}
+
+template <typename R>
+cudaError_t launch_sweep_exact(int dir, const DomainView<R> &d, const int *line_lo, const int *line_hi,
+                               CLayer<R> cur, CLayer<R> temp_in, Layer<R> next, Layer<R> temp_out,
+                               R *scratch, const SweepConst<R> &k, int merges, cudaStream_t s)
+{
+    LineGeom g = line_geom(dir, d.nx, d.ny, d.nz);
+    const int threads = 128;
+    const int blocks = (g.nlines + threads - 1) / threads;
+    if (dir == 0)
+        sweep_exact_kernel<R, 0><<<blocks, threads, 0, s>>>(d, g, line_lo, line_hi, cur, temp_in, next, temp_out,
+                                                             scratch, k, merges);
+    else if (dir == 1)
+        sweep_exact_kernel<R, 1><<<blocks, threads, 0, s>>>(d, g, line_lo, line_hi, cur, temp_in, next, temp_out,
+                                                             scratch, k, merges);
+    else
+        sweep_exact_kernel<R, 2><<<blocks, threads, 0, s>>>(d, g, line_lo, line_hi, cur, temp_in, next, temp_out,
+                                                             scratch, k, merges);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_sweep_exact<float>(int, const DomainView<float> &, const int *, const int *,
+                                               CLayer<float>, CLayer<float>, Layer<float>, Layer<float>, float *,
+                                               const SweepConst<float> &, int, cudaStream_t);
+template cudaError_t launch_sweep_exact<double>(int, const DomainView<double> &, const int *, const int *,
+                                                CLayer<double>, CLayer<double>, Layer<double>, Layer<double>,
+                                                double *, const SweepConst<double> &, int, cudaStream_t);
+
+} // namespace adi

@@ -1,0 +1,217 @@
+/*
+ * adi_b200.h — C ABI of the B200-native 3D ADI time step.
+ *
+ * This is the drop-in boundary for the reference solver's hot path
+ * (samech-git/cmc-fluid-solver, src/FluidSolver3D).  A C++ host that keeps the
+ * reference's Solver3D surface (Solver3D.h:24-49) calls these functions instead of
+ * the reference's host<->CUDA launchers.  Plain C types only: opaque handle,
+ * host pointers, sizes, status codes.  No exceptions cross this boundary and
+ * nothing here calls exit().
+ *
+ * Conventions
+ *   - Arrays are [i][j][k] with k fastest, i.e. index = (i*dimy + j)*dimz + k,
+ *     the layout of ScalarField3D::elem and Grid3D::GetType
+ *     (TimeLayer3D.h:256-259, Grid3D.cpp:242-245).
+ *   - Node types / BC codes are the reference enums (Common/Geometry.h:31-41):
+ *     NODE_IN=0 NODE_OUT=1 NODE_BOUND=2 NODE_VALVE=3; BC_NOSLIP=0 BC_FREE=1.
+ *   - "field buffers" for get/set are in the handle's precision (float for
+ *     ADI_FP32, double for ADI_FP64), four separate arrays u, v, w, T.
+ *   - Every call is asynchronous on the handle's stream except those that return
+ *     data to the host (get_*, div_error, build_segments statistics), which
+ *     synchronise that stream.
+ *   - A handle is not thread-safe; distinct handles are independent.
+ */
+#ifndef ADI_B200_H
+#define ADI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum adi_status {
+    ADI_OK = 0,
+    ADI_ERR_BAD_ARG = 1,       /* invalid argument or a mask the solver contract rejects */
+    ADI_ERR_CAPACITY = 2,      /* a size beyond a stated maximum */
+    ADI_ERR_NONFINITE = 3,     /* NaN/Inf found in a field after a step */
+    ADI_ERR_NOT_CONVERGED = 4, /* tolerance mode: max global iterations reached */
+    ADI_ERR_CUDA = 5,          /* a CUDA runtime call failed; see adi_last_error_string */
+    ADI_ERR_TIMEOUT = 6,       /* a bounded device-side wait gave up */
+    ADI_ERR_DIVERGENCE = 7,    /* divergence error above 0.01 (the reference throws,
+                                  AdiSolver3D.cpp:371-374); layers are left unswapped */
+    ADI_ERR_STATE = 8,         /* call order: e.g. a step before adi_set_mask */
+    ADI_ERR_NO_DEVICE = 9      /* no CUDA device, or not an sm_100 device */
+} adi_status;
+
+typedef enum adi_precision { ADI_FP32 = 4, ADI_FP64 = 8 } adi_precision;
+
+/* Sweep implementation.
+ * ADI_SOLVER_EXACT: Thomas elimination per segment in the reference's operation
+ *   order (Common/Algorithms.h:21-39) without fused multiply-add; results equal the
+ *   reference CPU solver's bit for bit.
+ * ADI_SOLVER_FAST: chunked elimination with register-resident coefficients; same
+ *   equations, different rounding (within the documented tolerance). */
+typedef enum adi_solver_kind { ADI_SOLVER_EXACT = 0, ADI_SOLVER_FAST = 1 } adi_solver_kind;
+
+typedef enum adi_dir { ADI_X = 0, ADI_Y = 1, ADI_Z = 2 } adi_dir;
+
+typedef struct adi_handle adi_handle;
+
+/* Grid3D geometry: dims and spacing (Grid3D.h:97-98), plus the run precision
+ * (replaces the compile-time FTYPE, Common/Geometry.h:21). */
+typedef struct adi_grid_desc {
+    int dimx, dimy, dimz;
+    double dx, dy, dz;
+    int precision; /* adi_precision */
+} adi_grid_desc;
+
+/* FluidParams (Common/Geometry.h:538-562). */
+typedef struct adi_fluid_params {
+    double v_T, v_vis, t_vis, t_phi;
+} adi_fluid_params;
+
+/* Per-direction segment statistics from adi_build_segments. */
+typedef struct adi_seg_stats {
+    int64_t num_segments[3];   /* per direction X, Y, Z */
+    int64_t num_nodes[3];      /* sum of segment sizes (endpoints included) */
+    int32_t max_size[3];       /* longest segment */
+    int32_t max_per_line[3];   /* most segments on one line */
+    int64_t num_in;            /* NODE_IN cells */
+} adi_seg_stats;
+
+/* ---- parameters -------------------------------------------------------- */
+
+/* FluidParams(Re, Pr, lambda): v_T=1, v_vis=1/Re, t_vis=1/(Re*Pr),
+ * t_phi=(lambda-1)/(lambda*Re).  Replaces Geometry.h:545-552. */
+adi_status adi_fluid_params_normalized(double Re, double Pr, double lambda, adi_fluid_params *out);
+
+/* FluidParams(vis, rho, R, k, cv).  Replaces Geometry.h:554-561. */
+adi_status adi_fluid_params_dimensional(double vis, double rho, double R, double k, double cv,
+                                        adi_fluid_params *out);
+
+/* ---- lifetime ---------------------------------------------------------- */
+
+/* Allocates every device buffer of one domain on the current CUDA device.
+ * Replaces AdiSolver3D::Init (AdiSolver3D.cpp:166-268) for the single-GPU case. */
+adi_status adi_create(const adi_grid_desc *grid, const adi_fluid_params *params, adi_handle **out);
+
+/* Frees all device memory of the handle.  Replaces AdiSolver3D::~AdiSolver3D /
+ * FreeMemory (AdiSolver3D.cpp:103-158). */
+adi_status adi_destroy(adi_handle *h);
+
+/* Binds the handle to a cudaStream_t (NULL = legacy default stream). */
+adi_status adi_set_stream(adi_handle *h, void *cuda_stream);
+
+/* Selects the sweep implementation (adi_solver_kind).  Default ADI_SOLVER_FAST. */
+adi_status adi_set_solver(adi_handle *h, int kind);
+
+/* Message for the last non-OK status of this handle (static storage). */
+const char *adi_last_error_string(const adi_handle *h);
+
+/* ---- grid / mask ------------------------------------------------------- */
+
+/* Uploads the Grid3D node array as SoA: node type, bc_vel, bc_temp and the
+ * node values v.x, v.y, v.z, T (Grid3D.h:73-88).  The values are the boundary
+ * data and also the initial state of every field (TimeLayer3D(grid) ->
+ * CopyFromGrid, TimeLayer3D.h:1077-1090).  Values are rounded to the handle's
+ * precision.  Also checks the solver contract: no IN cell on the outer frame, no
+ * IN cell next to an OUT cell, no BC_FREE cell between two fluid runs; a mask
+ * that breaks it is stored but adi_time_step returns ADI_ERR_BAD_ARG for it. */
+adi_status adi_set_mask(adi_handle *h, const uint8_t *node_type, const uint8_t *bc_vel,
+                        const uint8_t *bc_temp, const double *vx, const double *vy,
+                        const double *vz, const double *T);
+
+/* Builds the per-direction segment lists on the GPU from the mask, once.
+ * Replaces AdiSolver3D::CreateSegments / Grid3D::GenerateListSegments /
+ * GenerateGridBoundaries (AdiSolver3D.cpp:553-562, Grid3D.cpp:47-146).
+ * stats may be NULL. */
+adi_status adi_build_segments(adi_handle *h, adi_seg_stats *stats);
+
+/* Copies one direction's segment list to the host, in Grid3D::GenerateListSegments
+ * order, 7 int32 per segment: posx posy posz endx endy endz size.  If out7 is NULL
+ * only *count is written.  ADI_ERR_CAPACITY if cap < count. */
+adi_status adi_get_segments(adi_handle *h, int dir, int32_t *out7, int64_t cap, int64_t *count);
+
+/* ---- time stepping ----------------------------------------------------- */
+
+/* cur[BOUND|VALVE] = node values.  Replaces AdiSolver3D::UpdateBoundaries
+ * (AdiSolver3D.cpp:286-304; CPU semantics Solver3D.cpp:27-34). */
+adi_status adi_update_boundaries(adi_handle *h);
+
+/* One time step with num_global nonlinear iterations of Z, Y, X sweeps, each
+ * repeated num_local times.  Replaces AdiSolver3D::TimeStep (AdiSolver3D.cpp:306-391)
+ * with the CPU backend's merge schedule.  compute_error != 0 evaluates the
+ * divergence error of the result on the GPU; a value above 0.01 (the last one
+ * evaluated, as in the reference) returns ADI_ERR_DIVERGENCE. */
+adi_status adi_time_step(adi_handle *h, double dt, int num_global, int num_local, int compute_error);
+
+/* adi_update_boundaries + adi_time_step: one pass of the reference driver loop
+ * (FluidSolver3D.cpp:241-242). */
+adi_status adi_step(adi_handle *h, double dt, int num_global, int num_local, int compute_error);
+
+/* Runs n_steps driver-loop passes (adi_step) as one CUDA graph launch per step
+ * once captured; compute_error every err_every steps (0 = never) and on the last. */
+adi_status adi_run(adi_handle *h, double dt, int num_global, int num_local, int n_steps, int err_every);
+
+/* ---- fields ------------------------------------------------------------ */
+
+/* Layers: 0 = cur (latest state), 1 = next (scratch layer of the last step). */
+adi_status adi_get_state(adi_handle *h, int layer, void *u, void *v, void *w, void *T);
+adi_status adi_set_state(adi_handle *h, const void *u, const void *v, const void *w, const void *T);
+
+/* Solver3D::GetLayer (Solver3D.cpp:21-25 + TimeLayer3D::FilterToArrays,
+ * TimeLayer3D.h:819-924): OUT cells of the layer the reference reads (`next`,
+ * which after a step holds the state the step started from) are set to 99999
+ * (MISSING_VALUE), then the layer is point-sampled onto an outdimx x outdimy x
+ * outdimz grid (0 = full size) at x = i*dimx/outdimx (integer division), etc.
+ * v receives 3 interleaved values per point (Vec3D) in the handle's precision,
+ * T one double per point. */
+adi_status adi_get_layer(adi_handle *h, int outdimx, int outdimy, int outdimz, void *v, double *T);
+
+/* Mean absolute finite-volume divergence of cur over IN cells
+ * (TimeLayer3D::EvalDivError, TimeLayer3D.h:595-641), computed on the GPU. */
+adi_status adi_div_error(adi_handle *h, double *out);
+
+/* ---- profiling ----------------------------------------------------------- */
+
+/* Kernel classes timed by the built-in profiler; the names follow the reference's
+ * Profiler events (AdiSolver3D.cpp:297-301,319-321,592-652). */
+typedef enum adi_kernel_class {
+    ADI_K_STEP_BEGIN = 0,   /* UpdateBoundaries + CopyLayer (fused) */
+    ADI_K_SWEEP_X = 1,      /* SolveSegments_X */
+    ADI_K_SWEEP_Y = 2,      /* SolveSegments_Y */
+    ADI_K_SWEEP_Z = 3,      /* SolveSegments_Z */
+    ADI_K_MERGE = 4,        /* MergeLayer (only when not fused into a sweep) */
+    ADI_K_DIV_ERROR = 5,    /* EvalDivError */
+    ADI_K_OTHER = 6,
+    ADI_K_NUM = 7
+} adi_kernel_class;
+
+typedef struct adi_profile {
+    int64_t launches[ADI_K_NUM];  /* kernel launches since the last reset */
+    double ms[ADI_K_NUM];         /* summed CUDA-event time (profiling on only) */
+    int64_t bytes[ADI_K_NUM];     /* algorithmic HBM bytes of those launches */
+} adi_profile;
+
+/* on != 0: record a CUDA event pair around every kernel launch on the handle's
+ * stream.  Launch counts and algorithmic bytes are always kept. */
+adi_status adi_set_profiling(adi_handle *h, int on);
+
+/* Synchronises the stream, folds pending event pairs into the totals and copies
+ * them out; reset != 0 zeroes the totals afterwards. */
+adi_status adi_get_profile(adi_handle *h, adi_profile *out, int reset);
+
+/* Device pointers of the current layers (zero-copy, for a torch test harness):
+ * cur u, v, w, T then next u, v, w, T. */
+adi_status adi_device_pointers(adi_handle *h, void *out8[8]);
+
+/* Library build/version string. */
+const char *adi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ADI_B200_H */

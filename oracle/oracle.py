@@ -1,0 +1,198 @@
+"""ctypes front ends for the two CPU oracles.  TEST INFRASTRUCTURE ONLY.
+
+* ``RefSolver``    — the reference's own CPU solver compiled from its sources
+                     (``_ref/libref3d.so``, float as shipped).
+* ``OracleSolver`` — the C restatement (``liboracle_adi.so``) in float or double.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's cpu_baseline leg import
+this module, and only to check or to time the CPU baseline.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_LIB = os.path.join(HERE, "_ref", "libref3d.so")
+ORACLE_LIB = os.path.join(HERE, "liboracle_adi.so")
+
+_u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+
+
+def build(quiet: bool = True) -> None:
+    """Builds liboracle_adi.so and, when the reference checkout is present,
+    _ref/libref3d.so (oracle/Makefile)."""
+    subprocess.run(["make", "-C", HERE, "all"], check=True,
+                   stdout=subprocess.DEVNULL if quiet else None)
+
+
+def have_ref() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+_ref = None
+_orc = None
+
+
+def _load_ref():
+    global _ref
+    if _ref is None:
+        lib = C.CDLL(REF_LIB)
+        lib.ref_create.restype = C.c_void_p
+        lib.ref_create.argtypes = [C.c_int] * 3 + [C.c_double] * 3 + [_u8p] * 3 + [_f32p] * 4
+        lib.ref_segments.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int]
+        lib.ref_solver_init.argtypes = [C.c_void_p, C.c_int] + [C.c_double] * 5
+        lib.ref_fluid_params.argtypes = [C.c_void_p, _f32p]
+        lib.ref_step.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int]
+        lib.ref_get_fields.argtypes = [C.c_void_p, C.c_int] + [_f32p] * 4
+        lib.ref_set_state.argtypes = [C.c_void_p] + [_f32p] * 4
+        lib.ref_div_error.restype = C.c_double
+        lib.ref_div_error.argtypes = [C.c_void_p]
+        lib.ref_destroy.argtypes = [C.c_void_p]
+        _ref = lib
+    return _ref
+
+
+def _load_oracle():
+    global _orc
+    if _orc is None:
+        lib = C.CDLL(ORACLE_LIB)
+        lib.oracle_segments.argtypes = [_u8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int]
+        lib.oracle_create.restype = C.c_void_p
+        lib.oracle_create.argtypes = [C.c_int, C.c_int] + [C.c_int] * 3 + [C.c_double] * 3 + [_u8p] * 3 + [_f64p] * 4
+        lib.oracle_set_params.argtypes = [C.c_void_p] + [C.c_double] * 4
+        lib.oracle_step.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int]
+        lib.oracle_get_fields.argtypes = [C.c_void_p, C.c_int] + [_f64p] * 4
+        lib.oracle_set_state.argtypes = [C.c_void_p] + [_f64p] * 4
+        lib.oracle_div_error.restype = C.c_double
+        lib.oracle_div_error.argtypes = [C.c_void_p]
+        lib.oracle_last_div_error.restype = C.c_double
+        lib.oracle_last_div_error.argtypes = [C.c_void_p]
+        lib.oracle_destroy.argtypes = [C.c_void_p]
+        _orc = lib
+    return _orc
+
+
+def fluid_params_normalized(Re: float, Pr: float, lam: float):
+    """FluidParams(Re, Pr, lambda) in double (Common/Geometry.h:545-552)."""
+    return (1.0, 1.0 / Re, 1.0 / (Re * Pr), (lam - 1.0) / (lam * Re))
+
+
+def oracle_segments(type_arr: np.ndarray, direction: int) -> np.ndarray:
+    lib = _load_oracle()
+    t = np.ascontiguousarray(type_arr, np.uint8)
+    nx, ny, nz = t.shape
+    n = lib.oracle_segments(t, nx, ny, nz, direction, None, 0)
+    out = np.zeros((max(n, 1), 7), np.int32)
+    lib.oracle_segments(t, nx, ny, nz, direction, out.ctypes.data, n)
+    return out[:n]
+
+
+class RefSolver:
+    """The reference AdiSolver3D (CPU backend, float) on a synthetic Grid3D."""
+
+    def __init__(self, d, Re=None, Pr=0.72, lam=1.4, dimensional=None):
+        lib = _load_ref()
+        self.lib = lib
+        self.shape = d.shape
+        t, bv, bt, vx, vy, vz, T = d.arrays()
+        f = [np.ascontiguousarray(a, np.float32) for a in (vx, vy, vz, T)]
+        self.h = lib.ref_create(d.nx, d.ny, d.nz, d.dx, d.dy, d.dz, t, bv, bt, *f)
+        if not self.h:
+            raise RuntimeError("ref_create failed")
+        self._keep = (t, bv, bt, f)
+        self.initialised = False
+        if Re is not None or dimensional is not None:
+            self.init_solver(Re, Pr, lam, dimensional)
+
+    def init_solver(self, Re=None, Pr=0.72, lam=1.4, dimensional=None):
+        if dimensional is not None:
+            rc = self.lib.ref_solver_init(self.h, 1, *dimensional)
+        else:
+            rc = self.lib.ref_solver_init(self.h, 0, Re, Pr, lam, 0.0, 0.0)
+        if rc == -3:
+            raise ValueError("mask has more segments than the reference's fixed lists hold")
+        if rc != 0:
+            raise RuntimeError(f"ref_solver_init failed ({rc})")
+        self.initialised = True
+
+    def segments(self, direction: int) -> np.ndarray:
+        n = self.lib.ref_segments(self.h, direction, None, 0)
+        out = np.zeros((max(n, 1), 7), np.int32)
+        self.lib.ref_segments(self.h, direction, out.ctypes.data, n)
+        return out[:n]
+
+    def step(self, dt, num_global, num_local, compute_error=True) -> int:
+        return self.lib.ref_step(self.h, dt, num_global, num_local, int(compute_error))
+
+    def fields(self, which=0):
+        out = [np.zeros(self.shape, np.float32) for _ in range(4)]
+        self.lib.ref_get_fields(self.h, which, *out)
+        return out
+
+    def set_state(self, u, v, w, T):
+        arrs = [np.ascontiguousarray(a, np.float32) for a in (u, v, w, T)]
+        self.lib.ref_set_state(self.h, *arrs)
+
+    def div_error(self) -> float:
+        return self.lib.ref_div_error(self.h)
+
+    def close(self):
+        if self.h:
+            self.lib.ref_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class OracleSolver:
+    """The C restatement, precision 4 (float) or 8 (double)."""
+
+    def __init__(self, d, precision=8, Re=200.0, Pr=0.72, lam=1.4, params=None, nthreads=0):
+        lib = _load_oracle()
+        self.lib = lib
+        self.shape = d.shape
+        arrs = d.arrays()
+        self.h = lib.oracle_create(precision, nthreads, d.nx, d.ny, d.nz, d.dx, d.dy, d.dz, *arrs)
+        self._keep = arrs
+        p = params if params is not None else fluid_params_normalized(Re, Pr, lam)
+        lib.oracle_set_params(self.h, *p)
+
+    def step(self, dt, num_global, num_local, compute_error=True) -> int:
+        return self.lib.oracle_step(self.h, dt, num_global, num_local, int(compute_error))
+
+    def fields(self, which=0):
+        out = [np.zeros(self.shape, np.float64) for _ in range(4)]
+        self.lib.oracle_get_fields(self.h, which, *out)
+        return out
+
+    def set_state(self, u, v, w, T):
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (u, v, w, T)]
+        self.lib.oracle_set_state(self.h, *arrs)
+
+    def div_error(self) -> float:
+        return self.lib.oracle_div_error(self.h)
+
+    def last_div_error(self) -> float:
+        return self.lib.oracle_last_div_error(self.h)
+
+    def close(self):
+        if self.h:
+            self.lib.oracle_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
