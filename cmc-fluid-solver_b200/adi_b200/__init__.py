@@ -143,6 +143,21 @@ class AdiSolver3D:
         return {name: {"launches": p.launches[c], "ms": p.ms[c], "bytes": p.bytes[c]}
                 for c, name in enumerate(_abi.KERNEL_CLASSES)}
 
+    def fast_shapes(self):
+        """(K, NL, P) of the fast sweep per direction X, Y, Z."""
+        out = []
+        for dr in range(3):
+            K, NL, P = C.c_int(), C.c_int(), C.c_int()
+            self._check(self.lib.adi_get_fast_shape(self.h, dr, C.byref(K), C.byref(NL), C.byref(P)))
+            out.append((K.value, NL.value, P.value))
+        return out
+
+    def set_fast_shape(self, direction: int, K: int, NL: int):
+        self._check(self.lib.adi_set_fast_shape(self.h, direction, K, NL))
+
+    def autotune(self, reps: int = 3):
+        self._check(self.lib.adi_autotune(self.h, reps))
+
     def device_pointers(self):
         arr = (C.c_void_p * 8)()
         self._check(self.lib.adi_device_pointers(self.h, C.byref(arr)))

@@ -27,7 +27,7 @@ EXPORTED = [
     "adi_set_stream", "adi_set_solver", "adi_last_error_string", "adi_set_mask", "adi_build_segments",
     "adi_get_segments", "adi_update_boundaries", "adi_time_step", "adi_step", "adi_run", "adi_get_state",
     "adi_set_state", "adi_get_layer", "adi_div_error", "adi_device_pointers", "adi_version",
-    "adi_set_profiling", "adi_get_profile",
+    "adi_set_profiling", "adi_get_profile", "adi_get_fast_shape", "adi_set_fast_shape", "adi_autotune",
 ]
 
 K_NUM = 7
@@ -89,6 +89,9 @@ def load() -> C.CDLL:
         "adi_div_error": [vp, C.POINTER(d)],
         "adi_device_pointers": [vp, C.POINTER(vp * 8)],
         "adi_set_profiling": [vp, i],
+        "adi_get_fast_shape": [vp, i, C.POINTER(i), C.POINTER(i), C.POINTER(i)],
+        "adi_set_fast_shape": [vp, i, i, i],
+        "adi_autotune": [vp, i],
         "adi_get_profile": [vp, C.POINTER(Profile), i],
     }
     for name, args in sig.items():

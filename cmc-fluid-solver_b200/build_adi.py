@@ -31,6 +31,7 @@ SOURCES = [
     ("segments.cu", []),
     ("layer_ops.cu", ["--fmad=false"]),
     ("sweep_exact.cu", ["--fmad=false"]),
+    ("sweep_fast.cu", []),
 ]
 
 

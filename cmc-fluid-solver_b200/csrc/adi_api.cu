@@ -56,6 +56,8 @@ struct adi_handle {
     double ms[ADI_K_NUM] = {};
     int64_t bytes[ADI_K_NUM] = {};
     long long seg_nodes[3] = {0, 0, 0};
+    FastShape shape[3] = {{4, 8, 0}, {4, 8, 0}, {4, 8, 0}};
+    bool tuned = false;
 
     bool mask_set = false, segs_built = false, contract_ok = false;
     std::string contract_msg;
@@ -131,6 +133,11 @@ SweepConst<R> sweep_const(const adi_handle *h, int dir, R dt)
     k.two_dx = R(2) * dx;
     k.two_dy = R(2) * dy;
     k.two_dz = R(2) * dz;
+    k.three_dt = R(3) / dt;
+    k.inv_two_h = R(1) / k.two_h;
+    k.inv_two_dx = R(1) / k.two_dx;
+    k.inv_two_dy = R(1) / k.two_dy;
+    k.inv_two_dz = R(1) / k.two_dz;
     return k;
 }
 
@@ -248,6 +255,10 @@ adi_status run_sweeps(adi_handle *h, R dt, int num_global, int num_local)
             for (int l = 0; l < num_local; l++) {
                 const int merges = (dir == 0 && l == num_local - 1) ? 2 : 1;
                 CK(timed(h, cls, bytes, [&] {
+                    if (h->solver == ADI_SOLVER_FAST)
+                        return launch_sweep_fast<R>(dir, d, h->d_line_lo[dir], h->d_line_hi[dir],
+                                                    clayer<R>(h, src[q]), clayer<R>(h, h->ta), layer<R>(h, dst[q]),
+                                                    layer<R>(h, h->tb), k, merges, h->shape[dir], h->stream);
                     return launch_sweep_exact<R>(dir, d, h->d_line_lo[dir], h->d_line_hi[dir], clayer<R>(h, src[q]),
                                                  clayer<R>(h, h->ta), layer<R>(h, dst[q]), layer<R>(h, h->tb),
                                                  (R *)h->d_scratch, k, merges, h->stream);
@@ -256,6 +267,63 @@ adi_status run_sweeps(adi_handle *h, R dt, int num_global, int num_local)
             }
         }
     }
+    return ADI_OK;
+}
+
+int line_len(const adi_handle *h, int dir) { return dir == 0 ? h->nx : (dir == 1 ? h->ny : h->nz); }
+
+std::vector<FastShape> shape_candidates(const adi_handle *h, int dir)
+{
+    std::vector<FastShape> out;
+    const int len = line_len(h, dir);
+    for (int K : {4, 8, 12, 16})
+        for (int NL : {1, 2, 4, 8, 16, 32}) {
+            if (dir != 2 && NL < 8) continue;   // X/Y: lanes run along k, keep >= 32-byte runs
+            FastShape s{K, NL, (len + K - 1) / K};
+            if (s.NL * s.P < 64) continue;
+            if (fast_shape_supported(dir, s, len, (int)esize(h))) out.push_back(s);
+        }
+    return out;
+}
+
+// Autotuner: times every candidate shape of the fast sweep on this domain and keeps
+// the fastest per direction.  The timed launches read cur and write only layers
+// that every step rewrites before reading (half and the nonlinear buffers).
+template <typename R>
+adi_status autotune(adi_handle *h, int reps)
+{
+    const DomainView<R> d = view<R>(h);
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    for (int dir = 0; dir < 3; dir++) {
+        const SweepConst<R> k = sweep_const<R>(h, dir, (R)1e-3);
+        float best = 1e30f;
+        FastShape best_s = h->shape[dir];
+        for (const FastShape &s : shape_candidates(h, dir)) {
+            auto go = [&] {
+                return launch_sweep_fast<R>(dir, d, h->d_line_lo[dir], h->d_line_hi[dir], clayer<R>(h, h->cur),
+                                            clayer<R>(h, h->ta), layer<R>(h, h->half), layer<R>(h, h->tb), k, 1, s,
+                                            h->stream);
+            };
+            CK(go());
+            float tmin = 1e30f;
+            for (int r = 0; r < reps; r++) {
+                CK(cudaEventRecord(a, h->stream));
+                CK(go());
+                CK(cudaEventRecord(b, h->stream));
+                CK(cudaEventSynchronize(b));
+                float ms = 0.f;
+                CK(cudaEventElapsedTime(&ms, a, b));
+                tmin = ms < tmin ? ms : tmin;
+            }
+            if (tmin < best) { best = tmin; best_s = s; }
+        }
+        h->shape[dir] = best_s;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    h->tuned = true;
     return ADI_OK;
 }
 
@@ -355,6 +423,11 @@ adi_status adi_create(const adi_grid_desc *g, const adi_fluid_params *p, adi_han
     h->n = (long long)g->dimx * g->dimy * g->dimz;
     h->dx = g->dx; h->dy = g->dy; h->dz = g->dz;
     h->params = *p;
+    for (int d = 0; d < 3; d++) {
+        h->shape[d] = FastShape{4, d == 2 ? 2 : 8, 0};
+        h->shape[d].P = (line_len(h, d) + 3) / 4;
+        if (!fast_shape_supported(d, h->shape[d], line_len(h, d), (int)esize(h))) h->shape[d] = FastShape{16, 8, (line_len(h, d) + 15) / 16};
+    }
     const size_t fb = (size_t)h->n * esize(h);
     auto alloc = [&](void **ptr, size_t bytes) { return cudaMalloc(ptr, bytes); };
     cudaError_t e = alloc((void **)&h->d_code, h->n);
@@ -508,6 +581,36 @@ adi_status adi_build_segments(adi_handle *h, adi_seg_stats *stats)
     }
     h->segs_built = true;
     if (stats) *stats = st;
+    if (h->solver == ADI_SOLVER_FAST && !h->tuned) return adi_autotune(h, 3);
+    return ADI_OK;
+}
+
+adi_status adi_autotune(adi_handle *h, int reps)
+{
+    if (!h || reps < 1) return ADI_ERR_BAD_ARG;
+    if (!h->segs_built) return fail(h, ADI_ERR_STATE, "adi_build_segments has not been called");
+    if (h->prec == ADI_FP64) return autotune<double>(h, reps);
+    return autotune<float>(h, reps);
+}
+
+adi_status adi_get_fast_shape(adi_handle *h, int dir, int *K, int *NL, int *P)
+{
+    if (!h || dir < 0 || dir > 2) return ADI_ERR_BAD_ARG;
+    const FastShape s = h->shape[dir];
+    if (K) *K = s.K;
+    if (NL) *NL = s.NL;
+    if (P) *P = (line_len(h, dir) + s.K - 1) / s.K;
+    return ADI_OK;
+}
+
+adi_status adi_set_fast_shape(adi_handle *h, int dir, int K, int NL)
+{
+    if (!h || dir < 0 || dir > 2 || K <= 0) return ADI_ERR_BAD_ARG;
+    const int len = line_len(h, dir);
+    FastShape s{K, NL, (len + K - 1) / K};
+    if (!fast_shape_supported(dir, s, len, (int)esize(h))) return fail(h, ADI_ERR_BAD_ARG, "unsupported fast-sweep shape");
+    h->shape[dir] = s;
+    h->tuned = true;
     return ADI_OK;
 }
 

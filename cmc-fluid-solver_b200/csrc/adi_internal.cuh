@@ -72,6 +72,16 @@ struct SweepConst {
     R b_v, b_t;      // 3/dt + 2*vis
     R v_T, t_phi;
     R two_dx, two_dy, two_dz;
+    // reciprocal forms used by the fast sweep (multiply instead of divide)
+    R three_dt;                          // 3/dt
+    R inv_two_h;                         // 1/(2h) along the line
+    R inv_two_dx, inv_two_dy, inv_two_dz;
+};
+
+// Launch shape of the fast sweep: NL lines per CTA, chunks of K rows per thread,
+// P chunks per line (P*K >= line length).
+struct FastShape {
+    int K, NL, P;
 };
 
 // Device-side description of one domain, passed by value to kernels.
@@ -102,6 +112,13 @@ template <typename R>
 cudaError_t launch_sweep_exact(int dir, const DomainView<R> &d, const int *line_lo, const int *line_hi,
                                CLayer<R> cur, CLayer<R> temp_in, Layer<R> next, Layer<R> temp_out,
                                R *scratch, const SweepConst<R> &k, int merges, cudaStream_t s);
+
+template <typename R>
+cudaError_t launch_sweep_fast(int dir, const DomainView<R> &d, const int *line_lo, const int *line_hi,
+                              CLayer<R> cur, CLayer<R> temp_in, Layer<R> next, Layer<R> temp_out,
+                              const SweepConst<R> &k, int merges, FastShape shape, cudaStream_t s);
+// Shapes the fast sweep is compiled for (K values); returns false if `shape` is not one.
+bool fast_shape_supported(int dir, FastShape shape, int len, int elem_bytes);
 
 cudaError_t launch_segment_scan(int dir, int nx, int ny, int nz, const uint8_t *code, int *line_count,
                                 int *line_lo, int *line_hi, int *line_maxlen, long long *line_nodes,

@@ -174,6 +174,21 @@ adi_status adi_get_layer(adi_handle *h, int outdimx, int outdimy, int outdimz, v
  * (TimeLayer3D::EvalDivError, TimeLayer3D.h:595-641), computed on the GPU. */
 adi_status adi_div_error(adi_handle *h, double *out);
 
+/* ---- fast-sweep launch shapes (autotuner) -------------------------------- */
+
+/* Launch shape of the fast sweep for one direction: each thread owns K
+ * consecutive rows of a line, a CTA holds NL lines, P = ceil(len/K) chunks per
+ * line.  adi_build_segments times the candidate shapes on the domain (the
+ * autotuner) and keeps the fastest per direction; these calls read or override
+ * the choice.  adi_set_fast_shape returns ADI_ERR_BAD_ARG for a shape the kernel
+ * is not compiled for (K in {4, 8, 12, 16}, 32 <= NL*P <= 256). */
+adi_status adi_get_fast_shape(adi_handle *h, int dir, int *K, int *NL, int *P);
+adi_status adi_set_fast_shape(adi_handle *h, int dir, int K, int NL);
+
+/* Re-runs the autotuner for all three directions (reps timed launches per
+ * candidate); also called by adi_build_segments when the solver is ADI_SOLVER_FAST. */
+adi_status adi_autotune(adi_handle *h, int reps);
+
 /* ---- profiling ----------------------------------------------------------- */
 
 /* Kernel classes timed by the built-in profiler; the names follow the reference's

@@ -1,0 +1,118 @@
+"""GPU checks of the fast (chunked) sweep against the oracle.
+
+Tolerances: the fast sweep solves the same equations with a different elimination
+order, so it is compared (a) in double against the double oracle at 1e-11 of each
+field's scale, and (b) in float against the double oracle, where its error must
+stay within the reference's own float drift (the float oracle equals the reference
+bit for bit) and below 1e-5 of the flow scale.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from adi_b200 import geometry as G
+from golden_util import fluid_params_tuple, non_out
+
+pytestmark = pytest.mark.gpu
+
+
+def solver(adi_lib, d, params, precision=None, shapes=None):
+    from adi_b200 import _abi
+    fp = adi_lib.fluid_params_normalized(*params)
+    s = adi_lib.AdiSolver3D(d, params=fp, precision=precision or _abi.ADI_FP32, solver=_abi.ADI_SOLVER_FAST)
+    s.CreateSegments()
+    if shapes:
+        for dr, (K, NL) in enumerate(shapes):
+            s.set_fast_shape(dr, K, NL)
+    return s
+
+
+def rel_errors(got, want, m):
+    vs = max(np.max(np.abs(want[f][m])) for f in range(3))
+    out = []
+    for f in range(4):
+        scale = vs if f < 3 else np.max(np.abs(want[3][m]))
+        out.append(float(np.max(np.abs(got[f][m].astype(np.float64) - want[f][m])) / scale))
+    return out
+
+
+# (K, NL) per direction for a 34 x 30 x 40 domain; 32 <= NL * ceil(len/K) <= 256
+SHAPES = [
+    [(4, 8), (4, 8), (4, 4)],
+    [(8, 16), (8, 8), (8, 8)],
+    [(12, 16), (12, 16), (12, 8)],
+    [(16, 32), (16, 16), (16, 16)],
+    [(8, 8), (16, 16), (4, 4)],
+]
+
+
+@pytest.mark.parametrize("shapes", SHAPES, ids=lambda s: "-".join(f"K{k}NL{n}" for k, n in s))
+def test_fast_fp64_matches_oracle(adi_lib, shapes):
+    from adi_b200 import _abi
+    d = G.random_domain(34, 30, 40, seed=51, shell=True, n_obstacles=9, rmax=5.0)
+    params = (120.0, 0.72, 1.4)
+    s = solver(adi_lib, d, params, precision=_abi.ADI_FP64, shapes=shapes)
+    orc = O.OracleSolver(d, precision=8, params=fluid_params_tuple(("normalized", params)))
+    m = non_out(d)
+    for _ in range(3):
+        assert s.step(8e-4, 4, 2, True) == 0
+        assert orc.step(8e-4, 4, 2, True) == 0
+    errs = rel_errors(s.fields(0), orc.fields(0), m)
+    assert max(errs) < 1e-11, errs
+    # next layer (boundary writes of the last step) as well
+    errs_n = rel_errors(s.fields(1), orc.fields(1), m)
+    assert max(errs_n) < 1e-11, errs_n
+
+
+@pytest.mark.parametrize("shapes", [[(4, 8), (4, 8), (4, 4)], [(8, 16), (8, 8), (8, 8)], [(12, 16), (12, 16), (12, 8)]],
+                         ids=lambda s: "-".join(f"K{k}NL{n}" for k, n in s))
+def test_fast_fp32_within_reference_drift(adi_lib, shapes):
+    d = G.spheres_channel(dims=(48, 40, 44), n_spheres=5, rmin=3, rmax=6, seed=7).round_values_to_float32()
+    params = (200.0, 0.72, 1.4)
+    s = solver(adi_lib, d, params, shapes=shapes)
+    o32 = O.OracleSolver(d, precision=4, params=fluid_params_tuple(("normalized", params)))
+    o64 = O.OracleSolver(d, precision=8, params=fluid_params_tuple(("normalized", params)))
+    for _ in range(10):
+        assert s.step(5e-4, 4, 2, False) == 0
+        o32.step(5e-4, 4, 2, False)
+        o64.step(5e-4, 4, 2, False)
+    m = non_out(d)
+    e_gpu = rel_errors(s.fields(0), o64.fields(0), m)
+    e_ref = rel_errors(o32.fields(0), o64.fields(0), m)
+    for f in range(4):
+        assert e_gpu[f] <= 1e-5, (f, e_gpu, e_ref)
+        assert e_gpu[f] <= 2.0 * e_ref[f] + 2e-7, (f, e_gpu, e_ref)
+
+
+def test_autotuner_picks_supported_shapes(adi_lib):
+    from adi_b200 import _abi
+    d = G.spheres_channel(dims=(64, 48, 80), n_spheres=8, rmin=3, rmax=7, seed=3)
+    s = solver(adi_lib, d, (200.0, 0.72, 1.4))
+    shapes = s.fast_shapes()
+    for dr, (K, NL, P) in enumerate(shapes):
+        assert K in (4, 8, 12, 16)
+        assert P * K >= d.shape[dr]
+        assert 32 <= NL * P <= 256
+    with pytest.raises(_abi.AdiError):
+        s.set_fast_shape(0, 5, 8)
+    with pytest.raises(_abi.AdiError):
+        s.set_fast_shape(2, 4, 64)   # 64 lines x 20 chunks > 256 threads
+    s.autotune(2)
+    assert s.step(5e-4, 2, 1, True) == 0
+
+
+def test_fast_matches_exact_closely(adi_lib):
+    """Fast and exact sweeps agree to float rounding after a few steps."""
+    from adi_b200 import _abi
+    d = G.random_domain(24, 22, 26, seed=61, n_obstacles=6, rmax=4.0)
+    fp = adi_lib.fluid_params_normalized(150.0, 0.72, 1.4)
+    a = adi_lib.AdiSolver3D(d, params=fp, solver=_abi.ADI_SOLVER_FAST)
+    b = adi_lib.AdiSolver3D(d, params=fp, solver=_abi.ADI_SOLVER_EXACT)
+    a.CreateSegments()
+    b.CreateSegments()
+    for _ in range(3):
+        assert a.step(1e-3, 4, 2, True) == 0
+        assert b.step(1e-3, 4, 2, True) == 0
+    m = non_out(d)
+    errs = rel_errors(a.fields(0), [x.astype(np.float64) for x in b.fields(0)], m)
+    assert max(errs) < 2e-6, errs
