@@ -32,6 +32,8 @@ SOURCES = [
     ("layer_ops.cu", ["--fmad=false"]),
     ("sweep_exact.cu", ["--fmad=false"]),
     ("sweep_fast.cu", []),
+    ("sweep_zwarp.cu", []),
+    ("sweep_xytma.cu", []),
 ]
 
 

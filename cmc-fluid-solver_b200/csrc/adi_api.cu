@@ -41,6 +41,7 @@ struct adi_handle {
     void *d_scratch = nullptr;
     size_t scratch_bytes = 0;
 
+    int *d_err = nullptr;   // raised by a device-side bounded wait that gave up
     double *d_psum = nullptr, *d_sum = nullptr;
     unsigned long long *d_pcnt = nullptr, *d_cnt = nullptr;
 
@@ -205,6 +206,7 @@ void free_all(adi_handle *h)
         cudaFree(h->d_segs[d]);
     }
     cudaFree(h->d_scratch);
+    cudaFree(h->d_err);
     cudaFree(h->d_psum);
     cudaFree(h->d_pcnt);
     cudaFree(h->d_sum);
@@ -237,6 +239,31 @@ std::string check_contract(const adi_handle *h, const uint8_t *t, const uint8_t 
     return "";
 }
 
+int line_len(const adi_handle *h, int dir) { return dir == 0 ? h->nx : (dir == 1 ? h->ny : h->nz); }
+
+bool shape_ok(const adi_handle *h, int dir, const FastShape &s)
+{
+    if (s.mode == 1) return dir == 2 && zwarp_supported(h->nz, s.K, (int)esize(h));
+    if (s.mode == 2) return dir < 2 && xytma_supported(dir, h->nx, h->ny, h->nz, s.K, (int)esize(h));
+    return s.mode == 0 && fast_shape_supported(dir, s, line_len(h, dir), (int)esize(h));
+}
+
+// Dispatch of the fast sweep to the kernel variant named by the shape.
+template <typename R>
+cudaError_t launch_fast(adi_handle *h, int dir, CLayer<R> cur, CLayer<R> tin, Layer<R> next, Layer<R> tout,
+                        const SweepConst<R> &k, int merges, const FastShape &s)
+{
+    const DomainView<R> d = view<R>(h);
+    if (s.mode == 1)
+        return launch_sweep_zwarp<R>(d, h->d_line_lo[2], h->d_line_hi[2], cur, tin, next, tout, k, merges, s.K,
+                                     h->stream);
+    if (s.mode == 2)
+        return launch_sweep_xytma<R>(dir, d, h->d_line_lo[dir], cur, tin, next, tout, k, merges, s.K, h->d_err,
+                                     h->stream);
+    return launch_sweep_fast<R>(dir, d, h->d_line_lo[dir], h->d_line_hi[dir], cur, tin, next, tout, k, merges, s,
+                                h->stream);
+}
+
 template <typename R>
 adi_status run_sweeps(adi_handle *h, R dt, int num_global, int num_local)
 {
@@ -256,9 +283,8 @@ adi_status run_sweeps(adi_handle *h, R dt, int num_global, int num_local)
                 const int merges = (dir == 0 && l == num_local - 1) ? 2 : 1;
                 CK(timed(h, cls, bytes, [&] {
                     if (h->solver == ADI_SOLVER_FAST)
-                        return launch_sweep_fast<R>(dir, d, h->d_line_lo[dir], h->d_line_hi[dir],
-                                                    clayer<R>(h, src[q]), clayer<R>(h, h->ta), layer<R>(h, dst[q]),
-                                                    layer<R>(h, h->tb), k, merges, h->shape[dir], h->stream);
+                        return launch_fast<R>(h, dir, clayer<R>(h, src[q]), clayer<R>(h, h->ta), layer<R>(h, dst[q]),
+                                              layer<R>(h, h->tb), k, merges, h->shape[dir]);
                     return launch_sweep_exact<R>(dir, d, h->d_line_lo[dir], h->d_line_hi[dir], clayer<R>(h, src[q]),
                                                  clayer<R>(h, h->ta), layer<R>(h, dst[q]), layer<R>(h, h->tb),
                                                  (R *)h->d_scratch, k, merges, h->stream);
@@ -270,18 +296,26 @@ adi_status run_sweeps(adi_handle *h, R dt, int num_global, int num_local)
     return ADI_OK;
 }
 
-int line_len(const adi_handle *h, int dir) { return dir == 0 ? h->nx : (dir == 1 ? h->ny : h->nz); }
-
 std::vector<FastShape> shape_candidates(const adi_handle *h, int dir)
 {
     std::vector<FastShape> out;
     const int len = line_len(h, dir);
+    if (dir == 2)
+        for (int K : {4, 8}) {
+            FastShape s{K, 0, len / K, 1};
+            if (shape_ok(h, dir, s)) out.push_back(s);
+        }
+    else
+        for (int K : {8, 16}) {
+            FastShape s{K, 16, len / K, 2};
+            if (shape_ok(h, dir, s)) out.push_back(s);
+        }
     for (int K : {4, 8, 12, 16})
         for (int NL : {1, 2, 4, 8, 16, 32}) {
             if (dir != 2 && NL < 8) continue;   // X/Y: lanes run along k, keep >= 32-byte runs
-            FastShape s{K, NL, (len + K - 1) / K};
+            FastShape s{K, NL, (len + K - 1) / K, 0};
             if (s.NL * s.P < 64) continue;
-            if (fast_shape_supported(dir, s, len, (int)esize(h))) out.push_back(s);
+            if (shape_ok(h, dir, s)) out.push_back(s);
         }
     return out;
 }
@@ -292,7 +326,6 @@ std::vector<FastShape> shape_candidates(const adi_handle *h, int dir)
 template <typename R>
 adi_status autotune(adi_handle *h, int reps)
 {
-    const DomainView<R> d = view<R>(h);
     cudaEvent_t a, b;
     CK(cudaEventCreate(&a));
     CK(cudaEventCreate(&b));
@@ -302,9 +335,8 @@ adi_status autotune(adi_handle *h, int reps)
         FastShape best_s = h->shape[dir];
         for (const FastShape &s : shape_candidates(h, dir)) {
             auto go = [&] {
-                return launch_sweep_fast<R>(dir, d, h->d_line_lo[dir], h->d_line_hi[dir], clayer<R>(h, h->cur),
-                                            clayer<R>(h, h->ta), layer<R>(h, h->half), layer<R>(h, h->tb), k, 1, s,
-                                            h->stream);
+                return launch_fast<R>(h, dir, clayer<R>(h, h->cur), clayer<R>(h, h->ta), layer<R>(h, h->half),
+                                      layer<R>(h, h->tb), k, 1, s);
             };
             CK(go());
             float tmin = 1e30f;
@@ -327,6 +359,20 @@ adi_status autotune(adi_handle *h, int reps)
     return ADI_OK;
 }
 
+// Reads and clears the device error flag (the stream must be synchronised by the
+// caller's copy); ADI_ERR_TIMEOUT if a kernel's bounded wait gave up.
+adi_status check_device_flag(adi_handle *h)
+{
+    int flag = 0;
+    CK(cudaMemcpyAsync(&flag, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (flag) {
+        CK(cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream));
+        return fail(h, ADI_ERR_TIMEOUT, "a sweep's bounded wait for its input tiles gave up");
+    }
+    return ADI_OK;
+}
+
 template <typename R>
 adi_status div_error_of(adi_handle *h, int l, double *out)
 {
@@ -340,7 +386,7 @@ adi_status div_error_of(adi_handle *h, int l, double *out)
     CK(cudaMemcpyAsync(&cnt, h->d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     *out = cnt ? sum / (double)cnt : 0.0;
-    return ADI_OK;
+    return check_device_flag(h);
 }
 
 template <typename R>
@@ -424,9 +470,8 @@ adi_status adi_create(const adi_grid_desc *g, const adi_fluid_params *p, adi_han
     h->dx = g->dx; h->dy = g->dy; h->dz = g->dz;
     h->params = *p;
     for (int d = 0; d < 3; d++) {
-        h->shape[d] = FastShape{4, d == 2 ? 2 : 8, 0};
-        h->shape[d].P = (line_len(h, d) + 3) / 4;
-        if (!fast_shape_supported(d, h->shape[d], line_len(h, d), (int)esize(h))) h->shape[d] = FastShape{16, 8, (line_len(h, d) + 15) / 16};
+        h->shape[d] = FastShape{4, d == 2 ? 2 : 8, (line_len(h, d) + 3) / 4, 0};
+        if (!shape_ok(h, d, h->shape[d])) h->shape[d] = FastShape{16, 8, (line_len(h, d) + 15) / 16, 0};
     }
     const size_t fb = (size_t)h->n * esize(h);
     auto alloc = [&](void **ptr, size_t bytes) { return cudaMalloc(ptr, bytes); };
@@ -441,6 +486,8 @@ adi_status adi_create(const adi_grid_desc *g, const adi_fluid_params *p, adi_han
     }
     h->scratch_bytes = 6 * fb;
     if (e == cudaSuccess) e = alloc(&h->d_scratch, h->scratch_bytes);
+    if (e == cudaSuccess) e = alloc((void **)&h->d_err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(h->d_err, 0, sizeof(int));
     if (e == cudaSuccess) e = alloc((void **)&h->d_psum, sizeof(double) * DIV_BLOCKS);
     if (e == cudaSuccess) e = alloc((void **)&h->d_pcnt, sizeof(unsigned long long) * DIV_BLOCKS);
     if (e == cudaSuccess) e = alloc((void **)&h->d_sum, sizeof(double));
@@ -598,7 +645,7 @@ adi_status adi_get_fast_shape(adi_handle *h, int dir, int *K, int *NL, int *P)
     if (!h || dir < 0 || dir > 2) return ADI_ERR_BAD_ARG;
     const FastShape s = h->shape[dir];
     if (K) *K = s.K;
-    if (NL) *NL = s.NL;
+    if (NL) *NL = s.mode == 1 ? 0 : (s.mode == 2 ? -16 : s.NL);
     if (P) *P = (line_len(h, dir) + s.K - 1) / s.K;
     return ADI_OK;
 }
@@ -607,8 +654,8 @@ adi_status adi_set_fast_shape(adi_handle *h, int dir, int K, int NL)
 {
     if (!h || dir < 0 || dir > 2 || K <= 0) return ADI_ERR_BAD_ARG;
     const int len = line_len(h, dir);
-    FastShape s{K, NL, (len + K - 1) / K};
-    if (!fast_shape_supported(dir, s, len, (int)esize(h))) return fail(h, ADI_ERR_BAD_ARG, "unsupported fast-sweep shape");
+    FastShape s{K, NL < 0 ? -NL : NL, (len + K - 1) / K, NL == 0 ? 1 : (NL < 0 ? 2 : 0)};
+    if (!shape_ok(h, dir, s)) return fail(h, ADI_ERR_BAD_ARG, "unsupported fast-sweep shape");
     h->shape[dir] = s;
     h->tuned = true;
     return ADI_OK;
@@ -680,7 +727,7 @@ adi_status adi_get_state(adi_handle *h, int which, void *u, void *v, void *w, vo
     for (int f = 0; f < 4; f++)
         CK(cudaMemcpyAsync(dst[f], h->d_L[l][f], fb, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    return ADI_OK;
+    return check_device_flag(h);
 }
 
 adi_status adi_set_state(adi_handle *h, const void *u, const void *v, const void *w, const void *T)

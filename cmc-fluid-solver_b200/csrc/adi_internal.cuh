@@ -82,6 +82,8 @@ struct SweepConst {
 // P chunks per line (P*K >= line length).
 struct FastShape {
     int K, NL, P;
+    int mode;   // 0: generic chunked kernel; 1: warp-resident Z lines (sweep_zwarp.cu);
+                // 2: TMA-fed X/Y tiles (sweep_xytma.cu)
 };
 
 // Device-side description of one domain, passed by value to kernels.
@@ -119,6 +121,17 @@ cudaError_t launch_sweep_fast(int dir, const DomainView<R> &d, const int *line_l
                               const SweepConst<R> &k, int merges, FastShape shape, cudaStream_t s);
 // Shapes the fast sweep is compiled for (K values); returns false if `shape` is not one.
 bool fast_shape_supported(int dir, FastShape shape, int len, int elem_bytes);
+
+template <typename R>
+cudaError_t launch_sweep_zwarp(const DomainView<R> &d, const int *line_lo, const int *line_hi, CLayer<R> cur,
+                               CLayer<R> tin, Layer<R> next, Layer<R> tout, const SweepConst<R> &k, int merges,
+                               int K, cudaStream_t s);
+bool zwarp_supported(int nz, int K, int elem_bytes);
+template <typename R>
+cudaError_t launch_sweep_xytma(int dir, const DomainView<R> &d, const int *line_lo, CLayer<R> cur, CLayer<R> tin,
+                               Layer<R> next, Layer<R> tout, const SweepConst<R> &k, int merges, int K,
+                               int *err_flag, cudaStream_t s);
+bool xytma_supported(int dir, int nx, int ny, int nz, int K, int elem_bytes);
 
 cudaError_t launch_segment_scan(int dir, int nx, int ny, int nz, const uint8_t *code, int *line_count,
                                 int *line_lo, int *line_hi, int *line_maxlen, long long *line_nodes,

@@ -482,6 +482,7 @@ __global__ void __launch_bounds__(256)
 
 bool fast_shape_supported(int dir, FastShape s, int len, int elem_bytes)
 {
+    if (s.mode != 0) return false;
     if (s.K != 4 && s.K != 8 && s.K != 12 && s.K != 16) return false;
     if (s.NL < 1 || s.P < 1 || (long long)s.P * s.K < len) return false;
     const int threads = s.NL * s.P;

@@ -1,0 +1,447 @@
+// Z sweep with warp-resident lines.
+//
+// Z lines are contiguous in memory.  A line of L = P*K nodes is held by P
+// consecutive lanes of one warp (P in {4, 8, 16, 32}, 32/P lines per warp), lane
+// `ch` owning rows [ch*K, ch*K + K).  Every global access is a 16-byte vector
+// access: the own rows of cur and temp, the four off-line neighbour lines of the
+// advecting component (x+-1, y+-1), and the stores when a whole chunk is written.
+// The rows just outside a chunk (stencil halo) come from the neighbouring lanes
+// by shuffle, and the reduced system of the line -- one cyclic-reduction step
+// then parallel cyclic reduction over the P chunk-first unknowns -- runs entirely
+// in shuffles, so the kernel uses neither shared memory nor barriers.
+//
+// Rows, increment form, chunk elimination and boundary handling are those of the
+// generic fast sweep (sweep_fast.cu); see the comments there.  Requirements
+// (checked by the launcher): dimz == P*K, K*sizeof(R) a multiple of 16 bytes,
+// 16-byte aligned field arrays.
+#include "adi_internal.cuh"
+
+#include <climits>
+
+namespace adi {
+
+namespace {
+
+enum : int { Z_NONE = 0, Z_START = 1, Z_IN = 2, Z_END = 3, Z_SHARED = 4 };
+
+__device__ __forceinline__ int zkind(bool inm, bool in0, bool inp)
+{
+    if (in0) return Z_IN;
+    if (inm && inp) return Z_SHARED;
+    if (inp) return Z_START;
+    if (inm) return Z_END;
+    return Z_NONE;
+}
+
+template <typename R>
+__device__ __forceinline__ R zrcp(R x)
+{
+    return R(1) / x;
+}
+template <>
+__device__ __forceinline__ float zrcp<float>(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return fmaf(r, fmaf(-x, r, 1.0f), r);   // one Newton-Raphson step for 1/x
+}
+
+template <typename R, int K>
+__device__ __forceinline__ void vload(const R *p, R (&out)[K])
+{
+    if (sizeof(R) == 4) {
+#pragma unroll
+        for (int q = 0; q < K / 4; q++) {
+            const float4 v = __ldg(reinterpret_cast<const float4 *>(p) + q);
+            out[4 * q + 0] = v.x; out[4 * q + 1] = v.y; out[4 * q + 2] = v.z; out[4 * q + 3] = v.w;
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < K / 2; q++) {
+            const double2 v = __ldg(reinterpret_cast<const double2 *>(p) + q);
+            out[2 * q + 0] = v.x; out[2 * q + 1] = v.y;
+        }
+    }
+}
+
+template <typename R, int K>
+__device__ __forceinline__ void vstore(R *p, const R (&in)[K])
+{
+    if (sizeof(R) == 4) {
+#pragma unroll
+        for (int q = 0; q < K / 4; q++)
+            reinterpret_cast<float4 *>(p)[q] = make_float4(in[4 * q], in[4 * q + 1], in[4 * q + 2], in[4 * q + 3]);
+    } else {
+#pragma unroll
+        for (int q = 0; q < K / 2; q++)
+            reinterpret_cast<double2 *>(p)[q] = make_double2(in[2 * q], in[2 * q + 1]);
+    }
+}
+
+// shuffles within the P-lane segment of a line
+template <typename T>
+__device__ __forceinline__ T sh_up(T v, int d, int P) { return __shfl_up_sync(0xffffffffu, v, d, P); }
+template <typename T>
+__device__ __forceinline__ T sh_down(T v, int d, int P) { return __shfl_down_sync(0xffffffffu, v, d, P); }
+
+} // namespace
+
+template <typename R, int K, int P>
+__global__ void __launch_bounds__(128)
+    sweep_zwarp_kernel(DomainView<R> d, int nlines, const int *__restrict__ line_lo, const int *__restrict__ line_hi,
+                       CLayer<R> cur, CLayer<R> tin, Layer<R> next, Layer<R> tout, SweepConst<R> kc, int merges)
+{
+    constexpr int LPW = 32 / P;  // lines per warp
+    const int lane = threadIdx.x & 31;
+    const int ch = lane % P;
+    const int line = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * LPW + lane / P;
+    const int L = P * K;
+    bool has = false;
+    long long base = 0;
+    if (line < nlines) {
+        has = line_lo[line] >= 0;
+        base = (long long)line * L;
+    }
+    // a warp whose lines are all empty or beyond the grid leaves together
+    if (!__any_sync(0xffffffffu, has)) return;
+    const int p0 = ch * K;
+    const long long off0 = base + p0;
+    const long long sx = (long long)d.ny * d.nz, sy = d.nz;
+
+    // ---- loads: own rows, four off-line neighbour chunks, codes ----
+    R tv[4][K], cu[4][K], wxp[K], wxm[K], wyp[K], wym[K];
+    uint8_t cc[K];
+#pragma unroll
+    for (int v = 0; v < 4; v++)
+#pragma unroll
+        for (int i = 0; i < K; i++) { tv[v][i] = R(0); cu[v][i] = R(0); }
+#pragma unroll
+    for (int i = 0; i < K; i++) { wxp[i] = wxm[i] = wyp[i] = wym[i] = R(0); cc[i] = NODE_OUT; }
+    if (has) {
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            vload<R, K>(tin.f[v] + off0, tv[v]);
+            vload<R, K>(cur.f[v] + off0, cu[v]);
+        }
+        const R *W = tin.f[2];
+        vload<R, K>(W + off0 + sx, wxp);
+        vload<R, K>(W + off0 - sx, wxm);
+        vload<R, K>(W + off0 + sy, wyp);
+        vload<R, K>(W + off0 - sy, wym);
+        if (K == 4) {
+            const uint32_t c4 = __ldg(reinterpret_cast<const uint32_t *>(d.code + off0));
+#pragma unroll
+            for (int i = 0; i < K; i++) cc[i] = (c4 >> (8 * i)) & 0xff;
+        } else {
+#pragma unroll
+            for (int q = 0; q < K / 8; q++) {
+                const uint2 c8 = __ldg(reinterpret_cast<const uint2 *>(d.code + off0) + q);
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    cc[8 * q + i] = (c8.x >> (8 * i)) & 0xff;
+                    cc[8 * q + 4 + i] = (c8.y >> (8 * i)) & 0xff;
+                }
+            }
+        }
+    }
+    // halo rows from the neighbouring lanes of the line
+    R hm[4], hp[4], cm_[4], cp_[4];
+    uint8_t ccm, ccp;
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+        hm[v] = sh_up(tv[v][K - 1], 1, P);
+        hp[v] = sh_down(tv[v][0], 1, P);
+        cm_[v] = sh_up(cu[v][K - 1], 1, P);
+        cp_[v] = sh_down(cu[v][0], 1, P);
+    }
+    ccm = (uint8_t)sh_up((int)cc[K - 1], 1, P);
+    ccp = (uint8_t)sh_down((int)cc[0], 1, P);
+    if (ch == 0) { ccm = NODE_OUT; }
+    if (ch == P - 1) { ccp = NODE_OUT; }
+
+    // ---- rows ----
+    bool inr[K + 2];
+    inr[0] = code_is_in(ccm);
+    inr[K + 1] = code_is_in(ccp);
+#pragma unroll
+    for (int i = 0; i < K; i++) inr[i + 1] = code_is_in(cc[i]);
+    int kind[K];
+    R rr[K], dv[4][K];
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        kind[i] = zkind(inr[i], inr[i + 1], inr[i + 2]);
+        rr[i] = R(0);
+        const R tprev[4] = {i > 0 ? tv[0][i - 1] : hm[0], i > 0 ? tv[1][i - 1] : hm[1], i > 0 ? tv[2][i - 1] : hm[2],
+                            i > 0 ? tv[3][i - 1] : hm[3]};
+        const R tnext[4] = {i < K - 1 ? tv[0][i + 1] : hp[0], i < K - 1 ? tv[1][i + 1] : hp[1],
+                            i < K - 1 ? tv[2][i + 1] : hp[2], i < K - 1 ? tv[3][i + 1] : hp[3]};
+        if (kind[i] == Z_IN) {
+            const R r = tv[2][i] * kc.inv_two_h;
+            rr[i] = r;
+#pragma unroll
+            for (int v = 0; v < 4; v++) {
+                const R vis = v < 3 ? kc.vis_v : kc.vis_t;
+                const R cm = inr[i] ? (i > 0 ? cu[v][i - 1] : cm_[v]) : R(0);
+                const R cp = inr[i + 2] ? (i < K - 1 ? cu[v][i + 1] : cp_[v]) : R(0);
+                dv[v][i] = vis * (cm - R(2) * cu[v][i] + cp) - r * (cp - cm);
+            }
+            dv[2][i] -= kc.v_T * ((tnext[3] - tprev[3]) * kc.inv_two_h);
+            const R fa = (tnext[0] - tprev[0]) * kc.inv_two_h;
+            const R fb = (tnext[1] - tprev[1]) * kc.inv_two_h;
+            const R fc = (tnext[2] - tprev[2]) * kc.inv_two_h;
+            const R g1 = (wxp[i] - wxm[i]) * kc.inv_two_dx;
+            const R g2 = (wyp[i] - wym[i]) * kc.inv_two_dy;
+            // DissFuncZ (TimeLayer3D.h:578-588)
+            dv[3][i] += kc.t_phi * (fa * fa + fb * fb + R(2) * fc * fc + fa * g1 + fb * g2);
+        } else if (kind[i] == Z_NONE) {
+#pragma unroll
+            for (int v = 0; v < 4; v++) dv[v][i] = R(0);
+        } else {
+            const bool vf = (cc[i] & CODE_VEL_FREE) != 0, tf = (cc[i] & CODE_TEMP_FREE) != 0;
+            const long long off = off0 + i;
+#pragma unroll
+            for (int v = 0; v < 4; v++) {
+                const R nb = kind[i] == Z_END ? (i > 0 ? cu[v][i - 1] : cm_[v]) : (i < K - 1 ? cu[v][i + 1] : cp_[v]);
+                const bool fr = v < 3 ? vf : tf;
+                dv[v][i] = fr ? nb : __ldg(d.nv[v] + off);
+            }
+        }
+    }
+
+    // ---- chunk elimination (same scheme as sweep_fast.cu) ----
+    R ea[2][K], ec[2][K];
+    R Af[2], Cf[2], Al[2], Cl[2], Df[4], Dl[4];
+#pragma unroll
+    for (int m = 0; m < 2; m++) {
+        const R vis = m == 0 ? kc.vis_v : kc.vis_t;
+        const R bin = m == 0 ? kc.b_v : kc.b_t;
+        R A[K], B[K], C[K];
+#pragma unroll
+        for (int i = 0; i < K; i++) {
+            const int kd = kind[i];
+            const bool fr = m == 0 ? (cc[i] & CODE_VEL_FREE) != 0 : (cc[i] & CODE_TEMP_FREE) != 0;
+            if (kd == Z_IN) { A[i] = -rr[i] - vis; B[i] = bin; C[i] = rr[i] - vis; }
+            else if (kd == Z_NONE) { A[i] = R(0); B[i] = R(1); C[i] = R(0); }
+            else {
+                const bool first = kd != Z_END;
+                B[i] = fr ? R(2) : R(1);
+                A[i] = (!first && fr) ? R(-1) : R(0);
+                C[i] = (first && fr) ? R(-1) : R(0);
+            }
+        }
+        // interior rows 1..K-2 through x_first and x_last
+        {
+            const R r = zrcp<R>(B[1]);
+            ea[m][1] = A[1] * r;
+            ec[m][1] = C[1] * r;
+            if (m == 0) { dv[0][1] *= r; dv[1][1] *= r; dv[2][1] *= r; }
+            else dv[3][1] *= r;
+        }
+#pragma unroll
+        for (int i = 2; i <= K - 2; i++) {
+            const R r = zrcp<R>(B[i] - A[i] * ec[m][i - 1]);
+            if (m == 0) {
+#pragma unroll
+                for (int v = 0; v < 3; v++) dv[v][i] = (dv[v][i] - A[i] * dv[v][i - 1]) * r;
+            } else {
+                dv[3][i] = (dv[3][i] - A[i] * dv[3][i - 1]) * r;
+            }
+            ea[m][i] = -A[i] * ea[m][i - 1] * r;
+            ec[m][i] = C[i] * r;
+        }
+#pragma unroll
+        for (int i = K - 3; i >= 1; i--) {
+            const R ci = ec[m][i];
+            ea[m][i] -= ci * ea[m][i + 1];
+            if (m == 0) {
+#pragma unroll
+                for (int v = 0; v < 3; v++) dv[v][i] -= ci * dv[v][i + 1];
+            } else {
+                dv[3][i] -= ci * dv[3][i + 1];
+            }
+            ec[m][i] = -ci * ec[m][i + 1];
+        }
+        const R rf = zrcp<R>(B[0] - C[0] * ea[m][1]);
+        Af[m] = A[0] * rf;
+        Cf[m] = -C[0] * ec[m][1] * rf;
+        const R rl = zrcp<R>(B[K - 1] - A[K - 1] * ec[m][K - 2]);
+        Al[m] = -A[K - 1] * ea[m][K - 2] * rl;
+        Cl[m] = C[K - 1] * rl;
+        if (m == 0) {
+#pragma unroll
+            for (int v = 0; v < 3; v++) {
+                Df[v] = (dv[v][0] - C[0] * dv[v][1]) * rf;
+                Dl[v] = (dv[v][K - 1] - A[K - 1] * dv[v][K - 2]) * rl;
+            }
+        } else {
+            Df[3] = (dv[3][0] - C[0] * dv[3][1]) * rf;
+            Dl[3] = (dv[3][K - 1] - A[K - 1] * dv[3][K - 2]) * rl;
+        }
+    }
+
+    // ---- reduced system in shuffles ----
+    R ea_[2], ec_[2], ed[4];
+    {
+        // cyclic-reduction step: chunk-last row of the previous lane
+        R pA[2], pC[2], pD[4];
+#pragma unroll
+        for (int m = 0; m < 2; m++) {
+            pA[m] = sh_up(Al[m], 1, P);
+            pC[m] = sh_up(Cl[m], 1, P);
+        }
+#pragma unroll
+        for (int v = 0; v < 4; v++) pD[v] = sh_up(Dl[v], 1, P);
+        if (ch == 0) {
+            pA[0] = pA[1] = pC[0] = pC[1] = R(0);
+            pD[0] = pD[1] = pD[2] = pD[3] = R(0);
+        }
+#pragma unroll
+        for (int m = 0; m < 2; m++) {
+            const R r = zrcp<R>(R(1) - Af[m] * pC[m] - Cf[m] * Al[m]);
+            ea_[m] = -Af[m] * pA[m] * r;
+            ec_[m] = -Cf[m] * Cl[m] * r;
+            if (m == 0) {
+#pragma unroll
+                for (int v = 0; v < 3; v++) ed[v] = (Df[v] - Af[0] * pD[v] - Cf[0] * Dl[v]) * r;
+            } else {
+                ed[3] = (Df[3] - Af[1] * pD[3] - Cf[1] * Dl[3]) * r;
+            }
+        }
+    }
+#pragma unroll
+    for (int s = 1; s < P; s <<= 1) {
+        R mA[2], mC[2], mD[4], pA[2], pC[2], pD[4];
+#pragma unroll
+        for (int m = 0; m < 2; m++) {
+            mA[m] = sh_up(ea_[m], s, P);
+            mC[m] = sh_up(ec_[m], s, P);
+            pA[m] = sh_down(ea_[m], s, P);
+            pC[m] = sh_down(ec_[m], s, P);
+        }
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            mD[v] = sh_up(ed[v], s, P);
+            pD[v] = sh_down(ed[v], s, P);
+        }
+        const bool hasm = ch >= s, hasp = ch + s < P;
+#pragma unroll
+        for (int m = 0; m < 2; m++) {
+            if (!hasm) { mA[m] = R(0); mC[m] = R(0); }
+            if (!hasp) { pA[m] = R(0); pC[m] = R(0); }
+        }
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            if (!hasm) mD[v] = R(0);
+            if (!hasp) pD[v] = R(0);
+        }
+#pragma unroll
+        for (int m = 0; m < 2; m++) {
+            const R a = ea_[m], c = ec_[m];
+            const R r = zrcp<R>(R(1) - a * mC[m] - c * pA[m]);
+            if (m == 0) {
+#pragma unroll
+                for (int v = 0; v < 3; v++) ed[v] = (ed[v] - a * mD[v] - c * pD[v]) * r;
+            } else {
+                ed[3] = (ed[3] - a * mD[3] - c * pD[3]) * r;
+            }
+            ea_[m] = -a * mA[m] * r;
+            ec_[m] = -c * pC[m] * r;
+        }
+    }
+    R xf[4], xl[4];
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+        R nf = sh_down(ed[v], 1, P);
+        if (ch == P - 1) nf = R(0);
+        xf[v] = ed[v];
+        const int m = v < 3 ? 0 : 1;
+        xl[v] = Dl[v] - Al[m] * xf[v] - Cl[m] * nf;
+    }
+    if (!has) return;
+
+    // ---- write-back ----
+    R xo[4][K], mo[4][K];
+    bool all_seg = true, all_in = true;
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        all_seg = all_seg && kind[i] != Z_NONE;
+        all_in = all_in && kind[i] == Z_IN;
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            const int m = v < 3 ? 0 : 1;
+            R x = i == 0 ? xf[v] : (i == K - 1 ? xl[v] : dv[v][i] - ea[m][i] * xf[v] - ec[m][i] * xl[v]);
+            if (kind[i] == Z_IN) x += cu[v][i];
+            xo[v][i] = x;
+            R mm = (tv[v][i] + x) * R(0.5);
+            if (merges == 2) mm = (mm + x) * R(0.5);
+            mo[v][i] = mm;
+        }
+    }
+    if (all_seg) {
+#pragma unroll
+        for (int v = 0; v < 4; v++) vstore<R, K>(next.f[v] + off0, xo[v]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < K; i++)
+            if (kind[i] != Z_NONE) {
+#pragma unroll
+                for (int v = 0; v < 4; v++) next.f[v][off0 + i] = xo[v][i];
+            }
+    }
+    if (all_in) {
+#pragma unroll
+        for (int v = 0; v < 4; v++) vstore<R, K>(tout.f[v] + off0, mo[v]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < K; i++)
+            if (kind[i] == Z_IN) {
+#pragma unroll
+                for (int v = 0; v < 4; v++) tout.f[v][off0 + i] = mo[v][i];
+            }
+    }
+}
+
+bool zwarp_supported(int nz, int K, int elem_bytes)
+{
+    if (K * elem_bytes % 16 != 0) return false;
+    if (nz % K != 0) return false;
+    const int P = nz / K;
+    return P == 4 || P == 8 || P == 16 || P == 32;
+}
+
+template <typename R>
+cudaError_t launch_sweep_zwarp(const DomainView<R> &d, const int *line_lo, const int *line_hi, CLayer<R> cur,
+                               CLayer<R> tin, Layer<R> next, Layer<R> tout, const SweepConst<R> &k, int merges,
+                               int K, cudaStream_t s)
+{
+    if (!zwarp_supported(d.nz, K, (int)sizeof(R))) return cudaErrorInvalidConfiguration;
+    for (int v = 0; v < 4; v++)
+        if (((uintptr_t)cur.f[v] | (uintptr_t)tin.f[v] | (uintptr_t)next.f[v] | (uintptr_t)tout.f[v]) % 16)
+            return cudaErrorInvalidConfiguration;
+    const int nlines = d.nx * d.ny;
+    const int P = d.nz / K;
+    const int lines_per_block = 4 * (32 / P);  // 4 warps per block
+    const int blocks = (nlines + lines_per_block - 1) / lines_per_block;
+#define ZL(KK, PP)                                                                                              \
+    if (K == KK && P == PP) {                                                                                   \
+        sweep_zwarp_kernel<R, KK, PP><<<blocks, 128, 0, s>>>(d, nlines, line_lo, line_hi, cur, tin, next, tout, k, \
+                                                            merges);                                           \
+        return cudaGetLastError();                                                                              \
+    }
+    if (sizeof(R) == 4) {
+        ZL(4, 4) ZL(4, 8) ZL(4, 16) ZL(4, 32) ZL(8, 4) ZL(8, 8) ZL(8, 16) ZL(8, 32)
+    } else {
+        ZL(4, 4) ZL(4, 8) ZL(4, 16) ZL(4, 32) ZL(8, 4) ZL(8, 8) ZL(8, 16) ZL(8, 32)
+    }
+#undef ZL
+    return cudaErrorInvalidConfiguration;
+}
+
+template cudaError_t launch_sweep_zwarp<float>(const DomainView<float> &, const int *, const int *, CLayer<float>,
+                                               CLayer<float>, Layer<float>, Layer<float>, const SweepConst<float> &,
+                                               int, int, cudaStream_t);
+template cudaError_t launch_sweep_zwarp<double>(const DomainView<double> &, const int *, const int *, CLayer<double>,
+                                                CLayer<double>, Layer<double>, Layer<double>,
+                                                const SweepConst<double> &, int, int, cudaStream_t);
+
+} // namespace adi

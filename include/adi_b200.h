@@ -178,10 +178,14 @@ adi_status adi_div_error(adi_handle *h, double *out);
 
 /* Launch shape of the fast sweep for one direction: each thread owns K
  * consecutive rows of a line, a CTA holds NL lines, P = ceil(len/K) chunks per
- * line.  adi_build_segments times the candidate shapes on the domain (the
- * autotuner) and keeps the fastest per direction; these calls read or override
- * the choice.  adi_set_fast_shape returns ADI_ERR_BAD_ARG for a shape the kernel
- * is not compiled for (K in {4, 8, 12, 16}, 32 <= NL*P <= 256). */
+ * line.  NL = 0 selects the warp-resident Z kernel (Z only; dimz = P*K with P in
+ * {4, 8, 16, 32}, K in {4, 8}); NL = -16 selects the TMA-fed X/Y kernel (16 lines
+ * per CTA; dimz a multiple of 16, line length <= 256, even and a multiple of K,
+ * K in {8, 16}).  adi_build_segments times the candidate shapes on
+ * the domain (the autotuner) and keeps the fastest per direction; these calls
+ * read or override the choice.  adi_set_fast_shape returns ADI_ERR_BAD_ARG for a
+ * shape no kernel is compiled for (generic: K in {4, 8, 12, 16},
+ * 32 <= NL*P <= 256). */
 adi_status adi_get_fast_shape(adi_handle *h, int dir, int *K, int *NL, int *P);
 adi_status adi_set_fast_shape(adi_handle *h, int dir, int K, int NL);
 

@@ -116,3 +116,45 @@ def test_fast_matches_exact_closely(adi_lib):
     m = non_out(d)
     errs = rel_errors(a.fields(0), [x.astype(np.float64) for x in b.fields(0)], m)
     assert max(errs) < 2e-6, errs
+
+
+@pytest.mark.parametrize("zK", [4, 8])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_zwarp_kernel(adi_lib, zK, precision):
+    """Warp-resident Z kernel (NL = 0): dimz = P*K with P a power of two <= 32."""
+    from adi_b200 import _abi
+    d = G.random_domain(30, 26, 32, seed=71, shell=True, n_obstacles=7, rmax=4.0)
+    params = (110.0, 0.72, 1.4)
+    prec = _abi.ADI_FP64 if precision == "fp64" else _abi.ADI_FP32
+    s = solver(adi_lib, d, params, precision=prec, shapes=[(8, 8), (8, 8), (zK, 0)])
+    assert s.fast_shapes()[2][1] == 0
+    orc = O.OracleSolver(d, precision=8, params=fluid_params_tuple(("normalized", params)))
+    m = non_out(d)
+    for _ in range(3):
+        assert s.step(8e-4, 4, 2, True) == 0
+        assert orc.step(8e-4, 4, 2, True) == 0
+    errs = rel_errors(s.fields(0), orc.fields(0), m)
+    assert max(errs) < (1e-11 if precision == "fp64" else 2e-6), errs
+    errs_n = rel_errors(s.fields(1), orc.fields(1), m)
+    assert max(errs_n) < (1e-11 if precision == "fp64" else 2e-6), errs_n
+
+
+@pytest.mark.parametrize("xK", [8, 16])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_xytma_kernel(adi_lib, xK, precision):
+    """TMA-fed X/Y kernel (NL = -16): dimz a multiple of 16, lines a multiple of K."""
+    from adi_b200 import _abi
+    d = G.random_domain(48, 40, 32, seed=81, shell=True, n_obstacles=8, rmax=4.5)
+    params = (130.0, 0.72, 1.4)
+    prec = _abi.ADI_FP64 if precision == "fp64" else _abi.ADI_FP32
+    s = solver(adi_lib, d, params, precision=prec, shapes=[(xK, -16), (8, -16), (4, 0)])
+    assert s.fast_shapes()[0][1] == -16 and s.fast_shapes()[1][1] == -16
+    orc = O.OracleSolver(d, precision=8, params=fluid_params_tuple(("normalized", params)))
+    m = non_out(d)
+    for _ in range(3):
+        assert s.step(8e-4, 4, 2, True) == 0
+        assert orc.step(8e-4, 4, 2, True) == 0
+    errs = rel_errors(s.fields(0), orc.fields(0), m)
+    assert max(errs) < (1e-11 if precision == "fp64" else 2e-6), errs
+    errs_n = rel_errors(s.fields(1), orc.fields(1), m)
+    assert max(errs_n) < (1e-11 if precision == "fp64" else 2e-6), errs_n
