@@ -20,6 +20,7 @@
 // The mbarrier wait is bounded: if the tile has not landed after about a second
 // the CTA raises the handle's error flag and leaves without computing.
 #include "adi_internal.cuh"
+#include "sweep_common.cuh"
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -30,30 +31,6 @@
 namespace adi {
 
 namespace {
-
-enum : int { T_NONE = 0, T_START = 1, T_IN = 2, T_END = 3, T_SHARED = 4 };
-
-__device__ __forceinline__ int tkind(bool inm, bool in0, bool inp)
-{
-    if (in0) return T_IN;
-    if (inm && inp) return T_SHARED;
-    if (inp) return T_START;
-    if (inm) return T_END;
-    return T_NONE;
-}
-
-template <typename R>
-__device__ __forceinline__ R trcp(R x)
-{
-    return R(1) / x;
-}
-template <>
-__device__ __forceinline__ float trcp<float>(float x)
-{
-    float r;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return fmaf(r, fmaf(-x, r, 1.0f), r);   // one Newton-Raphson step for 1/x
-}
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
 {
@@ -164,246 +141,157 @@ __global__ void __launch_bounds__(256)
         }
     }
 
-    // ---------------- rows from the tiles ----------------
+    // ---------------- rows from the tiles: one pass, 3-row window ----------------
+    using namespace sweep;
     const int p0 = ch * K;
-    auto TC = [&](int v, int p) -> R { return tcur[(size_t)v * L * NLT + (size_t)p * NLT + li]; };
-    auto TT = [&](int v, int p) -> R {
-        return v == DIR ? twide[(size_t)p * WIDE + li + 4]
-                        : ttin[(size_t)(v < DIR ? v : v - 1) * L * NLT + (size_t)p * NLT + li];
-    };
-    auto CODE = [&](int p) -> uint8_t { return (p >= 0 && p < L) ? tcode[(size_t)p * NLT + li] : uint8_t(NODE_OUT); };
-
+    const int fs = L * NLT;                       // elements between two fields of a tile
+    const R *__restrict__ cT = tcur + li;         // cur tile column of this line
+    const R *__restrict__ tT = ttin + li;         // temp tiles (fields other than DIR)
+    const R *__restrict__ wT = twide + li + 4;    // advecting field column (k halo at -1/+1)
+    const R *__restrict__ hmT = thm + li;
+    const R *__restrict__ hpT = thp + li;
+    const uint8_t *__restrict__ kT = tcode + li;
+    // window slots: 0 = row i-1, 1 = row i, 2 = row i+1.  cur is kept only for IN
+    // rows (the reference vector of the increment form is 0 elsewhere).
+    R cw[3][4], tw[3][4];
+    uint8_t kw[3];
+#define XY_LOAD_ROW(SLOT_, P_)                                                                       \
+    {                                                                                                \
+        const int pp = (P_);                                                                         \
+        const bool ok = has && pp >= 0 && pp < L;                                                    \
+        const uint8_t c = ok ? kT[pp * NLT] : uint8_t(NODE_OUT);                                     \
+        kw[SLOT_] = c;                                                                               \
+        const bool in = code_is_in(c);                                                               \
+        _Pragma("unroll") for (int v = 0; v < 4; v++)                                                \
+        {                                                                                            \
+            tw[SLOT_][v] = ok ? (v == DIR ? wT[pp * WIDE] : tT[(v < DIR ? v : v - 1) * fs + pp * NLT]) : R(0); \
+            cw[SLOT_][v] = in ? cT[v * fs + pp * NLT] : R(0);                                        \
+        }                                                                                            \
+    }
     int kind[K];
     unsigned freebits = 0;
     R rr[K], dv[4][K];
-    bool inr[K + 2];
-    uint8_t cc[K + 2];
-#pragma unroll
-    for (int q = 0; q < K + 2; q++) {
-        cc[q] = has ? CODE(p0 - 1 + q) : uint8_t(NODE_OUT);
-        inr[q] = code_is_in(cc[q]);
-    }
-#pragma unroll
-    for (int i = 0; i < K; i++) {
-        kind[i] = tkind(inr[i], inr[i + 1], inr[i + 2]);
-        if (cc[i + 1] & CODE_VEL_FREE) freebits |= 1u << (2 * i);
-        if (cc[i + 1] & CODE_TEMP_FREE) freebits |= 2u << (2 * i);
-    }
+    XY_LOAD_ROW(0, p0 - 1)
+    XY_LOAD_ROW(1, p0)
+    // global offset of this line's node 0: X (0, j, k) = j*nz + k; Y (i, 0, k) = i*ny*nz + k
+    const long long lb = DIR == 0 ? (long long)outer * g.nz + k0 + li : (long long)outer * g.ny * g.nz + k0 + li;
 #pragma unroll
     for (int i = 0; i < K; i++) {
         const int p = p0 + i;
-        const int kd = kind[i];
+        XY_LOAD_ROW(2, p + 1)
+        const int kd = row_kind(code_is_in(kw[0]), code_is_in(kw[1]), code_is_in(kw[2]));
+        kind[i] = kd;
+        if (kw[1] & CODE_VEL_FREE) freebits |= 1u << (2 * i);
+        if (kw[1] & CODE_TEMP_FREE) freebits |= 2u << (2 * i);
         rr[i] = R(0);
-        if (kd == T_IN) {
+        if (kd == R_IN) {
             // IN rows are never the first or last node of a line
-            const R r = TT(DIR, p) * kc.inv_two_h;
+            const R r = tw[1][DIR] * kc.inv_two_h;
             rr[i] = r;
 #pragma unroll
             for (int v = 0; v < 4; v++) {
                 const R vis = v < 3 ? kc.vis_v : kc.vis_t;
-                const R cm = inr[i] ? TC(v, p - 1) : R(0);
-                const R cp = inr[i + 2] ? TC(v, p + 1) : R(0);
-                dv[v][i] = vis * (cm - R(2) * TC(v, p) + cp) - r * (cp - cm);
+                dv[v][i] = vis * (cw[0][v] - R(2) * cw[1][v] + cw[2][v]) - r * (cw[2][v] - cw[0][v]);
             }
-            dv[DIR][i] -= kc.v_T * ((TT(3, p + 1) - TT(3, p - 1)) * kc.inv_two_h);
-            const R fa = (TT(0, p + 1) - TT(0, p - 1)) * kc.inv_two_h;
-            const R fb = (TT(1, p + 1) - TT(1, p - 1)) * kc.inv_two_h;
-            const R fc = (TT(2, p + 1) - TT(2, p - 1)) * kc.inv_two_h;
-            const R g1 = (thp[(size_t)p * NLT + li] - thm[(size_t)p * NLT + li]) *
-                         (DIR == 0 ? kc.inv_two_dy : kc.inv_two_dx);
-            const R g2 = (twide[(size_t)p * WIDE + li + 5] - twide[(size_t)p * WIDE + li + 3]) * kc.inv_two_dz;
+            dv[DIR][i] -= kc.v_T * ((tw[2][3] - tw[0][3]) * kc.inv_two_h);
+            const R fa = (tw[2][0] - tw[0][0]) * kc.inv_two_h;
+            const R fb = (tw[2][1] - tw[0][1]) * kc.inv_two_h;
+            const R fc = (tw[2][2] - tw[0][2]) * kc.inv_two_h;
+            const R g1 = (hpT[p * NLT] - hmT[p * NLT]) * (DIR == 0 ? kc.inv_two_dy : kc.inv_two_dx);
+            const R g2 = (wT[p * WIDE + 1] - wT[p * WIDE - 1]) * kc.inv_two_dz;
             R diss;
             if (DIR == 0) diss = R(2) * fa * fa + fb * fb + fc * fc + fb * g1 + fc * g2;
             else diss = fa * fa + R(2) * fb * fb + fc * fc + fa * g1 + fc * g2;
             dv[3][i] += kc.t_phi * diss;
-        } else if (kd == T_NONE) {
+        } else if (kd == R_NONE) {
 #pragma unroll
             for (int v = 0; v < 4; v++) dv[v][i] = R(0);
         } else {
-            const bool vf = (freebits >> (2 * i)) & 1u, tf = (freebits >> (2 * i + 1)) & 1u;
-            const int pn = kd == T_END ? p - 1 : p + 1;   // the IN neighbour
-            const long long off = line_base(DIR, g, line) + (long long)p * g.stride;
+            // boundary row; BC_FREE moves the IN neighbour's cur to the right side
+            const bool vf = (kw[1] & CODE_VEL_FREE) != 0, tf = (kw[1] & CODE_TEMP_FREE) != 0;
+            const int nb = kd == R_END ? 0 : 2;
+            const long long off = lb + (long long)p * g.stride;
 #pragma unroll
             for (int v = 0; v < 4; v++) {
                 const bool fr = v < 3 ? vf : tf;
-                dv[v][i] = fr ? TC(v, pn) : __ldg(d.nv[v] + off);
+                dv[v][i] = fr ? cw[nb][v] : __ldg(d.nv[v] + off);
             }
         }
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            cw[0][v] = cw[1][v]; cw[1][v] = cw[2][v];
+            tw[0][v] = tw[1][v]; tw[1][v] = tw[2][v];
+        }
+        kw[0] = kw[1];
+        kw[1] = kw[2];
     }
+#undef XY_LOAD_ROW
 
     // ---------------- chunk elimination ----------------
     R ea[2][K], ec[2][K];
-    R Af[2], Cf[2], Al[2], Cl[2], Df[4], Dl[4];
-#pragma unroll
-    for (int m = 0; m < 2; m++) {
-        const R vis = m == 0 ? kc.vis_v : kc.vis_t;
-        const R bin = m == 0 ? kc.b_v : kc.b_t;
-        R A[K], B[K], C[K];
-#pragma unroll
-        for (int i = 0; i < K; i++) {
-            const int kd = kind[i];
-            const bool fr = (freebits >> (2 * i + m)) & 1u;
-            if (kd == T_IN) { A[i] = -rr[i] - vis; B[i] = bin; C[i] = rr[i] - vis; }
-            else if (kd == T_NONE) { A[i] = R(0); B[i] = R(1); C[i] = R(0); }
-            else {
-                const bool first = kd != T_END;
-                B[i] = fr ? R(2) : R(1);
-                A[i] = (!first && fr) ? R(-1) : R(0);
-                C[i] = (first && fr) ? R(-1) : R(0);
-            }
-        }
-        {
-            const R r = trcp<R>(B[1]);
-            ea[m][1] = A[1] * r;
-            ec[m][1] = C[1] * r;
-            if (m == 0) { dv[0][1] *= r; dv[1][1] *= r; dv[2][1] *= r; }
-            else dv[3][1] *= r;
-        }
-#pragma unroll
-        for (int i = 2; i <= K - 2; i++) {
-            const R r = trcp<R>(B[i] - A[i] * ec[m][i - 1]);
-            if (m == 0) {
-#pragma unroll
-                for (int v = 0; v < 3; v++) dv[v][i] = (dv[v][i] - A[i] * dv[v][i - 1]) * r;
-            } else {
-                dv[3][i] = (dv[3][i] - A[i] * dv[3][i - 1]) * r;
-            }
-            ea[m][i] = -A[i] * ea[m][i - 1] * r;
-            ec[m][i] = C[i] * r;
-        }
-#pragma unroll
-        for (int i = K - 3; i >= 1; i--) {
-            const R ci = ec[m][i];
-            ea[m][i] -= ci * ea[m][i + 1];
-            if (m == 0) {
-#pragma unroll
-                for (int v = 0; v < 3; v++) dv[v][i] -= ci * dv[v][i + 1];
-            } else {
-                dv[3][i] -= ci * dv[3][i + 1];
-            }
-            ec[m][i] = -ci * ec[m][i + 1];
-        }
-        const R rf = trcp<R>(B[0] - C[0] * ea[m][1]);
-        Af[m] = A[0] * rf;
-        Cf[m] = -C[0] * ec[m][1] * rf;
-        const R rl = trcp<R>(B[K - 1] - A[K - 1] * ec[m][K - 2]);
-        Al[m] = -A[K - 1] * ea[m][K - 2] * rl;
-        Cl[m] = C[K - 1] * rl;
-        if (m == 0) {
-#pragma unroll
-            for (int v = 0; v < 3; v++) {
-                Df[v] = (dv[v][0] - C[0] * dv[v][1]) * rf;
-                Dl[v] = (dv[v][K - 1] - A[K - 1] * dv[v][K - 2]) * rl;
-            }
-        } else {
-            Df[3] = (dv[3][0] - C[0] * dv[3][1]) * rf;
-            Dl[3] = (dv[3][K - 1] - A[K - 1] * dv[3][K - 2]) * rl;
-        }
-    }
+    Reduced<R> red;
+    eliminate<R, K>(kind, rr, freebits, kc, dv, ea, ec, red);
 
-    // ---------------- reduced system: one CR step + PCR, 8-value slots ----------------
-    auto SLOT = [&](R *b, int c) -> R * { return b + ((size_t)c * NLT + li) * 8; };
-    {
-        R *w = SLOT(buf0, ch);
-        w[0] = Al[0]; w[1] = Cl[0]; w[2] = Al[1]; w[3] = Cl[1];
-        w[4] = Dl[0]; w[5] = Dl[1]; w[6] = Dl[2]; w[7] = Dl[3];
-    }
+    // ---------------- reduced system: one CR step + PCR through shared slots ----------------
+    // Couplings to rows outside the line are exactly zero (the first row of a line
+    // has a = 0, the last c = 0, and PCR keeps them zero), so a thread whose partner
+    // row would lie outside reads its own slot instead: finite values times 0.
+    R *const s0 = buf0 + li * 8, *const s1 = buf1 + li * 8;
+    const int cs = NLT * 8;   // elements between the slots of two chunks
+    slot_store<R>(s0 + ch * cs, red.Al[0], red.Cl[0], red.Al[1], red.Cl[1], red.Dl[0], red.Dl[1], red.Dl[2],
+                  red.Dl[3]);
     __syncthreads();
     R ea_[2], ec_[2], ed[4];
     {
-        R pv[8] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};
-        if (ch > 0) {
-            const R *r = SLOT(buf0, ch - 1);
+        R pv[8];
+        slot_load<R>(s0 + (ch > 0 ? ch - 1 : ch) * cs, pv);
+        if (ch == 0) {
 #pragma unroll
-            for (int q = 0; q < 8; q++) pv[q] = r[q];
+            for (int q = 0; q < 8; q++) pv[q] = R(0);
         }
-#pragma unroll
-        for (int m = 0; m < 2; m++) {
-            const R pA = pv[2 * m], pC = pv[2 * m + 1];
-            const R r = trcp<R>(R(1) - Af[m] * pC - Cf[m] * Al[m]);
-            ea_[m] = -Af[m] * pA * r;
-            ec_[m] = -Cf[m] * Cl[m] * r;
-            if (m == 0) {
-#pragma unroll
-                for (int v = 0; v < 3; v++) ed[v] = (Df[v] - Af[0] * pv[4 + v] - Cf[0] * Dl[v]) * r;
-            } else {
-                ed[3] = (Df[3] - Af[1] * pv[7] - Cf[1] * Dl[3]) * r;
-            }
-        }
+        cr_step<R>(red, pv, ea_, ec_, ed);
     }
     int nstep = 0;
-    for (int s = 1; s < P; s <<= 1, nstep++) {
-        R *bw = (nstep & 1) ? buf0 : buf1;
-        {
-            R *w = SLOT(bw, ch);
-            w[0] = ea_[0]; w[1] = ec_[0]; w[2] = ea_[1]; w[3] = ec_[1];
-            w[4] = ed[0]; w[5] = ed[1]; w[6] = ed[2]; w[7] = ed[3];
-        }
+    for (int st = 1; st < P; st <<= 1, nstep++) {
+        R *const bw = (nstep & 1) ? s0 : s1;
+        slot_store<R>(bw + ch * cs, ea_[0], ec_[0], ea_[1], ec_[1], ed[0], ed[1], ed[2], ed[3]);
         __syncthreads();
-        R mv[8] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};
-        R pv[8] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};
-        if (ch - s >= 0) {
-            const R *r = SLOT(bw, ch - s);
-#pragma unroll
-            for (int q = 0; q < 8; q++) mv[q] = r[q];
-        }
-        if (ch + s < P) {
-            const R *r = SLOT(bw, ch + s);
-#pragma unroll
-            for (int q = 0; q < 8; q++) pv[q] = r[q];
-        }
-#pragma unroll
-        for (int m = 0; m < 2; m++) {
-            const R a = ea_[m], c = ec_[m];
-            const R r = trcp<R>(R(1) - a * mv[2 * m + 1] - c * pv[2 * m]);
-            if (m == 0) {
-#pragma unroll
-                for (int v = 0; v < 3; v++) ed[v] = (ed[v] - a * mv[4 + v] - c * pv[4 + v]) * r;
-            } else {
-                ed[3] = (ed[3] - a * mv[7] - c * pv[7]) * r;
-            }
-            ea_[m] = -a * mv[2 * m] * r;
-            ec_[m] = -c * pv[2 * m + 1] * r;
-        }
+        R mv[8], pv[8];
+        slot_load<R>(bw + (ch - st >= 0 ? ch - st : ch) * cs, mv);
+        slot_load<R>(bw + (ch + st < P ? ch + st : ch) * cs, pv);
+        pcr_update<R>(mv, pv, ea_, ec_, ed);
     }
-    R *bx = (nstep & 1) ? buf0 : buf1;
-    {
-        R *w = SLOT(bx, ch);
-        w[0] = ed[0]; w[1] = ed[1]; w[2] = ed[2]; w[3] = ed[3];
-    }
+    R *const bx = (nstep & 1) ? s0 : s1;
+    slot_store<R>(bx + ch * cs, ed[0], ed[1], ed[2], ed[3], R(0), R(0), R(0), R(0));
     __syncthreads();
     R xf[4], xl[4];
     {
-        R nf[4] = {R(0), R(0), R(0), R(0)};
-        if (ch + 1 < P) {
-            const R *r = SLOT(bx, ch + 1);
-#pragma unroll
-            for (int v = 0; v < 4; v++) nf[v] = r[v];
-        }
+        R nf[8];
+        slot_load<R>(bx + (ch + 1 < P ? ch + 1 : ch) * cs, nf);
 #pragma unroll
         for (int v = 0; v < 4; v++) {
             xf[v] = ed[v];
             const int m = v < 3 ? 0 : 1;
-            xl[v] = Dl[v] - Al[m] * xf[v] - Cl[m] * nf[v];
+            xl[v] = red.Dl[v] - red.Al[m] * xf[v] - red.Cl[m] * nf[v];   // Cl = 0 on the last chunk
         }
     }
     if (!has) return;
 
     // ---------------- write-back ----------------
-    const long long lb = line_base(DIR, g, line);
 #pragma unroll
     for (int i = 0; i < K; i++) {
         const int kd = kind[i];
-        if (kd == T_NONE) continue;
+        if (kd == R_NONE) continue;
         const int p = p0 + i;
         const long long off = lb + (long long)p * g.stride;
 #pragma unroll
         for (int v = 0; v < 4; v++) {
             const int m = v < 3 ? 0 : 1;
             R x = i == 0 ? xf[v] : (i == K - 1 ? xl[v] : dv[v][i] - ea[m][i] * xf[v] - ec[m][i] * xl[v]);
-            if (kd == T_IN) {
-                x += TC(v, p);
-                R mm = (TT(v, p) + x) * R(0.5);
+            if (kd == R_IN) {
+                x += cT[v * fs + p * NLT];
+                const R tv = v == DIR ? wT[p * WIDE] : tT[(v < DIR ? v : v - 1) * fs + p * NLT];
+                R mm = (tv + x) * R(0.5);
                 if (merges == 2) mm = (mm + x) * R(0.5);
                 tout.f[v][off] = mm;
             }

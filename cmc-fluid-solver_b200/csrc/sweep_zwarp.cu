@@ -323,17 +323,9 @@ __global__ void __launch_bounds__(128)
             mD[v] = sh_up(ed[v], s, P);
             pD[v] = sh_down(ed[v], s, P);
         }
-        const bool hasm = ch >= s, hasp = ch + s < P;
-#pragma unroll
-        for (int m = 0; m < 2; m++) {
-            if (!hasm) { mA[m] = R(0); mC[m] = R(0); }
-            if (!hasp) { pA[m] = R(0); pC[m] = R(0); }
-        }
-#pragma unroll
-        for (int v = 0; v < 4; v++) {
-            if (!hasm) mD[v] = R(0);
-            if (!hasp) pD[v] = R(0);
-        }
+        // lanes whose partner lies outside the line receive their own row from the
+        // shuffle; their coupling to it is exactly zero (first row a = 0, last row
+        // c = 0, preserved by every step), so the finite values drop out.
 #pragma unroll
         for (int m = 0; m < 2; m++) {
             const R a = ea_[m], c = ec_[m];
