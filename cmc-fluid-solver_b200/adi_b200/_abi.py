@@ -28,6 +28,7 @@ EXPORTED = [
     "adi_get_segments", "adi_update_boundaries", "adi_time_step", "adi_step", "adi_run", "adi_get_state",
     "adi_set_state", "adi_get_layer", "adi_div_error", "adi_device_pointers", "adi_version",
     "adi_set_profiling", "adi_get_profile", "adi_get_fast_shape", "adi_set_fast_shape", "adi_autotune",
+    "adi_sweep_exact_static", "adi_static_scratch_bytes",
 ]
 
 K_NUM = 7
@@ -46,6 +47,16 @@ class FluidParams(C.Structure):
 class SegStats(C.Structure):
     _fields_ = [("num_segments", C.c_int64 * 3), ("num_nodes", C.c_int64 * 3), ("max_size", C.c_int32 * 3),
                 ("max_per_line", C.c_int32 * 3), ("num_in", C.c_int64)]
+
+
+class StaticSweepArgs(C.Structure):
+    """adi_static_sweep_args: one allocation-free exact sweep on caller-owned device arrays."""
+    _fields_ = [("dir", C.c_int), ("dimx", C.c_int), ("dimy", C.c_int), ("dimz", C.c_int),
+                ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double), ("dt", C.c_double),
+                ("params", FluidParams), ("precision", C.c_int), ("merges", C.c_int),
+                ("node_type", C.c_void_p), ("bc_vel", C.c_void_p), ("bc_temp", C.c_void_p),
+                ("node_value", C.c_void_p * 4), ("cur", C.c_void_p * 4), ("temp_in", C.c_void_p * 4),
+                ("next", C.c_void_p * 4), ("temp_out", C.c_void_p * 4), ("stream", C.c_void_p)]
 
 
 class Profile(C.Structure):
@@ -88,6 +99,7 @@ def load() -> C.CDLL:
         "adi_get_layer": [vp, i, i, i, vp, vp],
         "adi_div_error": [vp, C.POINTER(d)],
         "adi_device_pointers": [vp, C.POINTER(vp * 8)],
+        "adi_sweep_exact_static": [C.POINTER(StaticSweepArgs)],
         "adi_set_profiling": [vp, i],
         "adi_get_fast_shape": [vp, i, C.POINTER(i), C.POINTER(i), C.POINTER(i)],
         "adi_set_fast_shape": [vp, i, i, i],
@@ -102,6 +114,8 @@ def load() -> C.CDLL:
     lib.adi_last_error_string.restype = C.c_char_p
     lib.adi_version.argtypes = []
     lib.adi_version.restype = C.c_char_p
+    lib.adi_static_scratch_bytes.argtypes = []
+    lib.adi_static_scratch_bytes.restype = C.c_size_t
     _lib = lib
     return lib
 

@@ -226,6 +226,56 @@ adi_status adi_get_profile(adi_handle *h, adi_profile *out, int reset);
  * cur u, v, w, T then next u, v, w, T. */
 adi_status adi_device_pointers(adi_handle *h, void *out8[8]);
 
+/* ---- allocation-free sweep ----------------------------------------------- */
+
+/* This entry point has no counterpart in the reference: it exists for callers
+ * that cannot allocate device memory while they run -- hosts whose device memory
+ * is owned by their own pool allocator, time loops that must not pay cudaMalloc's
+ * implicit synchronisation and latency, and code running where allocation is not
+ * allowed.  It performs one exact sweep of one direction (the arithmetic of the
+ * ADI_SOLVER_EXACT path: Thomas per segment, reference operation order) on device
+ * arrays the caller owns and allocates nothing:
+ *   - no handle and no segment lists: each line finds its own segments;
+ *   - the elimination scratch is one fixed static device array of
+ *     adi_static_scratch_bytes() (16 MiB), compiled into the library; every GPU
+ *     that loads the library holds it until the process exits.  Lines are
+ *     processed in batches that fit it (one launch per batch, in stream order).
+ *     A line longer than 16 MiB / (6 * 128 * element size) nodes (5461 in float,
+ *     2730 in double) is rejected with ADI_ERR_CAPACITY.
+ *   - every call shares that array and leaves its last contents behind; each
+ *     scratch value a launch reads was written earlier in the same launch by the
+ *     same thread, so nothing needs clearing.  Calls whose work overlaps on the GPU
+ *     (different streams, or different host threads on one device) race on the
+ *     array: serialise them, e.g. issue them on one stream.
+ *   - the first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress) with that device current; make that first call
+ *     before any stream capture.
+ * All pointers are device pointers in the precision's element type, except the
+ * three uint8 node arrays (Grid3D Node SoA).  temp_in and temp_out must not
+ * alias each other or cur; next must not alias cur or temp_in.  merges is 1, or 2
+ * for the sweep that also carries the per-iteration extra merge.  Asynchronous
+ * on `stream`. */
+typedef struct adi_static_sweep_args {
+    int dir;                  /* ADI_X, ADI_Y or ADI_Z */
+    int dimx, dimy, dimz;
+    double dx, dy, dz, dt;
+    adi_fluid_params params;
+    int precision;            /* ADI_FP32 or ADI_FP64 */
+    int merges;               /* 1 or 2 */
+    const uint8_t *node_type, *bc_vel, *bc_temp;
+    const void *node_value[4];  /* v.x v.y v.z T */
+    const void *cur[4];
+    const void *temp_in[4];
+    void *next[4];
+    void *temp_out[4];
+    void *stream;             /* cudaStream_t; NULL = legacy default stream */
+} adi_static_sweep_args;
+
+adi_status adi_sweep_exact_static(const adi_static_sweep_args *args);
+
+/* Size in bytes of the fixed scratch array used by adi_sweep_exact_static. */
+size_t adi_static_scratch_bytes(void);
+
 /* Library build/version string. */
 const char *adi_version(void);
 
