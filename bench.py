@@ -28,6 +28,7 @@ decomposition is out of scope), so N ranks run N independent replicas
 from __future__ import annotations
 
 import argparse
+import contextlib
 import json
 import os
 import statistics
@@ -85,14 +86,23 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(config: str, solver: str):
-    """Per-launch DRAM bytes of the sweep kernel from a committed ncu summary, if any."""
+def ncu_traffic(config: str, kernel: str):
+    """Per-launch DRAM bytes (read + write) of a sweep kernel from the committed ncu summary, if any."""
     p = os.path.join(ROOT, "profiles", "sweep_traffic.json")
     if not os.path.exists(p):
         return None
     with open(p) as f:
         d = json.load(f)
-    return d.get(f"{config}/{solver}")
+    return d.get(f"{config}/{kernel}")
+
+
+def sweep_kernel_name(solver: str, shape) -> str:
+    """Kernel that runs one direction's sweep: the exact kernel, or the fast variant its shape selects
+    (lines per CTA NL > 0 generic chunked, 0 warp-resident Z lines, -16 TMA-fed X/Y tiles)."""
+    if solver == "exact":
+        return "sweep_exact_kernel"
+    nl = shape[1]
+    return "sweep_fast_kernel" if nl > 0 else ("sweep_zwarp_kernel" if nl == 0 else "sweep_xytma_kernel")
 
 
 class ClockSampler:
@@ -149,6 +159,21 @@ def dist_setup():
     return world, rank, local
 
 
+@contextlib.contextmanager
+def stdout_to_stderr():
+    """Sends fd 1 to fd 2 while the reference solver runs: it prints progress and its profiler table
+    to stdout, and stdout carries only the JSON line."""
+    sys.stdout.flush()
+    saved = os.dup(1)
+    os.dup2(2, 1)
+    try:
+        yield
+    finally:
+        sys.stdout.flush()
+        os.dup2(saved, 1)
+        os.close(saved)
+
+
 def cpu_reference_run(cfg, steps: int, budget_s: float, d=None):
     """Times the reference CPU solver on the workload: up to `steps` steps or until
     budget_s seconds have passed (at least one).  Returns (cells*steps/s, steps, s)."""
@@ -177,9 +202,10 @@ def run_reference(args):
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
     d = cfg["make"]()
     # warm-up steps are part of the sample budget too (first-touch of the layers)
-    if args.warmup:
-        cpu_reference_run(cfg, min(args.warmup, 1), 60.0, d)
-    value, done, el = cpu_reference_run(cfg, args.steps, args.ref_budget, d)
+    with stdout_to_stderr():
+        if args.warmup:
+            cpu_reference_run(cfg, min(args.warmup, 1), 60.0, d)
+        value, done, el = cpu_reference_run(cfg, args.steps, args.ref_budget, d)
     cores = int(os.environ["OMP_NUM_THREADS"])
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
@@ -210,6 +236,11 @@ def run_ours(args):
     s = adi_b200.AdiSolver3D(d, Re=cfg["Re"], Pr=cfg["Pr"], lam=cfg["lam"], precision=adi_b200.ADI_FP32,
                              solver=solver_kind, stream=stream.cuda_stream)
     stats = s.CreateSegments()
+    if args.shapes:
+        for dr, kn in enumerate(args.shapes.split(";")):
+            K, NL = (int(x) for x in kn.split(","))
+            s.set_fast_shape(dr, K, NL)
+    shapes = ";".join(f"{K},{NL}" for K, NL, _ in s.fast_shapes())
     dt, ng, nl = cfg["dt"], cfg["ng"], cfg["nl"]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
@@ -283,13 +314,21 @@ def run_ours(args):
     e2e_value = world * d.cells * e2e_steps / (e2e_ms / 1e3)
     io_bytes = 4 * d.cells * 4
 
-    sweep_keys = ("sweep_x", "sweep_y", "sweep_z")
-    sw_bytes = sum(prof[k]["bytes"] for k in sweep_keys)
-    sw_ms = sum(prof[k]["ms"] for k in sweep_keys)
-    sw_launches = sum(prof[k]["launches"] for k in sweep_keys)
+    # group the sweep classes by the kernel that ran them; the roofline is the busiest kernel's
+    groups = {}
+    for dr, key in enumerate(("sweep_x", "sweep_y", "sweep_z")):
+        g = groups.setdefault(sweep_kernel_name(args.solver, s.fast_shapes()[dr]), [0.0, 0.0, 0])
+        g[0] += prof[key]["bytes"]
+        g[1] += prof[key]["ms"]
+        g[2] += prof[key]["launches"]
+    per_kernel = {k: {"launches_per_step": g[2] / args.steps, "us_per_launch": 1e3 * g[1] / g[2],
+                      "algorithmic_bytes_per_launch": g[0] / g[2],
+                      "achieved_gbs": (g[0] / g[2]) / (g[1] / g[2] / 1e3) / 1e9}
+                  for k, g in groups.items() if g[2] and g[1] > 0}
+    top = max(per_kernel, key=lambda k: groups[k][1])
     peak, peak_kind = measured_peaks()
-    achieved = (sw_bytes / sw_launches) / (sw_ms / sw_launches / 1e3) / 1e9 if sw_ms > 0 else 0.0
-    traffic = ncu_traffic(args.config, args.solver)
+    achieved = per_kernel[top]["achieved_gbs"]
+    traffic = ncu_traffic(args.config, top)
     launches = sum(v["launches"] for v in prof_plain.values())
     step_bytes = sum(v["bytes"] for v in prof.values()) / args.steps
 
@@ -299,7 +338,8 @@ def run_ours(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"{args.config}: {cfg['desc']}", "cells": d.cells,
                    "segments_xyz": stats["num_segments"], "segment_nodes_xyz": stats["num_nodes"],
-                   "solver": args.solver, "parallelism": f"replicas x{world}" if world > 1 else "single domain",
+                   "solver": args.solver, "fast_shapes": shapes if args.solver == "fast" else None,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single domain",
                    "l2": "flushed between steps (256 MiB memset, excluded from the time)",
                    "algorithmic_bytes_per_step": step_bytes},
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes,
@@ -307,13 +347,14 @@ def run_ours(args):
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if peak else None, "traffic": traffic,
-                     "kernel": f"sweep_{args.solver} (X, Y, Z)", "peak_source": peak_kind,
+                     "kernel": top, "peak_source": peak_kind, "per_kernel": per_kernel,
                      "per_class_ms_per_step": {k: v["ms"] / args.steps for k, v in prof.items() if v["launches"]}},
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
-        v, done, el = cpu_reference_run(cfg, 1000, args.cpu_budget, d)
+        with stdout_to_stderr():
+            v, done, el = cpu_reference_run(cfg, 1000, args.cpu_budget, d)
         line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": int(os.environ["OMP_NUM_THREADS"]),
                                 "kind": "reference",
                                 "sample": f"{done} full steps of {args.config} ({el:.1f} s) on the reference "
@@ -337,6 +378,9 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of reference CPU time for cpu_baseline")
     ap.add_argument("--ref-budget", type=float, default=120.0, help="seconds cap for --impl reference")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shapes", default=None,
+                    help='fast sweep shapes "K,NL;K,NL;K,NL" for X;Y;Z instead of the autotuned ones '
+                         '(profiling runs pin them: timings under a profiler mislead the autotuner)')
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
