@@ -34,6 +34,7 @@ SOURCES = [
     ("sweep_fast.cu", []),
     ("sweep_zwarp.cu", []),
     ("sweep_xytma.cu", []),
+    ("sweep_xypair.cu", []),
 ]
 
 

@@ -11,6 +11,8 @@
 #include "adi_b200.h"
 #include "adi_internal.cuh"
 
+#include <type_traits>
+
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -61,6 +63,7 @@ struct adi_handle {
     bool tuned = false;
 
     bool mask_set = false, segs_built = false, contract_ok = false;
+    bool bv_synced = false;   // cur == node values at every BOUND/VALVE node
     std::string contract_msg;
     std::string err;
     double diff_error = 0.0;
@@ -139,6 +142,7 @@ SweepConst<R> sweep_const(const adi_handle *h, int dir, R dt)
     k.inv_two_dx = R(1) / k.two_dx;
     k.inv_two_dy = R(1) / k.two_dy;
     k.inv_two_dz = R(1) / k.two_dz;
+    k.nv_in_temp = h->bv_synced ? 1 : 0;
     return k;
 }
 
@@ -245,6 +249,7 @@ bool shape_ok(const adi_handle *h, int dir, const FastShape &s)
 {
     if (s.mode == 1) return dir == 2 && zwarp_supported(h->nz, s.K, (int)esize(h));
     if (s.mode == 2) return dir < 2 && xytma_supported(dir, h->nx, h->ny, h->nz, s.K, (int)esize(h));
+    if (s.mode == 3) return dir < 2 && xypair_supported(dir, h->nx, h->ny, h->nz, s.K, (int)esize(h));
     return s.mode == 0 && fast_shape_supported(dir, s, line_len(h, dir), (int)esize(h));
 }
 
@@ -260,6 +265,12 @@ cudaError_t launch_fast(adi_handle *h, int dir, CLayer<R> cur, CLayer<R> tin, La
     if (s.mode == 2)
         return launch_sweep_xytma<R>(dir, d, h->d_line_lo[dir], cur, tin, next, tout, k, merges, s.K, h->d_err,
                                      h->stream);
+    if (s.mode == 3) {
+        if constexpr (std::is_same<R, float>::value)
+            return launch_sweep_xypair(dir, d, h->d_line_lo[dir], cur, tin, next, tout, k, merges, s.K, h->d_err,
+                                       h->stream);
+        return cudaErrorInvalidConfiguration;
+    }
     return launch_sweep_fast<R>(dir, d, h->d_line_lo[dir], h->d_line_hi[dir], cur, tin, next, tout, k, merges, s,
                                 h->stream);
 }
@@ -305,11 +316,16 @@ std::vector<FastShape> shape_candidates(const adi_handle *h, int dir)
             FastShape s{K, 0, len / K, 1};
             if (shape_ok(h, dir, s)) out.push_back(s);
         }
-    else
+    else {
+        for (int K : {4, 8}) {
+            FastShape s{K, 32, len / K, 3};
+            if (shape_ok(h, dir, s)) out.push_back(s);
+        }
         for (int K : {8, 16}) {
             FastShape s{K, 16, len / K, 2};
             if (shape_ok(h, dir, s)) out.push_back(s);
         }
+    }
     for (int K : {4, 8, 12, 16})
         for (int NL : {1, 2, 4, 8, 16, 32}) {
             if (dir != 2 && NL < 8) continue;   // X/Y: lanes run along k, keep >= 32-byte runs
@@ -397,6 +413,7 @@ adi_status time_step(adi_handle *h, double dt, int num_global, int num_local, in
         return launch_step_begin<R>(view<R>(h), layer<R>(h, h->cur), layer<R>(h, h->nxt), layer<R>(h, h->ta),
                                     layer<R>(h, h->tb), update_bnd, h->stream);
     }));
+    if (update_bnd) h->bv_synced = true;
     adi_status s = run_sweeps<R>(h, dtr, num_global, num_local);
     if (s != ADI_OK) return s;
     if (compute_error) {
@@ -409,6 +426,7 @@ adi_status time_step(adi_handle *h, double dt, int num_global, int num_local, in
         return fail(h, ADI_ERR_DIVERGENCE, buf);
     }
     std::swap(h->cur, h->nxt);
+    h->bv_synced = false;   // the new state holds the sweeps' boundary values
     return ADI_OK;
 }
 
@@ -572,6 +590,7 @@ adi_status adi_set_mask(adi_handle *h, const uint8_t *type, const uint8_t *bc_ve
     }
     h->mask_set = true;
     h->segs_built = false;
+    h->bv_synced = true;   // the initial state is the node values
     return ADI_OK;
 }
 
@@ -645,7 +664,7 @@ adi_status adi_get_fast_shape(adi_handle *h, int dir, int *K, int *NL, int *P)
     if (!h || dir < 0 || dir > 2) return ADI_ERR_BAD_ARG;
     const FastShape s = h->shape[dir];
     if (K) *K = s.K;
-    if (NL) *NL = s.mode == 1 ? 0 : (s.mode == 2 ? -16 : s.NL);
+    if (NL) *NL = s.mode == 1 ? 0 : (s.mode == 2 ? -16 : (s.mode == 3 ? -32 : s.NL));
     if (P) *P = (line_len(h, dir) + s.K - 1) / s.K;
     return ADI_OK;
 }
@@ -654,7 +673,8 @@ adi_status adi_set_fast_shape(adi_handle *h, int dir, int K, int NL)
 {
     if (!h || dir < 0 || dir > 2 || K <= 0) return ADI_ERR_BAD_ARG;
     const int len = line_len(h, dir);
-    FastShape s{K, NL < 0 ? -NL : NL, (len + K - 1) / K, NL == 0 ? 1 : (NL < 0 ? 2 : 0)};
+    if (NL < 0 && NL != -16 && NL != -32) return fail(h, ADI_ERR_BAD_ARG, "unsupported fast-sweep shape");
+    FastShape s{K, NL < 0 ? -NL : NL, (len + K - 1) / K, NL == 0 ? 1 : (NL == -16 ? 2 : (NL == -32 ? 3 : 0))};
     if (!shape_ok(h, dir, s)) return fail(h, ADI_ERR_BAD_ARG, "unsupported fast-sweep shape");
     h->shape[dir] = s;
     h->tuned = true;
@@ -684,6 +704,7 @@ adi_status adi_update_boundaries(adi_handle *h)
         if (h->prec == ADI_FP64) return launch_update_boundaries<double>(view<double>(h), layer<double>(h, h->cur), h->stream);
         return launch_update_boundaries<float>(view<float>(h), layer<float>(h, h->cur), h->stream);
     }));
+    h->bv_synced = true;
     return ADI_OK;
 }
 
@@ -738,6 +759,7 @@ adi_status adi_set_state(adi_handle *h, const void *u, const void *v, const void
     for (int f = 0; f < 4; f++)
         CK(cudaMemcpyAsync(h->d_L[h->cur][f], src[f], fb, cudaMemcpyHostToDevice, h->stream));
     CK(cudaStreamSynchronize(h->stream));
+    h->bv_synced = false;
     return ADI_OK;
 }
 
@@ -823,6 +845,7 @@ adi_status adi_device_pointers(adi_handle *h, void *out8[8])
         out8[f] = h->d_L[h->cur][f];
         out8[4 + f] = h->d_L[h->nxt][f];
     }
+    h->bv_synced = false;   // the caller may write the state through these
     return ADI_OK;
 }
 

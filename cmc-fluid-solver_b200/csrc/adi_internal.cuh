@@ -76,6 +76,12 @@ struct SweepConst {
     R three_dt;                          // 3/dt
     R inv_two_h;                         // 1/(2h) along the line
     R inv_two_dx, inv_two_dy, inv_two_dz;
+    // 1 when cur equals the node values at every BOUND/VALVE node at the start of
+    // the step (adi_update_boundaries ran since the state last changed).  The
+    // nonlinear layers are copies of cur that sweeps never write off NODE_IN, so
+    // Dirichlet boundary rows can then read their value from the temp tile they
+    // already hold instead of loading the node-value arrays.
+    int nv_in_temp;
 };
 
 // Launch shape of the fast sweep: NL lines per CTA, chunks of K rows per thread,
@@ -83,7 +89,8 @@ struct SweepConst {
 struct FastShape {
     int K, NL, P;
     int mode;   // 0: generic chunked kernel; 1: warp-resident Z lines (sweep_zwarp.cu);
-                // 2: TMA-fed X/Y tiles (sweep_xytma.cu)
+                // 2: TMA-fed X/Y tiles (sweep_xytma.cu); 3: persistent double-buffered
+                // X/Y tiles, two lines per thread (sweep_xypair.cu, FP32)
 };
 
 // Device-side description of one domain, passed by value to kernels.
@@ -132,6 +139,10 @@ cudaError_t launch_sweep_xytma(int dir, const DomainView<R> &d, const int *line_
                                Layer<R> next, Layer<R> tout, const SweepConst<R> &k, int merges, int K,
                                int *err_flag, cudaStream_t s);
 bool xytma_supported(int dir, int nx, int ny, int nz, int K, int elem_bytes);
+cudaError_t launch_sweep_xypair(int dir, const DomainView<float> &d, const int *line_lo, CLayer<float> cur,
+                                CLayer<float> tin, Layer<float> next, Layer<float> tout, const SweepConst<float> &k,
+                                int merges, int K, int *err_flag, cudaStream_t s);
+bool xypair_supported(int dir, int nx, int ny, int nz, int K, int elem_bytes);
 
 cudaError_t launch_segment_scan(int dir, int nx, int ny, int nz, const uint8_t *code, int *line_count,
                                 int *line_lo, int *line_hi, int *line_maxlen, long long *line_nodes,

@@ -256,10 +256,13 @@ __global__ void __launch_bounds__(256)
                 // -delta[n-2] + 2x[n-1] = cur[n-2].
                 const long long off = base + (long long)(p0 + i) * sl;
                 const bool vf = (freebits >> (2 * i)) & 1u, tf = (freebits >> (2 * i + 1)) & 1u;
-                const int nb = kd == K_END ? i : i + 2;   // cu index of the IN neighbour
+                const bool from_left = kd == K_END;   // IN neighbour at row i-1, else at i+1
 #pragma unroll
-                for (int v = 0; v < 3; v++) dv[v][i] = vf ? cu[v][nb] : __ldg(d.nv[v] + off);
-                dv[3][i] = tf ? cu[3][nb] : __ldg(d.nv[3] + off);
+                for (int v = 0; v < 4; v++) {
+                    const bool fr = v < 3 ? vf : tf;
+                    const R cn = from_left ? cu[v][i] : cu[v][i + 2];
+                    dv[v][i] = fr ? cn : (kc.nv_in_temp ? tv[v][i + 1] : __ldg(d.nv[v] + off));
+                }
             }
         }
     }

@@ -2,8 +2,7 @@
 //
 // A CTA owns NL = 16 neighbouring lines (16 consecutive k at one j for X, at one i
 // for Y) over their whole length L.  One thread issues the tile loads
-// (cp.async.bulk.tensor, no multicast) into shared memory, all completing on one
-// mbarrier:
+// (cp.async.bulk.tensor, no multicast) into shared memory:
 //   cur   U V W T           16 x L each
 //   temp  three fields      16 x L each
 //   temp  advecting field   24 x L (k0-4 .. k0+19: the lines plus the k+-1 halo,
@@ -17,47 +16,27 @@
 // tiles, and store results straight to global memory (lanes run along k, so
 // each warp store covers two 64-byte runs).
 //
-// The mbarrier wait is bounded: if the tile has not landed after about a second
-// the CTA raises the handle's error flag and leaves without computing.
+// The tile arrives as up to four boxes along the line, each on its own mbarrier,
+// and a thread waits only for the boxes its rows need.  Every wait is bounded: if
+// a box has not landed after about a second the CTA raises the handle's error flag
+// and leaves before writing anything.
 #include "adi_internal.cuh"
 #include "sweep_common.cuh"
 
-#include <cuda.h>
-#include <cudaTypedefs.h>
+#include "tma.cuh"
 
 #include <mutex>
 #include <vector>
 
 namespace adi {
 
+using tma::smem_u32;
+using tma::load_3d;
+
 namespace {
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p)
-{
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, uint64_t *bar)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
-        :
-        : "r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
-        : "memory");
-}
-
 constexpr int NLT = 16;   // lines per CTA
 constexpr int WIDE = 24;  // width of the advecting-field tile (k0-4 .. k0+19)
-
 } // namespace
-
-// Tensor maps of one launch (by value, in param space).
-struct XYMaps {
-    CUtensorMap cur[4];
-    CUtensorMap tin[4];   // plain 16-wide boxes
-    CUtensorMap fwide;    // advecting field of temp, 24-wide box
-    CUtensorMap code;
-};
 
 template <typename R, int DIR, int K>
 __global__ void __launch_bounds__(256)
@@ -87,58 +66,54 @@ __global__ void __launch_bounds__(256)
     const size_t code_bytes = ((size_t)L * NLT + 127) / 128 * 128;
     R *buf0 = reinterpret_cast<R *>(smem + 9 * plane + wide_bytes + code_bytes);
     R *buf1 = buf0 + (size_t)NLT * P * 8;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(buf1 + (size_t)NLT * P * 8);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(buf1 + (size_t)NLT * P * 8);   // one per box along the line
 
     const bool has = line < g.nlines && line_lo[line] >= 0;
     if (!__syncthreads_or(has)) return;   // no segment in these 16 lines
 
     if (t == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        for (int b = 0; b < nbox; b++) tma::mbar_init(&bar[b], 1);
+        tma::fence_barrier_init();
     }
     __syncthreads();
     if (t == 0) {
         // every box delivers its full size (zero fill included): cur 4, temp 3,
         // off-line halo 2 planes, the wide advecting tile and the code tile
-        const uint32_t bytes = (uint32_t)(9 * plane + (size_t)L * WIDE * sizeof(R) + (size_t)L * NLT);
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                     : "memory");
+        const uint32_t bytes = (uint32_t)(9 * (size_t)Lb * NLT * sizeof(R) + (size_t)Lb * WIDE * sizeof(R) +
+                                          (size_t)Lb * NLT);
         for (int b = 0; b < nbox; b++) {
+            uint64_t *bb = &bar[b];
+            tma::arrive_expect_tx(bb, bytes);
             const int p0 = b * Lb;
             const size_t po = (size_t)p0 * NLT;        // row offset inside a [L][16] tile
             // coordinates (innermost first): X {k, j, x}, Y {k, y, i}
             const int c1 = DIR == 0 ? outer : p0, c2 = DIR == 0 ? p0 : outer;
             for (int v = 0; v < 4; v++) {
-                tma_load_3d(tcur + v * (plane / sizeof(R)) + po, &maps.cur[v], k0, c1, c2, bar);
+                load_3d(tcur + v * (plane / sizeof(R)) + po, &maps.cur[v], k0, c1, c2, bb);
                 if (v != DIR)
-                    tma_load_3d(ttin + (v < DIR ? v : v - 1) * (plane / sizeof(R)) + po, &maps.tin[v], k0, c1, c2, bar);
+                    load_3d(ttin + (v < DIR ? v : v - 1) * (plane / sizeof(R)) + po, &maps.tin[v], k0, c1, c2, bb);
             }
-            tma_load_3d(twide + (size_t)p0 * WIDE, &maps.fwide, k0 - 4, c1, c2, bar);
+            load_3d(twide + (size_t)p0 * WIDE, &maps.fwide, k0 - 4, c1, c2, bb);
             if (DIR == 0) {
-                tma_load_3d(thm + po, &maps.tin[DIR], k0, outer - 1, p0, bar);
-                tma_load_3d(thp + po, &maps.tin[DIR], k0, outer + 1, p0, bar);
+                load_3d(thm + po, &maps.tin[DIR], k0, outer - 1, p0, bb);
+                load_3d(thp + po, &maps.tin[DIR], k0, outer + 1, p0, bb);
             } else {
-                tma_load_3d(thm + po, &maps.tin[DIR], k0, p0, outer - 1, bar);
-                tma_load_3d(thp + po, &maps.tin[DIR], k0, p0, outer + 1, bar);
+                load_3d(thm + po, &maps.tin[DIR], k0, p0, outer - 1, bb);
+                load_3d(thp + po, &maps.tin[DIR], k0, p0, outer + 1, bb);
             }
-            tma_load_3d(tcode + po, &maps.code, k0, c1, c2, bar);
+            load_3d(tcode + po, &maps.code, k0, c1, c2, bb);
         }
     }
-    // bounded wait for the tiles (phase 0): at most 2^17 tries of at most ~10 us
+    // Bounded waits (phase 0) for just the boxes holding this thread's rows and
+    // their +-1 neighbours, so chunks near the start of the line begin while the
+    // rest of the tile is still landing.  A thread whose wait gave up computes on
+    // whatever the tile holds; the CTA checks every thread's wait at its first
+    // barrier and leaves before writing anything.
+    bool tiles_ok = true;
     {
-        uint32_t done = 0;
-        for (int it = 0; it < (1 << 17) && !done; it++) {
-            asm volatile(
-                "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0, 10000; selp.u32 %0, 1, 0, p; }"
-                : "=r"(done)
-                : "r"(smem_u32(bar))
-                : "memory");
-        }
-        if (__syncthreads_or(!done)) {
-            if (t == 0) atomicExch(err_flag, 1);
-            return;
-        }
+        const int rlo = ch * K > 0 ? ch * K - 1 : 0;
+        const int rhi = ch * K + K < L ? ch * K + K : L - 1;
+        for (int b = rlo / Lb; b <= rhi / Lb; b++) tiles_ok &= tma::mbar_wait(&bar[b], 0, 1 << 17);
     }
 
     // ---------------- rows from the tiles: one pass, 3-row window ----------------
@@ -209,12 +184,13 @@ __global__ void __launch_bounds__(256)
         } else {
             // boundary row; BC_FREE moves the IN neighbour's cur to the right side
             const bool vf = (kw[1] & CODE_VEL_FREE) != 0, tf = (kw[1] & CODE_TEMP_FREE) != 0;
-            const int nb = kd == R_END ? 0 : 2;
+            const bool from_left = kd == R_END;   // IN neighbour at p-1, else at p+1
             const long long off = lb + (long long)p * g.stride;
 #pragma unroll
             for (int v = 0; v < 4; v++) {
                 const bool fr = v < 3 ? vf : tf;
-                dv[v][i] = fr ? cw[nb][v] : __ldg(d.nv[v] + off);
+                const R cn = from_left ? cw[0][v] : cw[2][v];
+                dv[v][i] = fr ? cn : (kc.nv_in_temp ? tw[1][v] : __ldg(d.nv[v] + off));
             }
         }
 #pragma unroll
@@ -240,7 +216,13 @@ __global__ void __launch_bounds__(256)
     const int cs = NLT * 8;   // elements between the slots of two chunks
     slot_store<R>(s0 + ch * cs, red.Al[0], red.Cl[0], red.Al[1], red.Cl[1], red.Dl[0], red.Dl[1], red.Dl[2],
                   red.Dl[3]);
-    __syncthreads();
+    if (__syncthreads_or(!tiles_ok)) {
+        if (t == 0) {
+            atomicExch(err_flag, 1);
+            for (int b = 0; b < nbox; b++) tma::mbar_wait(&bar[b], 0, 1 << 10);   // copies still in flight
+        }
+        return;
+    }
     R ea_[2], ec_[2], ed[4];
     {
         R pv[8];
@@ -304,7 +286,7 @@ __global__ void __launch_bounds__(256)
 // host side: tensor maps and launch
 // ---------------------------------------------------------------------------
 
-static PFN_cuTensorMapEncodeTiled_v12000 get_encoder()
+static PFN_cuTensorMapEncodeTiled_v12000 get_encoder_fn()
 {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     static bool tried = false;
@@ -322,8 +304,10 @@ static PFN_cuTensorMapEncodeTiled_v12000 get_encoder()
 // Box {w, 1, Lb} for X lines / {w, Lb, 1} for Y lines over a [nx][ny][nz] array.
 // Encoded maps are cached by their arguments (the arrays live as long as their
 // handle; a freed-and-reused address gets the same, still valid, map).
-static bool make_map(CUtensorMap *m, const void *base, int dir, int nx, int ny, int nz, int w, int Lb, int es,
-                     CUtensorMapDataType dt)
+bool have_tensor_map_encoder() { return get_encoder_fn() != nullptr; }
+
+bool make_tile_map(CUtensorMap *m, const void *base, int dir, int nx, int ny, int nz, int w, int Lb, int es,
+                   CUtensorMapDataType dt)
 {
     struct Key {
         const void *base;
@@ -346,7 +330,7 @@ static bool make_map(CUtensorMap *m, const void *base, int dir, int nx, int ny, 
         for (const Ent &e : cache)
             if (e.k == key) { *m = e.m; return true; }
     }
-    auto enc = get_encoder();
+    auto enc = get_encoder_fn();
     if (!enc) return false;
     cuuint64_t dims[3] = {(cuuint64_t)nz, (cuuint64_t)ny, (cuuint64_t)nx};
     cuuint64_t strides[2] = {(cuuint64_t)nz * es, (cuuint64_t)ny * nz * es};
@@ -367,19 +351,19 @@ size_t xytma_smem_bytes(int L, int P, int elem_bytes)
     const size_t plane = (size_t)L * NLT * elem_bytes;
     const size_t wide = ((size_t)L * WIDE * elem_bytes + 127) / 128 * 128;
     const size_t code = ((size_t)L * NLT + 127) / 128 * 128;
-    return 9 * plane + wide + code + 2 * (size_t)NLT * P * 8 * elem_bytes + 16;
+    return 9 * plane + wide + code + 2 * (size_t)NLT * P * 8 * elem_bytes + 64;   // + up to 4 mbarriers
 }
 
 bool xytma_supported(int dir, int nx, int ny, int nz, int K, int elem_bytes)
 {
-    if (dir > 1 || !get_encoder()) return false;
+    if (dir > 1 || !have_tensor_map_encoder()) return false;
     const int L = dir == 0 ? nx : ny;
     if (nz % NLT != 0) return false;            // CTA tiles of 16 lines; code rows 16-byte strided
     if (K != 8 && K != 16) return false;
     if (L % K != 0) return false;
     const int P = L / K;
     if (NLT * P > 256 || NLT * P < 32) return false;
-    if (L > 256 || L % 2 != 0) return false;    // one box along the line; 128-byte aligned tiles
+    if (L > 256 || L % 2 != 0) return false;    // boxes of <= 256 rows; 128-byte aligned tiles
     return xytma_smem_bytes(L, P, elem_bytes) <= 200 * 1024;
 }
 
@@ -392,15 +376,17 @@ cudaError_t launch_sweep_xytma(int dir, const DomainView<R> &d, const int *line_
     if (!xytma_supported(dir, d.nx, d.ny, d.nz, K, es)) return cudaErrorInvalidConfiguration;
     const LineGeom g = line_geom(dir, d.nx, d.ny, d.nz);
     const int L = g.len, P = L / K;
+    // one box along the line (lines of up to 256 rows); the kernel also takes
+    // several boxes per line, each on its own mbarrier, but splitting measured slower
     const int nbox = (L + 255) / 256, Lb = L / nbox;
     const CUtensorMapDataType dt = es == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
     XYMaps maps;
     for (int v = 0; v < 4; v++) {
-        if (!make_map(&maps.cur[v], cur.f[v], dir, d.nx, d.ny, d.nz, NLT, Lb, es, dt)) return cudaErrorInvalidValue;
-        if (!make_map(&maps.tin[v], tin.f[v], dir, d.nx, d.ny, d.nz, NLT, Lb, es, dt)) return cudaErrorInvalidValue;
+        if (!make_tile_map(&maps.cur[v], cur.f[v], dir, d.nx, d.ny, d.nz, NLT, Lb, es, dt)) return cudaErrorInvalidValue;
+        if (!make_tile_map(&maps.tin[v], tin.f[v], dir, d.nx, d.ny, d.nz, NLT, Lb, es, dt)) return cudaErrorInvalidValue;
     }
-    if (!make_map(&maps.fwide, tin.f[dir], dir, d.nx, d.ny, d.nz, WIDE, Lb, es, dt)) return cudaErrorInvalidValue;
-    if (!make_map(&maps.code, d.code, dir, d.nx, d.ny, d.nz, NLT, Lb, 1, CU_TENSOR_MAP_DATA_TYPE_UINT8))
+    if (!make_tile_map(&maps.fwide, tin.f[dir], dir, d.nx, d.ny, d.nz, WIDE, Lb, es, dt)) return cudaErrorInvalidValue;
+    if (!make_tile_map(&maps.code, d.code, dir, d.nx, d.ny, d.nz, NLT, Lb, 1, CU_TENSOR_MAP_DATA_TYPE_UINT8))
         return cudaErrorInvalidValue;
     const size_t smem = xytma_smem_bytes(L, P, es);
     const int blocks = (dir == 0 ? d.ny : d.nx) * (d.nz / NLT);

@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(128)
             for (int v = 0; v < 4; v++) {
                 const R nb = kind[i] == Z_END ? (i > 0 ? cu[v][i - 1] : cm_[v]) : (i < K - 1 ? cu[v][i + 1] : cp_[v]);
                 const bool fr = v < 3 ? vf : tf;
-                dv[v][i] = fr ? nb : __ldg(d.nv[v] + off);
+                dv[v][i] = fr ? nb : (kc.nv_in_temp ? tv[v][i] : __ldg(d.nv[v] + off));
             }
         }
     }

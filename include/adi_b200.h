@@ -181,7 +181,10 @@ adi_status adi_div_error(adi_handle *h, double *out);
  * line.  NL = 0 selects the warp-resident Z kernel (Z only; dimz = P*K with P in
  * {4, 8, 16, 32}, K in {4, 8}); NL = -16 selects the TMA-fed X/Y kernel (16 lines
  * per CTA; dimz a multiple of 16, line length <= 256, even and a multiple of K,
- * K in {8, 16}).  adi_build_segments times the candidate shapes on
+ * K in {8, 16}); NL = -32 selects the persistent, double-buffered X/Y kernel with
+ * two lines per thread (FP32 only; dimz a multiple of 16, K in {4, 8}, 2 <= P <= 32,
+ * both tile buffers within 227 KB of shared memory, e.g. line length <= 136 at
+ * K = 4).  adi_build_segments times the candidate shapes on
  * the domain (the autotuner) and keeps the fastest per direction; these calls
  * read or override the choice.  adi_set_fast_shape returns ADI_ERR_BAD_ARG for a
  * shape no kernel is compiled for (generic: K in {4, 8, 12, 16},
@@ -223,7 +226,9 @@ adi_status adi_set_profiling(adi_handle *h, int on);
 adi_status adi_get_profile(adi_handle *h, adi_profile *out, int reset);
 
 /* Device pointers of the current layers (zero-copy, for a torch test harness):
- * cur u, v, w, T then next u, v, w, T. */
+ * cur u, v, w, T then next u, v, w, T.  The state may be written through them
+ * between steps; the next adi_step (or adi_update_boundaries) re-applies the
+ * boundary values. */
 adi_status adi_device_pointers(adi_handle *h, void *out8[8]);
 
 /* ---- allocation-free sweep ----------------------------------------------- */

@@ -172,8 +172,16 @@ int oracle_set_params(void *vh, double v_T, double v_vis, double t_vis, double t
 int oracle_step(void *vh, double dt, int num_global, int num_local, int compute_error)
 {
     oracle_h *h = (oracle_h *)vh;
-    if (h->precision == 8) return step_f64(h->s, dt, num_global, num_local, compute_error);
-    return step_f32(h->s, dt, num_global, num_local, compute_error);
+    if (h->precision == 8) return step_f64(h->s, dt, num_global, num_local, compute_error, 1);
+    return step_f32(h->s, dt, num_global, num_local, compute_error, 1);
+}
+
+/* TimeStep alone (AdiSolver3D.cpp:306-391), without UpdateBoundaries. */
+int oracle_time_step(void *vh, double dt, int num_global, int num_local, int compute_error)
+{
+    oracle_h *h = (oracle_h *)vh;
+    if (h->precision == 8) return step_f64(h->s, dt, num_global, num_local, compute_error, 0);
+    return step_f32(h->s, dt, num_global, num_local, compute_error, 0);
 }
 
 /* which: 0 cur, 1 next, 2 half, 3 temp.  Output as double. */

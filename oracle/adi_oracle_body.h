@@ -248,13 +248,15 @@ static double FN(div_error)(FN(solver) *s, FN(layer) *l)
     return count ? err / count : 0.0;
 }
 
-/* UpdateBoundaries() followed by TimeStep(): one pass of the reference driver
- * loop.  Returns 0, or 1 if the divergence guard (> 0.01) fires, in which case
- * the layers are left unswapped exactly as the reference's throw leaves them. */
-static int FN(step)(FN(solver) *s, double dt_in, int num_global, int num_local, int compute_error)
+/* UpdateBoundaries() (when update_bnd) followed by TimeStep(): with update_bnd
+ * one pass of the reference driver loop (FluidSolver3D.cpp:241-242), without it
+ * TimeStep alone.  Returns 0, or 1 if the divergence guard (> 0.01) fires, in
+ * which case the layers are left unswapped exactly as the reference's throw
+ * leaves them. */
+static int FN(step)(FN(solver) *s, double dt_in, int num_global, int num_local, int compute_error, int update_bnd)
 {
     REAL dt = (REAL)dt_in;
-    FN(update_boundaries)(s);
+    if (update_bnd) FN(update_boundaries)(s);
     FN(layer) *cur = &s->L[s->cur], *next = &s->L[s->next], *half = &s->L[s->half], *temp = &s->L[s->temp];
     FN(copy_where)(s, cur, next, NODE_BOUND_, NODE_BOUND_);
     FN(copy_where)(s, cur, next, NODE_VALVE_, NODE_VALVE_);

@@ -50,6 +50,7 @@ def _load_ref():
         lib.ref_solver_init.argtypes = [C.c_void_p, C.c_int] + [C.c_double] * 5
         lib.ref_fluid_params.argtypes = [C.c_void_p, _f32p]
         lib.ref_step.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int]
+        lib.ref_time_step.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int]
         lib.ref_get_fields.argtypes = [C.c_void_p, C.c_int] + [_f32p] * 4
         lib.ref_set_state.argtypes = [C.c_void_p] + [_f32p] * 4
         lib.ref_div_error.restype = C.c_double
@@ -68,6 +69,7 @@ def _load_oracle():
         lib.oracle_create.argtypes = [C.c_int, C.c_int] + [C.c_int] * 3 + [C.c_double] * 3 + [_u8p] * 3 + [_f64p] * 4
         lib.oracle_set_params.argtypes = [C.c_void_p] + [C.c_double] * 4
         lib.oracle_step.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int]
+        lib.oracle_time_step.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int]
         lib.oracle_get_fields.argtypes = [C.c_void_p, C.c_int] + [_f64p] * 4
         lib.oracle_set_state.argtypes = [C.c_void_p] + [_f64p] * 4
         lib.oracle_div_error.restype = C.c_double
@@ -131,6 +133,10 @@ class RefSolver:
     def step(self, dt, num_global, num_local, compute_error=True) -> int:
         return self.lib.ref_step(self.h, dt, num_global, num_local, int(compute_error))
 
+    def time_step(self, dt, num_global, num_local, compute_error=True) -> int:
+        """TimeStep without UpdateBoundaries."""
+        return self.lib.ref_time_step(self.h, dt, num_global, num_local, int(compute_error))
+
     def fields(self, which=0):
         out = [np.zeros(self.shape, np.float32) for _ in range(4)]
         self.lib.ref_get_fields(self.h, which, *out)
@@ -170,6 +176,10 @@ class OracleSolver:
 
     def step(self, dt, num_global, num_local, compute_error=True) -> int:
         return self.lib.oracle_step(self.h, dt, num_global, num_local, int(compute_error))
+
+    def time_step(self, dt, num_global, num_local, compute_error=True) -> int:
+        """TimeStep without UpdateBoundaries."""
+        return self.lib.oracle_time_step(self.h, dt, num_global, num_local, int(compute_error))
 
     def fields(self, which=0):
         out = [np.zeros(self.shape, np.float64) for _ in range(4)]

@@ -239,6 +239,23 @@ int ref_step(void *vh, double dt, int num_global, int num_local, int compute_err
 	}
 }
 
+// AdiSolver3D::TimeStep alone, without UpdateBoundaries.
+int ref_time_step(void *vh, double dt, int num_global, int num_local, int compute_error)
+{
+	RefHandle *h = (RefHandle *)vh;
+	if (h->solver == NULL) return -2;
+	try
+	{
+		h->solver->TimeStep((FTYPE)dt, num_global, num_local, compute_error != 0);
+		h->steps_done++;
+		return 0;
+	}
+	catch (std::exception &)
+	{
+		return 1;
+	}
+}
+
 // which = 0: cur (latest state after the step's swap), 1: next.
 int ref_get_fields(void *vh, int which, float *u, float *v, float *w, float *T)
 {

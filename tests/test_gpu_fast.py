@@ -92,7 +92,12 @@ def test_autotuner_picks_supported_shapes(adi_lib):
     for dr, (K, NL, P) in enumerate(shapes):
         assert K in (4, 8, 12, 16)
         assert P * K >= d.shape[dr]
-        assert 32 <= NL * P <= 256
+        if NL == 0:
+            assert dr == 2 and P * K == d.shape[2]          # warp-resident Z lines
+        elif NL < 0:
+            assert dr < 2 and NL in (-16, -32) and P * K == d.shape[dr]   # TMA-fed X/Y tiles
+        else:
+            assert 32 <= NL * P <= 256
     with pytest.raises(_abi.AdiError):
         s.set_fast_shape(0, 5, 8)
     with pytest.raises(_abi.AdiError):
@@ -158,3 +163,81 @@ def test_xytma_kernel(adi_lib, xK, precision):
     assert max(errs) < (1e-11 if precision == "fp64" else 2e-6), errs
     errs_n = rel_errors(s.fields(1), orc.fields(1), m)
     assert max(errs_n) < (1e-11 if precision == "fp64" else 2e-6), errs_n
+
+
+def _slab_domain(nx, ny, nz, seed):
+    """Random shell domain plus a wall slab at k = 1..16, so that the first 16-line
+    tile of every X and Y plane holds no segment (the persistent kernel skips it)."""
+    d = G.random_domain(nx, ny, nz, seed=seed, shell=True, n_obstacles=10, rmax=6.0)
+    slab = np.zeros(d.shape, bool)
+    slab[:, :, 1:17] = True
+    slab &= d.type != G.NODE_BOUND
+    d.type[slab] = G.NODE_BOUND
+    d.bc_vel[slab] = G.BC_NOSLIP
+    d.bc_temp[slab] = G.BC_NOSLIP
+    for name in ("vx", "vy", "vz"):
+        getattr(d, name)[slab] = 0.0
+    assert G.validate_for_solver(d) is None
+    return d
+
+
+@pytest.mark.parametrize("xK", [4, 8])
+@pytest.mark.parametrize("slab", [False, True], ids=["plain", "empty-tiles"])
+def test_xypair_kernel(adi_lib, xK, slab):
+    """Persistent double-buffered X/Y kernel (NL = -32, FP32): more tiles than CTAs,
+    so every CTA cycles both tile buffers; with the slab, tiles without segments
+    are skipped without a load."""
+    d = (_slab_domain(128, 96, 48, seed=85) if slab else
+         G.random_domain(128, 96, 48, seed=84, shell=True, n_obstacles=12, rmax=7.0))
+    params = (160.0, 0.72, 1.4)
+    s = solver(adi_lib, d, params, shapes=[(xK, -32), (xK, -32), (8, 8)])
+    assert s.fast_shapes()[0][1] == -32 and s.fast_shapes()[1][1] == -32
+    orc = O.OracleSolver(d, precision=8, params=fluid_params_tuple(("normalized", params)))
+    m = non_out(d)
+    for _ in range(3):
+        assert s.step(6e-4, 4, 2, True) == 0
+        assert orc.step(6e-4, 4, 2, True) == 0
+    errs = rel_errors(s.fields(0), orc.fields(0), m)
+    assert max(errs) < 2e-6, errs
+    errs_n = rel_errors(s.fields(1), orc.fields(1), m)
+    assert max(errs_n) < 2e-6, errs_n
+
+
+def test_xypair_rejects_fp64_and_bad_shapes(adi_lib):
+    from adi_b200 import _abi
+    d = G.random_domain(64, 48, 32, seed=86, n_obstacles=4)
+    s = solver(adi_lib, d, (100.0, 0.72, 1.4), precision=_abi.ADI_FP64)
+    with pytest.raises(_abi.AdiError):
+        s.set_fast_shape(0, 4, -32)          # FP32 only
+    s32 = solver(adi_lib, d, (100.0, 0.72, 1.4))
+    s32.set_fast_shape(0, 4, -32)
+    with pytest.raises(_abi.AdiError):
+        s32.set_fast_shape(2, 4, -32)        # X and Y only
+    with pytest.raises(_abi.AdiError):
+        s32.set_fast_shape(0, 16, -32)       # K in {4, 8}
+    with pytest.raises(_abi.AdiError):
+        s32.set_fast_shape(0, 4, -24)        # no such variant
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_time_step_with_boundary_state_off_node_values(adi_lib, precision):
+    """adi_time_step without a boundary update, from a state whose BOUND/VALVE cells
+    differ from the node values: the fast kernels must load the node values for
+    Dirichlet rows rather than read them from the nonlinear layer."""
+    from adi_b200 import _abi
+    d = G.random_domain(48, 40, 32, seed=87, shell=True, n_obstacles=8, rmax=4.5)
+    params = (140.0, 0.72, 1.4)
+    prec = _abi.ADI_FP64 if precision == "fp64" else _abi.ADI_FP32
+    s = solver(adi_lib, d, params, precision=prec)
+    orc = O.OracleSolver(d, precision=8, params=fluid_params_tuple(("normalized", params)))
+    rng = np.random.default_rng(87)
+    state = [(a + 0.05 * rng.standard_normal(d.shape)).astype(np.float32).astype(np.float64)
+             for a in (d.vx, d.vy, d.vz, d.T)]
+    s.set_state(*[a.astype(np.float64 if precision == "fp64" else np.float32) for a in state])
+    orc.set_state(*state)
+    m = non_out(d)
+    for _ in range(2):
+        s.TimeStep(7e-4, 3, 2, True)
+        assert orc.time_step(7e-4, 3, 2, True) == 0
+    errs = rel_errors(s.fields(0), orc.fields(0), m)
+    assert max(errs) < (1e-11 if precision == "fp64" else 2e-6), errs

@@ -63,6 +63,25 @@ def test_restatement_matches_reference_live(seed):
 
 
 @pytest.mark.skipif(not O.have_ref(), reason="reference build oracle/_ref/libref3d.so not present")
+def test_time_step_without_boundary_update_live():
+    """TimeStep alone, from a state whose boundary cells differ from the node values:
+    Dirichlet rows take the node values, every other read takes the state."""
+    d = G.random_domain(14, 13, 15, seed=24, shell=True, n_obstacles=5)
+    ref = O.RefSolver(d, Re=110.0, Pr=0.8, lam=1.3)
+    orc = O.OracleSolver(d, precision=4, Re=110.0, Pr=0.8, lam=1.3)
+    rng = np.random.default_rng(24)
+    state = [(a + 0.05 * rng.standard_normal(d.shape)).astype(np.float32) for a in (d.vx, d.vy, d.vz, d.T)]
+    ref.set_state(*state)
+    orc.set_state(*[a.astype(np.float64) for a in state])
+    m = non_out(d)
+    for s in range(2):
+        assert ref.time_step(6e-4, 2, 2, True) == orc.time_step(6e-4, 2, 2, True)
+        fr, fo = ref.fields(0), orc.fields(0)
+        for f in range(4):
+            assert np.array_equal(fr[f][m].astype(np.float64), fo[f][m])
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="reference build oracle/_ref/libref3d.so not present")
 def test_segment_lists_random_masks_live():
     rng = np.random.default_rng(5)
     for trial in range(6):
