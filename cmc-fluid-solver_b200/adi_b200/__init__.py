@@ -104,6 +104,16 @@ class AdiSolver3D:
     def run(self, dt, num_global, num_local, n_steps, err_every=10):
         self._check(self.lib.adi_run(self.h, dt, num_global, num_local, n_steps, err_every))
 
+    def step_tol(self, dt, max_global, num_local, tol, compute_error=False):
+        """UpdateBoundaries + TimeStep in tolerance mode; returns (status, iterations, residual)."""
+        it, res = C.c_int(0), C.c_double(0.0)
+        rc = self.lib.adi_step_tol(self.h, dt, max_global, num_local, tol, int(compute_error), C.byref(it),
+                                   C.byref(res))
+        return rc, it.value, res.value
+
+    def set_graphs(self, on: bool):
+        self._check(self.lib.adi_set_graphs(self.h, int(on)))
+
     def GetLayer(self, outdimx=0, outdimy=0, outdimz=0):
         ox, oy, oz = outdimx or self.shape[0], outdimy or self.shape[1], outdimz or self.shape[2]
         v = np.zeros((ox, oy, oz, 3), self.dtype)

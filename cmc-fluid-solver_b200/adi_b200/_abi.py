@@ -28,7 +28,7 @@ EXPORTED = [
     "adi_get_segments", "adi_update_boundaries", "adi_time_step", "adi_step", "adi_run", "adi_get_state",
     "adi_set_state", "adi_get_layer", "adi_div_error", "adi_device_pointers", "adi_version",
     "adi_set_profiling", "adi_get_profile", "adi_get_fast_shape", "adi_set_fast_shape", "adi_autotune",
-    "adi_sweep_exact_static", "adi_static_scratch_bytes",
+    "adi_sweep_exact_static", "adi_static_scratch_bytes", "adi_step_tol", "adi_set_graphs",
 ]
 
 K_NUM = 7
@@ -94,6 +94,8 @@ def load() -> C.CDLL:
         "adi_time_step": [vp, d, i, i, i],
         "adi_step": [vp, d, i, i, i],
         "adi_run": [vp, d, i, i, i, i],
+        "adi_step_tol": [vp, d, i, i, d, i, C.POINTER(i), C.POINTER(d)],
+        "adi_set_graphs": [vp, i],
         "adi_get_state": [vp, i, vp, vp, vp, vp],
         "adi_set_state": [vp, vp, vp, vp, vp],
         "adi_get_layer": [vp, i, i, i, vp, vp],

@@ -64,6 +64,32 @@ struct adi_handle {
 
     bool mask_set = false, segs_built = false, contract_ok = false;
     bool bv_synced = false;   // cur == node values at every BOUND/VALVE node
+
+    // Step results the host reads back: divergence sum and count, the device error
+    // flag, the residual maxima (bit patterns).  Pinned, so the copies can sit in a
+    // captured graph.
+    struct Pinned {
+        double sum;
+        unsigned long long cnt;
+        int err;
+        int pad;
+        unsigned long long res[2];
+    };
+    Pinned *h_pin = nullptr;
+    unsigned long long *d_res = nullptr;
+
+    // CUDA graphs of whole steps, one per (dt, iteration counts, error flag,
+    // boundary update, layer roles); replayed by adi_step / adi_time_step / adi_run.
+    struct GraphEntry {
+        uint64_t key[4];
+        cudaGraphExec_t exec;
+        int post_ta, post_tb;
+        int64_t launches[ADI_K_NUM];
+        int64_t bytes[ADI_K_NUM];
+    };
+    std::vector<GraphEntry> graphs;
+    bool graphs_on = true;
+    cudaStream_t cap_stream = nullptr;
     std::string contract_msg;
     std::string err;
     double diff_error = 0.0;
@@ -209,6 +235,12 @@ void free_all(adi_handle *h)
         cudaFree(h->d_line_hi[d]);
         cudaFree(h->d_segs[d]);
     }
+    for (auto &g : h->graphs) cudaGraphExecDestroy(g.exec);
+    h->graphs.clear();
+    if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
+    h->cap_stream = nullptr;
+    cudaFreeHost(h->h_pin);
+    cudaFree(h->d_res);
     cudaFree(h->d_scratch);
     cudaFree(h->d_err);
     cudaFree(h->d_psum);
@@ -275,33 +307,35 @@ cudaError_t launch_fast(adi_handle *h, int dir, CLayer<R> cur, CLayer<R> tin, La
                                 h->stream);
 }
 
+// One global iteration of TimeStep (AdiSolver3D.cpp:335-357): Z (cur -> next),
+// Y (next -> half), X (half -> next), each num_local times, every sweep merging
+// into the nonlinear layer; the last X sweep merges twice (the extra merge after
+// X).  The two nonlinear buffers swap roles after every sweep.
 template <typename R>
-adi_status run_sweeps(adi_handle *h, R dt, int num_global, int num_local)
+adi_status enqueue_global_iteration(adi_handle *h, R dt, int num_local)
 {
     const DomainView<R> d = view<R>(h);
-    for (int it = 0; it < num_global; it++) {
-        const int order[3] = {2, 1, 0};
-        const int src[3] = {h->cur, h->nxt, h->half};
-        const int dst[3] = {h->nxt, h->half, h->nxt};
-        for (int q = 0; q < 3; q++) {
-            const int dir = order[q];
-            const SweepConst<R> k = sweep_const<R>(h, dir, dt);
-            // algorithmic bytes: IN rows read cur, temp and write next, temp (16
-            // values); end rows write next (4 values)
-            const int64_t bytes = (int64_t)sizeof(R) * (16 * h->num_in + 4 * (h->seg_nodes[dir] - h->num_in));
-            const int cls = dir == 0 ? ADI_K_SWEEP_X : (dir == 1 ? ADI_K_SWEEP_Y : ADI_K_SWEEP_Z);
-            for (int l = 0; l < num_local; l++) {
-                const int merges = (dir == 0 && l == num_local - 1) ? 2 : 1;
-                CK(timed(h, cls, bytes, [&] {
-                    if (h->solver == ADI_SOLVER_FAST)
-                        return launch_fast<R>(h, dir, clayer<R>(h, src[q]), clayer<R>(h, h->ta), layer<R>(h, dst[q]),
-                                              layer<R>(h, h->tb), k, merges, h->shape[dir]);
-                    return launch_sweep_exact<R>(dir, d, h->d_line_lo[dir], h->d_line_hi[dir], clayer<R>(h, src[q]),
-                                                 clayer<R>(h, h->ta), layer<R>(h, dst[q]), layer<R>(h, h->tb),
-                                                 (R *)h->d_scratch, k, merges, h->stream);
-                }));
-                std::swap(h->ta, h->tb);
-            }
+    const int order[3] = {2, 1, 0};
+    const int src[3] = {h->cur, h->nxt, h->half};
+    const int dst[3] = {h->nxt, h->half, h->nxt};
+    for (int q = 0; q < 3; q++) {
+        const int dir = order[q];
+        const SweepConst<R> k = sweep_const<R>(h, dir, dt);
+        // algorithmic bytes: IN rows read cur, temp and write next, temp (16
+        // values); end rows write next (4 values)
+        const int64_t bytes = (int64_t)sizeof(R) * (16 * h->num_in + 4 * (h->seg_nodes[dir] - h->num_in));
+        const int cls = dir == 0 ? ADI_K_SWEEP_X : (dir == 1 ? ADI_K_SWEEP_Y : ADI_K_SWEEP_Z);
+        for (int l = 0; l < num_local; l++) {
+            const int merges = (dir == 0 && l == num_local - 1) ? 2 : 1;
+            CK(timed(h, cls, bytes, [&] {
+                if (h->solver == ADI_SOLVER_FAST)
+                    return launch_fast<R>(h, dir, clayer<R>(h, src[q]), clayer<R>(h, h->ta), layer<R>(h, dst[q]),
+                                          layer<R>(h, h->tb), k, merges, h->shape[dir]);
+                return launch_sweep_exact<R>(dir, d, h->d_line_lo[dir], h->d_line_hi[dir], clayer<R>(h, src[q]),
+                                             clayer<R>(h, h->ta), layer<R>(h, dst[q]), layer<R>(h, h->tb),
+                                             (R *)h->d_scratch, k, merges, h->stream);
+            }));
+            std::swap(h->ta, h->tb);
         }
     }
     return ADI_OK;
@@ -375,8 +409,8 @@ adi_status autotune(adi_handle *h, int reps)
     return ADI_OK;
 }
 
-// Reads and clears the device error flag (the stream must be synchronised by the
-// caller's copy); ADI_ERR_TIMEOUT if a kernel's bounded wait gave up.
+// Reads and clears the device error flag; ADI_ERR_TIMEOUT if a kernel's bounded
+// wait gave up.
 adi_status check_device_flag(adi_handle *h)
 {
     int flag = 0;
@@ -389,35 +423,66 @@ adi_status check_device_flag(adi_handle *h)
     return ADI_OK;
 }
 
+// Divergence error of layer l into the pinned results, with the device error flag
+// (enqueue only).
 template <typename R>
-adi_status div_error_of(adi_handle *h, int l, double *out)
+adi_status enqueue_div_error(adi_handle *h, int l)
 {
     CK(timed(h, ADI_K_DIV_ERROR, (int64_t)h->n * (1 + 3 * (int64_t)sizeof(R)), [&] {
         return launch_div_error<R>(view<R>(h), clayer<R>(h, l), (R)h->dx, (R)h->dy, (R)h->dz, h->d_psum, h->d_pcnt,
                                    DIV_BLOCKS, h->d_sum, h->d_cnt, h->stream);
     }));
-    double sum = 0;
-    unsigned long long cnt = 0;
-    CK(cudaMemcpyAsync(&sum, h->d_sum, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(&cnt, h->d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(&h->h_pin->sum, h->d_sum, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(&h->h_pin->cnt, h->d_cnt, sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(&h->h_pin->err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    return ADI_OK;
+}
+
+// Waits for an enqueued divergence error and returns it through *out.
+adi_status read_div_error(adi_handle *h, double *out)
+{
     CK(cudaStreamSynchronize(h->stream));
-    *out = cnt ? sum / (double)cnt : 0.0;
-    return check_device_flag(h);
+    *out = h->h_pin->cnt ? h->h_pin->sum / (double)h->h_pin->cnt : 0.0;
+    if (h->h_pin->err) {
+        h->h_pin->err = 0;
+        CK(cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream));
+        return fail(h, ADI_ERR_TIMEOUT, "a sweep's bounded wait for its input tiles gave up");
+    }
+    return ADI_OK;
 }
 
 template <typename R>
-adi_status time_step(adi_handle *h, double dt, int num_global, int num_local, int compute_error, bool update_bnd)
+adi_status div_error_of(adi_handle *h, int l, double *out)
 {
-    const R dtr = (R)dt;
+    adi_status s = enqueue_div_error<R>(h, l);
+    if (s != ADI_OK) return s;
+    return read_div_error(h, out);
+}
+
+// Everything one fixed-iteration step puts on the stream: the step start (with
+// the boundary update for adi_step), num_global global iterations, and the
+// divergence error when requested.
+template <typename R>
+adi_status enqueue_step(adi_handle *h, R dt, int num_global, int num_local, int compute_error, bool update_bnd)
+{
     CK(timed(h, ADI_K_STEP_BEGIN, (int64_t)h->n * (1 + 8 * (int64_t)sizeof(R)), [&] {
         return launch_step_begin<R>(view<R>(h), layer<R>(h, h->cur), layer<R>(h, h->nxt), layer<R>(h, h->ta),
                                     layer<R>(h, h->tb), update_bnd, h->stream);
     }));
-    if (update_bnd) h->bv_synced = true;
-    adi_status s = run_sweeps<R>(h, dtr, num_global, num_local);
-    if (s != ADI_OK) return s;
+    for (int it = 0; it < num_global; it++) {
+        adi_status s = enqueue_global_iteration<R>(h, dt, num_local);
+        if (s != ADI_OK) return s;
+    }
+    if (compute_error) return enqueue_div_error<R>(h, h->nxt);
+    return ADI_OK;
+}
+
+// The host side of the end of TimeStep (AdiSolver3D.cpp:363-390): the divergence
+// value when it was computed, the guard, the layer swap.
+adi_status finish_step(adi_handle *h, int compute_error)
+{
     if (compute_error) {
-        s = div_error_of<R>(h, h->nxt, &h->diff_error);
+        adi_status s = read_div_error(h, &h->diff_error);
         if (s != ADI_OK) return s;
     }
     if (h->diff_error > 0.01) {
@@ -428,6 +493,153 @@ adi_status time_step(adi_handle *h, double dt, int num_global, int num_local, in
     std::swap(h->cur, h->nxt);
     h->bv_synced = false;   // the new state holds the sweeps' boundary values
     return ADI_OK;
+}
+
+void invalidate_graphs(adi_handle *h)
+{
+    for (auto &g : h->graphs) cudaGraphExecDestroy(g.exec);
+    h->graphs.clear();
+}
+
+// Replays (capturing on first use) the graph of one fixed-iteration step for the
+// handle's current layer roles.  Captures on the handle's private stream, so the
+// caller's stream may be the legacy default stream; the graph is launched on the
+// caller's stream.  The launch counters advance by what the graph holds.
+template <typename R>
+adi_status step_graph(adi_handle *h, R dt, int num_global, int num_local, int compute_error, bool update_bnd)
+{
+    uint64_t key[4];
+    double dd = (double)dt;
+    memcpy(&key[0], &dd, sizeof dd);
+    key[1] = (uint64_t)num_global | ((uint64_t)num_local << 20) | ((uint64_t)(compute_error != 0) << 40) |
+             ((uint64_t)update_bnd << 41) | ((uint64_t)h->bv_synced << 42);
+    key[2] = (uint64_t)h->cur | ((uint64_t)h->nxt << 4) | ((uint64_t)h->half << 8) | ((uint64_t)h->ta << 12) |
+             ((uint64_t)h->tb << 16);
+    key[3] = (uint64_t)h->stream;
+    for (auto &g : h->graphs)
+        if (!memcmp(g.key, key, sizeof key)) {
+            CK(cudaGraphLaunch(g.exec, h->stream));
+            h->ta = g.post_ta;
+            h->tb = g.post_tb;
+            for (int c = 0; c < ADI_K_NUM; c++) {
+                h->launches[c] += g.launches[c];
+                h->bytes[c] += g.bytes[c];
+            }
+            return ADI_OK;
+        }
+    adi_handle::GraphEntry ge;
+    memcpy(ge.key, key, sizeof key);
+    int64_t l0[ADI_K_NUM], b0[ADI_K_NUM];
+    memcpy(l0, h->launches, sizeof l0);
+    memcpy(b0, h->bytes, sizeof b0);
+    const int ta0 = h->ta, tb0 = h->tb;
+    const cudaStream_t user = h->stream;
+    h->stream = h->cap_stream;
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+    adi_status st = e == cudaSuccess ? enqueue_step<R>(h, dt, num_global, num_local, compute_error, update_bnd)
+                                     : fail(h, ADI_ERR_CUDA, "cudaStreamBeginCapture failed");
+    if (e == cudaSuccess) {
+        cudaError_t e2 = cudaStreamEndCapture(h->stream, &graph);
+        if (st == ADI_OK && e2 != cudaSuccess)
+            st = fail(h, ADI_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e2));
+    }
+    h->stream = user;
+    if (st == ADI_OK) {
+        e = cudaGraphInstantiate(&ge.exec, graph, 0);
+        if (e != cudaSuccess) st = fail(h, ADI_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    }
+    if (graph) cudaGraphDestroy(graph);
+    for (int c = 0; c < ADI_K_NUM; c++) {
+        ge.launches[c] = h->launches[c] - l0[c];
+        ge.bytes[c] = h->bytes[c] - b0[c];
+    }
+    ge.post_ta = h->ta;
+    ge.post_tb = h->tb;
+    if (st != ADI_OK) {
+        // nothing ran: restore the bookkeeping the capture advanced
+        memcpy(h->launches, l0, sizeof l0);
+        memcpy(h->bytes, b0, sizeof b0);
+        h->ta = ta0;
+        h->tb = tb0;
+        cudaGetLastError();
+        return st;
+    }
+    if (h->graphs.size() >= 16) {
+        cudaGraphExecDestroy(h->graphs.front().exec);
+        h->graphs.erase(h->graphs.begin());
+    }
+    h->graphs.push_back(ge);
+    // run it for this step
+    h->ta = ta0;
+    h->tb = tb0;
+    memcpy(h->launches, l0, sizeof l0);
+    memcpy(h->bytes, b0, sizeof b0);
+    return step_graph<R>(h, dt, num_global, num_local, compute_error, update_bnd);
+}
+
+template <typename R>
+adi_status time_step(adi_handle *h, double dt, int num_global, int num_local, int compute_error, bool update_bnd)
+{
+    const R dtr = (R)dt;
+    if (update_bnd) h->bv_synced = true;   // step_begin applies the boundary values first
+    adi_status s;
+    if (h->graphs_on && !h->prof_on) s = step_graph<R>(h, dtr, num_global, num_local, compute_error, update_bnd);
+    else s = enqueue_step<R>(h, dtr, num_global, num_local, compute_error, update_bnd);
+    if (s != ADI_OK) return s;
+    return finish_step(h, compute_error);
+}
+
+// Tolerance mode: global iterations until the residual max|x - t| / max|x| over
+// NODE_IN cells (x the iteration's result, t the nonlinear layer its last sweep
+// linearised about) is <= tol, at most max_global of them.  The host reads the
+// residual after each iteration, so this path runs eagerly.
+template <typename R>
+adi_status time_step_tol(adi_handle *h, double dt, int max_global, int num_local, double tol, int compute_error,
+                         bool update_bnd, int *iters_used, double *residual)
+{
+    const R dtr = (R)dt;
+    if (update_bnd) h->bv_synced = true;
+    CK(timed(h, ADI_K_STEP_BEGIN, (int64_t)h->n * (1 + 8 * (int64_t)sizeof(R)), [&] {
+        return launch_step_begin<R>(view<R>(h), layer<R>(h, h->cur), layer<R>(h, h->nxt), layer<R>(h, h->ta),
+                                    layer<R>(h, h->tb), update_bnd, h->stream);
+    }));
+    int it = 0;
+    double r = NAN;
+    while (it < max_global) {
+        adi_status s = enqueue_global_iteration<R>(h, dtr, num_local);
+        if (s != ADI_OK) return s;
+        it++;
+        // after the last X sweep the buffers swapped: tb holds the layer it read
+        CK(cudaMemsetAsync(h->d_res, 0, 2 * sizeof(unsigned long long), h->stream));
+        CK(timed(h, ADI_K_OTHER, (int64_t)h->num_in * 8 * (int64_t)sizeof(R), [&] {
+            return launch_residual<R>(view<R>(h), clayer<R>(h, h->nxt), clayer<R>(h, h->tb), h->d_res, h->stream);
+        }));
+        CK(cudaMemcpyAsync(h->h_pin->res, h->d_res, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                           h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        double dm, xm;
+        if (sizeof(R) == 4) {
+            float a, b;
+            const uint32_t ua = (uint32_t)h->h_pin->res[0], ub = (uint32_t)h->h_pin->res[1];
+            memcpy(&a, &ua, 4);
+            memcpy(&b, &ub, 4);
+            dm = a;
+            xm = b;
+        } else {
+            memcpy(&dm, &h->h_pin->res[0], 8);
+            memcpy(&xm, &h->h_pin->res[1], 8);
+        }
+        r = xm > 0 ? dm / xm : dm;
+        if (r <= tol) break;
+    }
+    if (iters_used) *iters_used = it;
+    if (residual) *residual = r;
+    if (compute_error) {
+        adi_status s = enqueue_div_error<R>(h, h->nxt);
+        if (s != ADI_OK) return s;
+    }
+    return finish_step(h, compute_error);
 }
 
 adi_status check_ready(adi_handle *h)
@@ -510,6 +722,10 @@ adi_status adi_create(const adi_grid_desc *g, const adi_fluid_params *p, adi_han
     if (e == cudaSuccess) e = alloc((void **)&h->d_pcnt, sizeof(unsigned long long) * DIV_BLOCKS);
     if (e == cudaSuccess) e = alloc((void **)&h->d_sum, sizeof(double));
     if (e == cudaSuccess) e = alloc((void **)&h->d_cnt, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = alloc((void **)&h->d_res, 2 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_pin, sizeof(adi_handle::Pinned));
+    if (e == cudaSuccess) memset(h->h_pin, 0, sizeof(adi_handle::Pinned));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess)
         for (int l = 0; l < 5 && e == cudaSuccess; l++)
             for (int v = 0; v < 4 && e == cudaSuccess; v++) e = cudaMemset(h->d_L[l][v], 0, fb);
@@ -544,6 +760,7 @@ adi_status adi_set_solver(adi_handle *h, int kind)
     if (!h) return ADI_ERR_BAD_ARG;
     if (kind != ADI_SOLVER_EXACT && kind != ADI_SOLVER_FAST) return fail(h, ADI_ERR_BAD_ARG, "unknown solver kind");
     h->solver = kind;
+    invalidate_graphs(h);
     return ADI_OK;
 }
 
@@ -590,6 +807,7 @@ adi_status adi_set_mask(adi_handle *h, const uint8_t *type, const uint8_t *bc_ve
     }
     h->mask_set = true;
     h->segs_built = false;
+    invalidate_graphs(h);
     h->bv_synced = true;   // the initial state is the node values
     return ADI_OK;
 }
@@ -598,6 +816,7 @@ adi_status adi_build_segments(adi_handle *h, adi_seg_stats *stats)
 {
     if (!h) return ADI_ERR_BAD_ARG;
     if (!h->mask_set) return fail(h, ADI_ERR_STATE, "adi_set_mask has not been called");
+    invalidate_graphs(h);
     adi_seg_stats st;
     memset(&st, 0, sizeof st);
     st.num_in = h->num_in;
@@ -655,6 +874,7 @@ adi_status adi_autotune(adi_handle *h, int reps)
 {
     if (!h || reps < 1) return ADI_ERR_BAD_ARG;
     if (!h->segs_built) return fail(h, ADI_ERR_STATE, "adi_build_segments has not been called");
+    invalidate_graphs(h);
     if (h->prec == ADI_FP64) return autotune<double>(h, reps);
     return autotune<float>(h, reps);
 }
@@ -678,6 +898,7 @@ adi_status adi_set_fast_shape(adi_handle *h, int dir, int K, int NL)
     if (!shape_ok(h, dir, s)) return fail(h, ADI_ERR_BAD_ARG, "unsupported fast-sweep shape");
     h->shape[dir] = s;
     h->tuned = true;
+    invalidate_graphs(h);
     return ADI_OK;
 }
 
@@ -736,6 +957,27 @@ adi_status adi_run(adi_handle *h, double dt, int num_global, int num_local, int 
         adi_status s = adi_step(h, dt, num_global, num_local, ce);
         if (s != ADI_OK) return s;
     }
+    return ADI_OK;
+}
+
+adi_status adi_step_tol(adi_handle *h, double dt, int max_global, int num_local, double tol, int compute_error,
+                        int *iters_used, double *residual)
+{
+    adi_status s = check_ready(h);
+    if (s != ADI_OK) return s;
+    if (max_global < 1 || num_local < 1) return fail(h, ADI_ERR_BAD_ARG, "max_global and num_local must be >= 1");
+    if (!(dt > 0) || !std::isfinite(dt)) return fail(h, ADI_ERR_BAD_ARG, "dt must be positive and finite");
+    if (!(tol >= 0)) return fail(h, ADI_ERR_BAD_ARG, "tol must be >= 0");
+    if (h->prec == ADI_FP64)
+        return time_step_tol<double>(h, dt, max_global, num_local, tol, compute_error, true, iters_used, residual);
+    return time_step_tol<float>(h, dt, max_global, num_local, tol, compute_error, true, iters_used, residual);
+}
+
+adi_status adi_set_graphs(adi_handle *h, int on)
+{
+    if (!h) return ADI_ERR_BAD_ARG;
+    h->graphs_on = on != 0;
+    if (!h->graphs_on) invalidate_graphs(h);
     return ADI_OK;
 }
 

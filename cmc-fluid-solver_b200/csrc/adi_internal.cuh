@@ -116,6 +116,10 @@ cudaError_t launch_div_error(const DomainView<R> &d, CLayer<R> l, R dx, R dy, R 
                              unsigned long long *out_cnt, cudaStream_t s);
 template <typename R>
 cudaError_t launch_fill_missing(const DomainView<R> &d, Layer<R> l, cudaStream_t s);
+// out[0] |= max |x - t|, out[1] |= max |x| over NODE_IN cells (bit patterns, atomicMax;
+// out must start at zero).
+template <typename R>
+cudaError_t launch_residual(const DomainView<R> &d, CLayer<R> x, CLayer<R> t, unsigned long long *out, cudaStream_t s);
 
 template <typename R>
 cudaError_t launch_sweep_exact(int dir, const DomainView<R> &d, const int *line_lo, const int *line_hi,

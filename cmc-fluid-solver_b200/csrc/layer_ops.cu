@@ -120,15 +120,76 @@ __global__ void div_error_partial_kernel(DomainView<R> d, CLayer<R> l, R dx, R d
     }
 }
 
+// One warp: lane l sums partials l, l+32, ... in order, then a fixed shuffle tree
+// combines the lanes, so the result does not depend on scheduling.
 __global__ void div_error_final_kernel(const double *psum, const unsigned long long *pcnt, int nblocks,
                                        double *out_sum, unsigned long long *out_cnt)
 {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        double s = 0.0;
-        unsigned long long c = 0;
-        for (int b = 0; b < nblocks; b++) { s += psum[b]; c += pcnt[b]; }
+    const int lane = threadIdx.x;
+    double s = 0.0;
+    unsigned long long c = 0;
+    for (int b = lane; b < nblocks; b += 32) {
+        s += psum[b];
+        c += pcnt[b];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+        c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    if (lane == 0) {
         *out_sum = s;
         *out_cnt = c;
+    }
+}
+
+// Nonlinear-iteration residual: the largest |x - t| and |x| over NODE_IN cells and
+// the four fields, where x is the layer a global iteration produced and t the
+// nonlinear layer its last sweep linearised about.  Each thread keeps running
+// maxima over a grid-stride range, a warp combines them with shuffles, and lane 0
+// folds them into out[0], out[1] with atomicMax on the bit patterns (non-negative
+// floating-point values order like their unsigned bit patterns; a NaN has larger
+// bits than every finite value and infinity, so it survives the reduction).
+template <typename R>
+struct Bits;
+template <>
+struct Bits<float> {
+    using T = unsigned int;
+    __device__ static T of(float x) { return __float_as_uint(x); }
+};
+template <>
+struct Bits<double> {
+    using T = unsigned long long;
+    __device__ static T of(double x) { return (unsigned long long)__double_as_longlong(x); }
+};
+
+template <typename R>
+__device__ __forceinline__ R max_keep_nan(R a, R b)
+{
+    return (b > a || b != b) ? b : a;
+}
+
+template <typename R>
+__global__ void residual_kernel(DomainView<R> d, CLayer<R> x, CLayer<R> t, unsigned long long *out)
+{
+    R dm = R(0), xm = R(0);
+    for (long long i = gtid(); i < d.n; i += gstride()) {
+        if (!code_is_in(d.code[i])) continue;
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            const R a = x.f[v][i];
+            dm = max_keep_nan(dm, fabs(a - t.f[v][i]));
+            xm = max_keep_nan(xm, fabs(a));
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        dm = max_keep_nan(dm, __shfl_xor_sync(0xffffffffu, dm, o));
+        xm = max_keep_nan(xm, __shfl_xor_sync(0xffffffffu, xm, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(out, (unsigned long long)Bits<R>::of(dm));
+        atomicMax(out + 1, (unsigned long long)Bits<R>::of(xm));
     }
 }
 
@@ -186,7 +247,16 @@ cudaError_t launch_fill_missing(const DomainView<R> &d, Layer<R> l, cudaStream_t
     return cudaGetLastError();
 }
 
+template <typename R>
+cudaError_t launch_residual(const DomainView<R> &d, CLayer<R> x, CLayer<R> t, unsigned long long *out, cudaStream_t s)
+{
+    residual_kernel<R><<<DIV_BLOCKS, 256, 0, s>>>(d, x, t, out);
+    return cudaGetLastError();
+}
+
 #define INST(R)                                                                                                  \
+    template cudaError_t launch_residual<R>(const DomainView<R> &, CLayer<R>, CLayer<R>, unsigned long long *,   \
+                                            cudaStream_t);                                                        \
     template cudaError_t launch_update_boundaries<R>(const DomainView<R> &, Layer<R>, cudaStream_t);            \
     template cudaError_t launch_step_begin<R>(const DomainView<R> &, Layer<R>, Layer<R>, Layer<R>, Layer<R>,    \
                                               bool, cudaStream_t);                                                \

@@ -151,9 +151,30 @@ adi_status adi_time_step(adi_handle *h, double dt, int num_global, int num_local
  * (FluidSolver3D.cpp:241-242). */
 adi_status adi_step(adi_handle *h, double dt, int num_global, int num_local, int compute_error);
 
-/* Runs n_steps driver-loop passes (adi_step) as one CUDA graph launch per step
- * once captured; compute_error every err_every steps (0 = never) and on the last. */
+/* Runs n_steps driver-loop passes (adi_step); compute_error every err_every steps
+ * (0 = never) and on the last, like the driver loop
+ * (FluidSolver3D.cpp:224-262) without output. */
 adi_status adi_run(adi_handle *h, double dt, int num_global, int num_local, int n_steps, int err_every);
+
+/* adi_step in tolerance mode (no counterpart in the reference's 3D solver, whose
+ * TimeStep runs a fixed num_global; its 2D solver loops on a divergence threshold,
+ * AdiSolver2D.cpp:290-314).  Global iterations run until the residual
+ *   r = max |x - t| / max |x|   over NODE_IN cells and the four fields,
+ * x the layer the iteration produced and t the nonlinear layer its last sweep
+ * linearised about, is <= tol, or max_global iterations have run.  *iters_used and
+ * *residual (either may be NULL) report the count and the last r.  The residual is
+ * a warp-shuffle max-reduction on the GPU read back after each iteration. */
+adi_status adi_step_tol(adi_handle *h, double dt, int max_global, int num_local, double tol, int compute_error,
+                        int *iters_used, double *residual);
+
+/* adi_step, adi_time_step and adi_run replay one CUDA graph per step shape (dt,
+ * iteration counts, error flag, layer roles), captured on first use on a private
+ * stream and launched on the handle's stream; a step that computes the divergence
+ * error waits for it, any other step returns without synchronising.  on = 0 issues
+ * every kernel directly instead (as does profiling, adi_set_profiling).  Graphs are
+ * rebuilt after adi_set_mask, adi_build_segments, adi_autotune, adi_set_fast_shape
+ * and adi_set_solver.  Default on. */
+adi_status adi_set_graphs(adi_handle *h, int on);
 
 /* ---- fields ------------------------------------------------------------ */
 

@@ -176,6 +176,15 @@ int oracle_step(void *vh, double dt, int num_global, int num_local, int compute_
     return step_f32(h->s, dt, num_global, num_local, compute_error, 1);
 }
 
+/* adi_step_tol's semantics (tolerance mode), for its parity tests. */
+int oracle_step_tol(void *vh, double dt, int max_global, int num_local, double tol, int compute_error, int *iters,
+                    double *res)
+{
+    oracle_h *h = (oracle_h *)vh;
+    if (h->precision == 8) return step_tol_f64(h->s, dt, max_global, num_local, tol, compute_error, iters, res);
+    return step_tol_f32(h->s, dt, max_global, num_local, tol, compute_error, iters, res);
+}
+
 /* TimeStep alone (AdiSolver3D.cpp:306-391), without UpdateBoundaries. */
 int oracle_time_step(void *vh, double dt, int num_global, int num_local, int compute_error)
 {

@@ -189,21 +189,28 @@ static void FN(merge)(FN(solver) *s, FN(layer) *src, FN(layer) *dest)
     }
 }
 
-static void FN(solve_direction)(FN(solver) *s, int dir, REAL dt, int num_local,
-                                FN(layer) *cur, FN(layer) *temp, FN(layer) *next)
+/* One local iteration of SolveDirection without its merge: every segment of the
+ * direction, four variables (AdiSolver3D.cpp:584-632). */
+static void FN(solve_segments)(FN(solver) *s, int dir, REAL dt, FN(layer) *cur, FN(layer) *temp, FN(layer) *next)
 {
     const seg_list *sl = &s->segs[dir];
     int mx = s->nx > s->ny ? s->nx : s->ny;
     mx = mx > s->nz ? mx : s->nz;
+    #pragma omp parallel num_threads(s->nthreads)
+    {
+        REAL *work = s->scratch + (size_t)omp_get_thread_num() * 5 * mx;
+        #pragma omp for schedule(static)
+        for (int q = 0; q < sl->count; q++)
+            for (int var = 0; var < 4; var++)
+                FN(solve_segment)(s, dt, work, &sl->seg[q], var, dir, cur, temp, next);
+    }
+}
+
+static void FN(solve_direction)(FN(solver) *s, int dir, REAL dt, int num_local,
+                                FN(layer) *cur, FN(layer) *temp, FN(layer) *next)
+{
     for (int it = 0; it < num_local; it++) {
-        #pragma omp parallel num_threads(s->nthreads)
-        {
-            REAL *work = s->scratch + (size_t)omp_get_thread_num() * 5 * mx;
-            #pragma omp for schedule(static)
-            for (int q = 0; q < sl->count; q++)
-                for (int var = 0; var < 4; var++)
-                    FN(solve_segment)(s, dt, work, &sl->seg[q], var, dir, cur, temp, next);
-        }
+        FN(solve_segments)(s, dir, dt, cur, temp, next);
         FN(merge)(s, next, temp);
     }
 }
@@ -268,6 +275,59 @@ static int FN(step)(FN(solver) *s, double dt_in, int num_global, int num_local, 
         FN(solve_direction)(s, 0, dt, num_local, half, temp, next);
         FN(merge)(s, next, temp);
     }
+    if (compute_error) s->diff_error = FN(div_error)(s, next);
+    if (s->diff_error > 0.01) return 1;
+    int t = s->next; s->next = s->cur; s->cur = t;
+    return 0;
+}
+
+/* Tolerance-mode residual (the library's adi_step_tol; no reference counterpart):
+ * max |x - t| and max |x| over NODE_IN cells and the four fields. */
+static void FN(residual)(FN(solver) *s, FN(layer) *x, FN(layer) *t, double *dm, double *xm)
+{
+    size_t n = (size_t)s->nx * s->ny * s->nz;
+    double a = 0.0, b = 0.0;
+    for (int v = 0; v < 4; v++)
+        for (size_t id = 0; id < n; id++)
+            if (s->type[id] == NODE_IN_) {
+                double xv = x->f[v][id], d = fabs(xv - (double)t->f[v][id]);
+                if (d > a || d != d) a = d;
+                if (fabs(xv) > b) b = fabs(xv);
+            }
+    *dm = a;
+    *xm = b;
+}
+
+/* UpdateBoundaries + TimeStep in tolerance mode: global iterations until
+ * max|x - t| / max|x| <= tol (t the nonlinear layer the last X sweep read, before
+ * its merge), at most max_global of them. */
+static int FN(step_tol)(FN(solver) *s, double dt_in, int max_global, int num_local, double tol, int compute_error,
+                        int *iters, double *res)
+{
+    REAL dt = (REAL)dt_in;
+    FN(update_boundaries)(s);
+    FN(layer) *cur = &s->L[s->cur], *next = &s->L[s->next], *half = &s->L[s->half], *temp = &s->L[s->temp];
+    FN(copy_where)(s, cur, next, NODE_BOUND_, NODE_BOUND_);
+    FN(copy_where)(s, cur, next, NODE_VALVE_, NODE_VALVE_);
+    size_t n = (size_t)s->nx * s->ny * s->nz;
+    for (int v = 0; v < 4; v++) memcpy(temp->f[v], cur->f[v], n * sizeof(REAL));
+    int it = 0;
+    double r = NAN;
+    while (it < max_global) {
+        FN(solve_direction)(s, 2, dt, num_local, cur, temp, next);
+        FN(solve_direction)(s, 1, dt, num_local, next, temp, half);
+        FN(solve_direction)(s, 0, dt, num_local - 1, half, temp, next);
+        FN(solve_segments)(s, 0, dt, half, temp, next);
+        double dm, xm;
+        FN(residual)(s, next, temp, &dm, &xm);
+        FN(merge)(s, next, temp);
+        FN(merge)(s, next, temp);
+        it++;
+        r = xm > 0 ? dm / xm : dm;
+        if (r <= tol) break;
+    }
+    *iters = it;
+    *res = r;
     if (compute_error) s->diff_error = FN(div_error)(s, next);
     if (s->diff_error > 0.01) return 1;
     int t = s->next; s->next = s->cur; s->cur = t;

@@ -70,6 +70,8 @@ def _load_oracle():
         lib.oracle_set_params.argtypes = [C.c_void_p] + [C.c_double] * 4
         lib.oracle_step.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int]
         lib.oracle_time_step.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int]
+        lib.oracle_step_tol.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int,
+                                        C.POINTER(C.c_int), C.POINTER(C.c_double)]
         lib.oracle_get_fields.argtypes = [C.c_void_p, C.c_int] + [_f64p] * 4
         lib.oracle_set_state.argtypes = [C.c_void_p] + [_f64p] * 4
         lib.oracle_div_error.restype = C.c_double
@@ -180,6 +182,13 @@ class OracleSolver:
     def time_step(self, dt, num_global, num_local, compute_error=True) -> int:
         """TimeStep without UpdateBoundaries."""
         return self.lib.oracle_time_step(self.h, dt, num_global, num_local, int(compute_error))
+
+    def step_tol(self, dt, max_global, num_local, tol, compute_error=False):
+        """Tolerance-mode step; returns (status, iterations, residual)."""
+        it, res = C.c_int(0), C.c_double(0.0)
+        rc = self.lib.oracle_step_tol(self.h, dt, max_global, num_local, tol, int(compute_error), C.byref(it),
+                                      C.byref(res))
+        return rc, it.value, res.value
 
     def fields(self, which=0):
         out = [np.zeros(self.shape, np.float64) for _ in range(4)]

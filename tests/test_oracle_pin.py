@@ -109,3 +109,22 @@ def test_fp64_oracle_tracks_fp32():
     for fa, fb in zip(a.fields(), b.fields()):
         scale = np.max(np.abs(fb[m]))
         assert np.max(np.abs(fa[m] - fb[m])) <= 1e-5 * scale
+
+
+def test_oracle_tolerance_mode_consistent():
+    """The oracle's tolerance-mode step: tol = 0 runs max_global iterations and equals
+    the fixed-iteration step; a loose tol stops after one; residuals shrink."""
+    d = G.random_domain(16, 14, 18, seed=31, shell=True, n_obstacles=5)
+    a = O.OracleSolver(d, precision=8, Re=150.0, Pr=0.72, lam=1.4)
+    b = O.OracleSolver(d, precision=8, Re=150.0, Pr=0.72, lam=1.4)
+    rc, it, r3 = a.step_tol(6e-4, 3, 2, 0.0, True)
+    assert (rc, it) == (0, 3)
+    assert b.step(6e-4, 3, 2, True) == 0
+    for f in range(4):
+        assert np.array_equal(a.fields(0)[f], b.fields(0)[f])
+    r1 = O.OracleSolver(d, precision=8, Re=150.0, Pr=0.72, lam=1.4).step_tol(6e-4, 1, 2, 0.0, False)[2]
+    r2 = O.OracleSolver(d, precision=8, Re=150.0, Pr=0.72, lam=1.4).step_tol(6e-4, 2, 2, 0.0, False)[2]
+    assert r3 < r2 < r1
+    e = O.OracleSolver(d, precision=8, Re=150.0, Pr=0.72, lam=1.4)
+    rc, it, r = e.step_tol(6e-4, 5, 2, r1 * 1.01, False)
+    assert (rc, it) == (0, 1) and r == r1
