@@ -62,6 +62,11 @@ def _spheres64():
     return G.spheres_channel(n=64, n_spheres=10, rmin=3.0, rmax=7.0, seed=0)
 
 
+def _batched64():
+    return G.batch_of_domains(n_domains=64, seed=2, size_lo=64, size_hi=160, spheres=(10, 60), rmin=4.0, rmax=12.0,
+                              re=(50.0, 400.0))
+
+
 CONFIGS = {
     "spheres128": dict(make=_spheres128, Re=200.0, Pr=0.72, lam=1.4, dt=5e-4, ng=4, nl=2,
                        desc="plain 3D ADI forward: 128^3 FP32 box, 40 solid spheres (radii U[4,12], "
@@ -71,6 +76,10 @@ CONFIGS = {
                           desc="large 3D single domain: 384^3 FP32, 300 solid ellipsoids (semi-axes "
                                "U[3,20], seed 1) plus a thin-walled tube along x, Re=500, dt=2e-4, "
                                "num_global=4, num_local=2"),
+    "batched64": dict(make=_batched64, batch=True, Pr=0.72, lam=1.4, dt=5e-4, ng=4, nl=2,
+                      desc="batched: 64 independent 3D FP32 domains, axes U{64..160} (seed 2), 10-60 solid spheres "
+                           "each (radii U[4,12]), Re U[50,400], dt=5e-4, num_global=4, num_local=2; all domains "
+                           "in one persistent launch per sweep, step replayed as a CUDA graph"),
     "spheres64": dict(make=_spheres64, Re=200.0, Pr=0.72, lam=1.4, dt=5e-4, ng=4, nl=2,
                       desc="small case for profiling: 64^3 FP32, 10 spheres, Re=200, dt=5e-4, "
                            "num_global=4, num_local=2"),
@@ -203,6 +212,21 @@ def run_reference(args):
     if rank != 0:
         return 0
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+    if cfg.get("batch"):
+        domains = cfg["make"]()
+        with stdout_to_stderr():
+            value, done, el = cpu_reference_batch(domains, cfg, args.ref_budget)
+        cores = int(os.environ["OMP_NUM_THREADS"])
+        sample = f"one step of each of the first {done} of {len(domains)} domains ({el:.1f} s), OpenMP {cores} threads"
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+            "steps": 1, "warmup": 0, "ms_per_step": 1e3 * el, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{args.config}: {cfg['desc']}", "cells": sum(d.cells for d in domains)},
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }), flush=True)
+        return 0
     d = cfg["make"]()
     # warm-up steps are part of the sample budget too (first-touch of the layers)
     with stdout_to_stderr():
@@ -370,6 +394,185 @@ def run_ours(args):
     return 0
 
 
+def cpu_reference_batch(domains, cfg, budget_s: float):
+    """The reference CPU solver stepping the batch's domains one after another, one
+    step each, until budget_s has passed.  Returns (cell-steps/s, domains stepped, s)."""
+    import oracle as O
+    if not O.have_ref():
+        O.build()
+    done, cells, el = 0, 0, 0.0
+    for d in domains:
+        ref = O.RefSolver(d, Re=d.meta["Re"], Pr=cfg["Pr"], lam=cfg["lam"])
+        t0 = time.perf_counter()
+        ref.step(cfg["dt"], cfg["ng"], cfg["nl"], True)
+        el += time.perf_counter() - t0
+        ref.close()
+        done += 1
+        cells += d.cells
+        if el > budget_s:
+            break
+    return cells / el, done, el
+
+
+def run_batch(args):
+    """Batched workload: every rank steps its LPT share of the domains as one batch;
+    value = all ranks' cell-steps / max-over-ranks device time."""
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    import adi_b200
+    from adi_b200.partition import domain_cost, lpt_partition, part_loads
+    cfg = CONFIGS[args.config]
+    domains = cfg["make"]()
+    costs = [domain_cost(d.shape, cfg["ng"]) for d in domains]
+    parts = lpt_partition(costs, world)
+    mine = [domains[i] for i in parts[rank]]
+    stream = torch.cuda.current_stream()
+    dt, ng, nl = cfg["dt"], cfg["ng"], cfg["nl"]
+    members, stats = [], []
+    for d in mine:
+        m = adi_b200.AdiSolver3D(d, Re=d.meta["Re"], Pr=cfg["Pr"], lam=cfg["lam"], precision=adi_b200.ADI_FP32,
+                                 solver=adi_b200.ADI_SOLVER_EXACT, stream=stream.cuda_stream)
+        stats.append(m.CreateSegments())
+        members.append(m)
+    batch = adi_b200.AdiBatch(members, stream=stream.cuda_stream)
+    batch.autotune(dt, 2)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def one_step(i):
+        rc = batch.step(dt, ng, nl, i % 10 == 0)
+        if rc != 0:
+            raise RuntimeError(f"adi_batch_step failed with status {rc}")
+
+    for i in range(args.warmup):
+        one_step(i)
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = batch.launches()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier()
+    for i in range(args.steps):
+        flush.zero_()
+        ev[i][0].record(stream)
+        one_step(i)
+        ev[i][1].record(stream)
+    barrier()
+    launches = batch.launches() - l0
+    total_ms = float(sum(a.elapsed_time(b) for a, b in ev))
+    sweep_ms = batch.time_sweeps(dt, 3)
+    clk = clocks.stop()
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    all_cells = sum(d.cells for d in domains)
+    value = all_cells * args.steps / (total_ms / 1e3)
+
+    # ---- end to end through the C ABI with host buffers (every member's state) ----
+    pinned = [[torch.empty(m.shape, dtype=torch.float32, pin_memory=True).numpy() for _ in range(4)] for m in members]
+    for m, pb in zip(members, pinned):
+        for a, b in zip(pb, m.fields(0)):
+            a[...] = b
+    e2e_steps = max(1, min(args.steps, 3))
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(e2e_steps):
+        for m, pb in zip(members, pinned):
+            m.set_state(*pb)
+        one_step(1)
+        for m, pb in zip(members, pinned):
+            m._check(m.lib.adi_get_state(m.h, 0, *[p.ctypes.data for p in pb]))
+    e1.record(stream)
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = all_cells * e2e_steps / (e2e_ms / 1e3)
+    my_cells = sum(d.cells for d in mine)
+
+    # ---- roofline: the batched sweep, algorithmic bytes per launch / its time ----
+    sweep_bytes = [sum(4 * (16 * st["num_in"] + 4 * (st["num_nodes"][dr] - st["num_in"])) for st in stats)
+                   for dr in range(3)]
+    achieved = sum(sweep_bytes) / (sum(sweep_ms) / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+
+    # ---- the same domains stepped one at a time (plain per-domain steps) ----
+    plain = None
+    if world == 1 and not args.no_plain_loop:
+        for m in members:
+            m._check(m.lib.adi_set_solver(m.h, adi_b200.ADI_SOLVER_FAST))
+            m.autotune(1)
+        for i in range(2):
+            for m in members:
+                m.step(dt, ng, nl, False)
+        barrier()
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        psteps = max(1, min(args.steps, 5))
+        p0.record(stream)
+        for i in range(psteps):
+            for m in members:
+                rc = m.step(dt, ng, nl, i % 10 == 0)
+                if rc != 0:
+                    raise RuntimeError(f"adi_step failed with status {rc}")
+        p1.record(stream)
+        barrier()
+        plain = {"value": my_cells * psteps / (p0.elapsed_time(p1) / 1e3), "unit": METRIC, "steps": psteps,
+                 "how": "the same domains, adi_step one domain at a time, each with its own autotuned fast shapes"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{args.config}: {cfg['desc']}", "cells": all_cells, "domains": len(domains),
+                   "domains_this_rank": len(mine), "chunk_K_xyz": batch.chunks(),
+                   "parallelism": (f"domains LPT-sharded over {world} ranks (loads "
+                                   f"{[int(x) for x in part_loads(costs, parts)]})" if world > 1 else "one batch"),
+                   "l2": "flushed between steps (256 MiB memset, excluded from the time); working set far above L2"},
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 16 * my_cells,
+                "d2h_bytes_per_step": 16 * my_cells, "steps": e2e_steps},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if peak else None, "traffic": ncu_traffic(args.config,
+                                                                                     "sweep_fast_batch_kernel"),
+                     "kernel": "sweep_fast_batch_kernel", "peak_source": peak_kind,
+                     "per_direction_ms_per_launch": sweep_ms,
+                     "algorithmic_bytes_per_launch": sweep_bytes},
+        "plain_per_domain": plain,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+        with stdout_to_stderr():
+            v, done, el = cpu_reference_batch(domains, cfg, args.cpu_budget)
+        line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": int(os.environ["OMP_NUM_THREADS"]),
+                                "kind": "reference",
+                                "sample": f"one step of each of the first {done} domains ({el:.1f} s) on the "
+                                          f"reference CPU solver, OpenMP {os.environ['OMP_NUM_THREADS']} threads"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    batch.close()
+    for m in members:
+        m.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -381,6 +584,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of reference CPU time for cpu_baseline")
     ap.add_argument("--ref-budget", type=float, default=120.0, help="seconds cap for --impl reference")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain-loop", action="store_true",
+                    help="batched configs: skip timing the same domains stepped one at a time")
     ap.add_argument("--shapes", default=None,
                     help='fast sweep shapes "K,NL;K,NL;K,NL" for X;Y;Z instead of the autotuned ones '
                          '(profiling runs pin them: timings under a profiler mislead the autotuner)')
@@ -389,6 +594,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if CONFIGS[args.config].get("batch"):
+        return run_batch(args)
     return run_ours(args)
 
 

@@ -15,7 +15,7 @@ from . import _abi
 from ._abi import ADI_FP32, ADI_FP64, ADI_SOLVER_EXACT, ADI_SOLVER_FAST, AdiError  # noqa: F401
 
 __all__ = ["AdiSolver3D", "AdiError", "fluid_params_normalized", "ADI_FP32", "ADI_FP64",
-           "ADI_SOLVER_EXACT", "ADI_SOLVER_FAST", "library_path"]
+           "ADI_SOLVER_EXACT", "ADI_SOLVER_FAST", "library_path", "AdiBatch"]
 
 
 def library_path() -> str:
@@ -172,3 +172,83 @@ class AdiSolver3D:
         arr = (C.c_void_p * 8)()
         self._check(self.lib.adi_device_pointers(self.h, C.byref(arr)))
         return [arr[i] for i in range(8)]
+
+
+class AdiBatch:
+    """Many domains stepped together (adi_batch_*): one launch per sweep over all
+    members, the step replayed as a CUDA graph.  Keeps its member solvers alive."""
+
+    def __init__(self, solvers, stream=None):
+        self.lib = _abi.load()
+        self.members = list(solvers)
+        n = len(self.members)
+        arr = (C.c_void_p * n)(*[s.h.value for s in self.members])
+        self.b = C.c_void_p()
+        rc = self.lib.adi_batch_create(arr, n, C.byref(self.b))
+        if rc != _abi.ADI_OK:
+            msgs = [self.lib.adi_last_error_string(s.h) for s in self.members]
+            raise _abi.AdiError(rc, "; ".join(m.decode() for m in msgs if m))
+        if stream is not None:
+            handle = stream if isinstance(stream, int) else getattr(stream, "cuda_stream", stream)
+            self._check(self.lib.adi_batch_set_stream(self.b, C.c_void_p(handle)))
+
+    def _check(self, status):
+        if status != _abi.ADI_OK:
+            raw = self.lib.adi_batch_last_error_string(self.b) if self.b else b""
+            raise _abi.AdiError(status, raw.decode() if raw else "")
+
+    def step(self, dt, num_global, num_local, compute_error=False) -> int:
+        """One step of every member; returns the raw status (0 = OK)."""
+        return self.lib.adi_batch_step(self.b, dt, num_global, num_local, int(compute_error))
+
+    def last_error(self) -> str:
+        raw = self.lib.adi_batch_last_error_string(self.b)
+        return raw.decode() if raw else ""
+
+    def div_errors(self) -> np.ndarray:
+        out = np.zeros(len(self.members), np.float64)
+        self._check(self.lib.adi_batch_div_errors(self.b, out.ctypes.data))
+        return out
+
+    def set_chunk(self, direction: int, K: int):
+        self._check(self.lib.adi_batch_set_chunk(self.b, direction, K))
+
+    def chunks(self):
+        out = []
+        for dr in range(3):
+            k = C.c_int()
+            self._check(self.lib.adi_batch_get_chunk(self.b, dr, C.byref(k)))
+            out.append(k.value)
+        return out
+
+    def autotune(self, dt: float, reps: int = 3):
+        self._check(self.lib.adi_batch_autotune(self.b, dt, reps))
+
+    def set_graphs(self, on: bool):
+        self._check(self.lib.adi_batch_set_graphs(self.b, int(on)))
+
+    def launches(self) -> int:
+        v = C.c_int64()
+        self._check(self.lib.adi_batch_launches(self.b, C.byref(v)))
+        return v.value
+
+    def time_sweeps(self, dt: float, reps: int = 3):
+        """Mean ms of one batched sweep launch per direction X, Y, Z."""
+        out = np.zeros(3, np.float32)
+        self._check(self.lib.adi_batch_time_sweeps(self.b, dt, reps, out.ctypes.data))
+        return [float(x) for x in out]
+
+    @property
+    def cells(self) -> int:
+        return int(sum(int(np.prod(s.shape)) for s in self.members))
+
+    def close(self):
+        if self.b:
+            self.lib.adi_batch_destroy(self.b)
+            self.b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

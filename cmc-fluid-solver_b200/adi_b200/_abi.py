@@ -18,6 +18,7 @@ STATUS_NAMES = {
     4: "ADI_ERR_NOT_CONVERGED", 5: "ADI_ERR_CUDA", 6: "ADI_ERR_TIMEOUT", 7: "ADI_ERR_DIVERGENCE",
     8: "ADI_ERR_STATE", 9: "ADI_ERR_NO_DEVICE",
 }
+globals().update({name: code for code, name in STATUS_NAMES.items()})
 ADI_FP32, ADI_FP64 = 4, 8
 ADI_SOLVER_EXACT, ADI_SOLVER_FAST = 0, 1
 
@@ -29,6 +30,9 @@ EXPORTED = [
     "adi_set_state", "adi_get_layer", "adi_div_error", "adi_device_pointers", "adi_version",
     "adi_set_profiling", "adi_get_profile", "adi_get_fast_shape", "adi_set_fast_shape", "adi_autotune",
     "adi_sweep_exact_static", "adi_static_scratch_bytes", "adi_step_tol", "adi_set_graphs",
+    "adi_batch_create", "adi_batch_destroy", "adi_batch_set_stream", "adi_batch_step", "adi_batch_div_errors",
+    "adi_batch_set_chunk", "adi_batch_get_chunk", "adi_batch_autotune", "adi_batch_set_graphs",
+    "adi_batch_launches", "adi_batch_last_error_string", "adi_batch_time_sweeps",
 ]
 
 K_NUM = 7
@@ -96,6 +100,17 @@ def load() -> C.CDLL:
         "adi_run": [vp, d, i, i, i, i],
         "adi_step_tol": [vp, d, i, i, d, i, C.POINTER(i), C.POINTER(d)],
         "adi_set_graphs": [vp, i],
+        "adi_batch_create": [vp, i, C.POINTER(vp)],
+        "adi_batch_destroy": [vp],
+        "adi_batch_set_stream": [vp, vp],
+        "adi_batch_step": [vp, d, i, i, i],
+        "adi_batch_div_errors": [vp, vp],
+        "adi_batch_set_chunk": [vp, i, i],
+        "adi_batch_get_chunk": [vp, i, C.POINTER(i)],
+        "adi_batch_autotune": [vp, d, i],
+        "adi_batch_set_graphs": [vp, i],
+        "adi_batch_launches": [vp, C.POINTER(C.c_int64)],
+        "adi_batch_time_sweeps": [vp, d, i, vp],
         "adi_get_state": [vp, i, vp, vp, vp, vp],
         "adi_set_state": [vp, vp, vp, vp, vp],
         "adi_get_layer": [vp, i, i, i, vp, vp],
@@ -114,6 +129,8 @@ def load() -> C.CDLL:
         f.restype = C.c_int
     lib.adi_last_error_string.argtypes = [vp]
     lib.adi_last_error_string.restype = C.c_char_p
+    lib.adi_batch_last_error_string.argtypes = [vp]
+    lib.adi_batch_last_error_string.restype = C.c_char_p
     lib.adi_version.argtypes = []
     lib.adi_version.restype = C.c_char_p
     lib.adi_static_scratch_bytes.argtypes = []

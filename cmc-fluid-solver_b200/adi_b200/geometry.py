@@ -157,6 +157,25 @@ def spheres_channel(n: int = 128, n_spheres: int = 40, rmin: float = 4.0, rmax: 
     return d
 
 
+def batch_of_domains(n_domains: int = 64, seed: int = 2, size_lo: int = 64, size_hi: int = 160,
+                     spheres=(10, 60), rmin: float = 4.0, rmax: float = 12.0, re=(50.0, 400.0)):
+    """Batched workload: n_domains independent sphere channels, each axis uniform in
+    {size_lo..size_hi}, a sphere count uniform in spheres[0]..spheres[1] (radii
+    U[rmin, rmax]), Reynolds number U[re]; all drawn from default_rng(seed).  Each
+    domain's Re is in its meta["Re"]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_domains):
+        dims = tuple(int(x) for x in rng.integers(size_lo, size_hi + 1, size=3))
+        ns = int(rng.integers(spheres[0], spheres[1] + 1))
+        Re = float(rng.uniform(*re))
+        sub = int(rng.integers(0, 2**31 - 1))
+        d = spheres_channel(dims=dims, n_spheres=ns, rmin=rmin, rmax=rmax, seed=sub)
+        d.meta.update(kind="batch_member", Re=Re)
+        out.append(d)
+    return out
+
+
 def ellipsoids_tube(n: int = 384, n_ellipsoids: int = 300, amin: float = 3.0, amax: float = 20.0,
                     seed: int = 1, inflow_u: float = 1.0, T_solid: float = 1.2, shell: bool = True) -> Domain:
     """Large 3D workload: n^3 box with `n_ellipsoids` solid ellipsoids (semi-axes

@@ -16,6 +16,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <new>
 #include <string>
 #include <vector>
@@ -1089,6 +1090,465 @@ adi_status adi_device_pointers(adi_handle *h, void *out8[8])
     }
     h->bv_synced = false;   // the caller may write the state through these
     return ADI_OK;
+}
+
+} // extern "C"
+
+// ===========================================================================
+// Batches: many independent domains stepped together, one persistent launch per
+// sweep direction over every domain's lines, the whole step replayed as a graph.
+// ===========================================================================
+
+struct adi_batch {
+    int prec = ADI_FP32;
+    std::vector<adi_handle *> hs;
+    cudaStream_t stream = nullptr, cap_stream = nullptr;
+    void *d_doms = nullptr;                 // BatchDomain<R>[n]
+    std::vector<unsigned char> host_doms;   // its host image
+    int2 *d_items[3] = {};
+    int nitems[3] = {0, 0, 0};
+    int K[3] = {4, 4, 4};
+    int grid[3] = {0, 0, 0};
+    long long max_cells = 0;
+    double dt_loaded = NAN;                 // dt the uploaded sweep constants are for
+    double *d_psum = nullptr, *d_sum = nullptr;
+    unsigned long long *d_pcnt = nullptr, *d_cnt = nullptr;
+    double *h_sum = nullptr;                // pinned, n each
+    unsigned long long *h_cnt = nullptr;
+    std::vector<double> diff_error;
+    bool graphs_on = true;
+    struct GraphEntry {
+        uint64_t key[4];
+        cudaGraphExec_t exec;
+        int post_ta, post_tb;
+    };
+    std::vector<GraphEntry> graphs;
+    int64_t launches = 0;
+    std::string err;
+};
+
+namespace {
+
+constexpr int BATCH_DIV_BLOCKS = 32;
+
+adi_status bfail(adi_batch *b, adi_status s, const std::string &m)
+{
+    if (b) b->err = m;
+    return s;
+}
+
+#define BCK(call)                                                                                      \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess)                                                                         \
+            return bfail(b, ADI_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));        \
+    } while (0)
+
+void batch_invalidate(adi_batch *b)
+{
+    for (auto &g : b->graphs) cudaGraphExecDestroy(g.exec);
+    b->graphs.clear();
+}
+
+// Host image of every domain's BatchDomain and the per-direction work lists.
+template <typename R>
+adi_status batch_build(adi_batch *b)
+{
+    const int n = (int)b->hs.size();
+    b->host_doms.assign(sizeof(BatchDomain<R>) * n, 0);
+    BatchDomain<R> *bd = reinterpret_cast<BatchDomain<R> *>(b->host_doms.data());
+    std::vector<std::pair<long long, int2>> items[3];
+    b->max_cells = 0;
+    for (int q = 0; q < n; q++) {
+        adi_handle *h = b->hs[q];
+        bd[q].d = view<R>(h);
+        for (int l = 0; l < 5; l++)
+            for (int v = 0; v < 4; v++) bd[q].L[l][v] = (R *)h->d_L[l][v];
+        bd[q].dx = h->dx;
+        bd[q].dy = h->dy;
+        bd[q].dz = h->dz;
+        bd[q].vec_ok = (h->nz % (16 / (int)sizeof(R))) == 0;
+        b->max_cells = std::max(b->max_cells, h->n);
+        for (int dir = 0; dir < 3; dir++) {
+            bd[q].lo[dir] = h->d_line_lo[dir];
+            bd[q].hi[dir] = h->d_line_hi[dir];
+            const LineGeom g = line_geom(dir, h->nx, h->ny, h->nz);
+            const int P = (g.len + b->K[dir] - 1) / b->K[dir];
+            if (P > 256) return bfail(b, ADI_ERR_CAPACITY, "a domain's lines are too long for the batched sweep");
+            const int NL = std::max(1, 256 / P);
+            bd[q].P[dir] = P;
+            bd[q].NL[dir] = NL;
+            for (int l0 = 0; l0 < g.nlines; l0 += NL)
+                items[dir].push_back({(long long)P * b->K[dir] * NL, make_int2(q, l0)});
+        }
+    }
+    for (int dir = 0; dir < 3; dir++) {
+        // longest items first (LPT order over the persistent CTAs)
+        std::stable_sort(items[dir].begin(), items[dir].end(),
+                         [](const std::pair<long long, int2> &a, const std::pair<long long, int2> &c) {
+                             return a.first > c.first;
+                         });
+        std::vector<int2> w(items[dir].size());
+        for (size_t i = 0; i < w.size(); i++) w[i] = items[dir][i].second;
+        cudaFree(b->d_items[dir]);
+        b->d_items[dir] = nullptr;
+        b->nitems[dir] = (int)w.size();
+        if (!w.empty()) {
+            BCK(cudaMalloc((void **)&b->d_items[dir], sizeof(int2) * w.size()));
+            BCK(cudaMemcpy(b->d_items[dir], w.data(), sizeof(int2) * w.size(), cudaMemcpyHostToDevice));
+        }
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        b->grid[dir] = std::max(1, std::min(b->nitems[dir], sms * (b->K[dir] == 4 ? 2 : 1)));
+    }
+    if (!b->d_doms) BCK(cudaMalloc(&b->d_doms, b->host_doms.size()));
+    b->dt_loaded = NAN;
+    batch_invalidate(b);
+    return ADI_OK;
+}
+
+// Sweep constants of every domain for dt, uploaded when dt changes.
+template <typename R>
+adi_status batch_load_dt(adi_batch *b, double dt)
+{
+    if (dt == b->dt_loaded) return ADI_OK;
+    BatchDomain<R> *bd = reinterpret_cast<BatchDomain<R> *>(b->host_doms.data());
+    for (size_t q = 0; q < b->hs.size(); q++) {
+        b->hs[q]->bv_synced = true;   // the batched step always applies the boundary values first
+        for (int dir = 0; dir < 3; dir++) bd[q].kc[dir] = sweep_const<R>(b->hs[q], dir, (R)dt);
+    }
+    BCK(cudaStreamSynchronize(b->stream));
+    BCK(cudaMemcpy(b->d_doms, b->host_doms.data(), b->host_doms.size(), cudaMemcpyHostToDevice));
+    b->dt_loaded = dt;
+    batch_invalidate(b);
+    return ADI_OK;
+}
+
+template <typename R>
+adi_status batch_enqueue(adi_batch *b, int num_global, int num_local, int compute_error, int &ta, int &tb)
+{
+    const adi_handle *h0 = b->hs[0];
+    const int n = (int)b->hs.size();
+    const BatchDomain<R> *doms = (const BatchDomain<R> *)b->d_doms;
+    BCK(launch_step_begin_batch<R>(doms, n, b->max_cells, h0->cur, h0->nxt, ta, tb, true, b->stream));
+    b->launches++;
+    const int order[3] = {2, 1, 0};
+    const int src[3] = {h0->cur, h0->nxt, h0->half};
+    const int dst[3] = {h0->nxt, h0->half, h0->nxt};
+    for (int it = 0; it < num_global; it++)
+        for (int q = 0; q < 3; q++) {
+            const int dir = order[q];
+            for (int l = 0; l < num_local; l++) {
+                const int merges = (dir == 0 && l == num_local - 1) ? 2 : 1;
+                BCK(launch_sweep_fast_batch<R>(dir, b->K[dir], doms, b->d_items[dir], b->nitems[dir], b->grid[dir],
+                                               src[q], ta, dst[q], tb, merges, b->stream));
+                b->launches += b->nitems[dir] > 0;
+                std::swap(ta, tb);
+            }
+        }
+    if (compute_error) {
+        BCK(launch_div_error_batch<R>(doms, n, h0->nxt, BATCH_DIV_BLOCKS, b->d_psum, b->d_pcnt, b->d_sum, b->d_cnt,
+                                      b->stream));
+        b->launches += 2;
+        BCK(cudaMemcpyAsync(b->h_sum, b->d_sum, sizeof(double) * n, cudaMemcpyDeviceToHost, b->stream));
+        BCK(cudaMemcpyAsync(b->h_cnt, b->d_cnt, sizeof(unsigned long long) * n, cudaMemcpyDeviceToHost, b->stream));
+    }
+    return ADI_OK;
+}
+
+template <typename R>
+adi_status batch_step(adi_batch *b, double dt, int num_global, int num_local, int compute_error)
+{
+    adi_status s = batch_load_dt<R>(b, dt);
+    if (s != ADI_OK) return s;
+    adi_handle *h0 = b->hs[0];
+    int ta = h0->ta, tb = h0->tb;
+    if (b->graphs_on) {
+        uint64_t key[4] = {0, 0, 0, 0};
+        memcpy(&key[0], &dt, sizeof dt);
+        key[1] = (uint64_t)num_global | ((uint64_t)num_local << 20) | ((uint64_t)(compute_error != 0) << 40);
+        key[2] = (uint64_t)h0->cur | ((uint64_t)h0->nxt << 4) | ((uint64_t)h0->half << 8) | ((uint64_t)ta << 12) |
+                 ((uint64_t)tb << 16);
+        key[3] = (uint64_t)b->stream;
+        adi_batch::GraphEntry *ge = nullptr;
+        for (auto &g : b->graphs)
+            if (!memcmp(g.key, key, sizeof key)) ge = &g;
+        if (!ge) {
+            adi_batch::GraphEntry e;
+            memcpy(e.key, key, sizeof key);
+            const cudaStream_t user = b->stream;
+            const int64_t l0 = b->launches;
+            b->stream = b->cap_stream;
+            cudaGraph_t graph = nullptr;
+            BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+            int ta2 = ta, tb2 = tb;
+            s = batch_enqueue<R>(b, num_global, num_local, compute_error, ta2, tb2);
+            cudaError_t ec = cudaStreamEndCapture(b->stream, &graph);
+            b->stream = user;
+            b->launches = l0;
+            if (s != ADI_OK) {
+                if (graph) cudaGraphDestroy(graph);
+                return s;
+            }
+            if (ec != cudaSuccess) return bfail(b, ADI_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(ec));
+            cudaError_t ei = cudaGraphInstantiate(&e.exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (ei != cudaSuccess) return bfail(b, ADI_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(ei));
+            e.post_ta = ta2;
+            e.post_tb = tb2;
+            if (b->graphs.size() >= 8) {
+                cudaGraphExecDestroy(b->graphs.front().exec);
+                b->graphs.erase(b->graphs.begin());
+            }
+            b->graphs.push_back(e);
+            ge = &b->graphs.back();
+        }
+        BCK(cudaGraphLaunch(ge->exec, b->stream));
+        b->launches += 1 + (int64_t)num_global * num_local * 3 + (compute_error ? 2 : 0);
+        ta = ge->post_ta;
+        tb = ge->post_tb;
+    } else {
+        s = batch_enqueue<R>(b, num_global, num_local, compute_error, ta, tb);
+        if (s != ADI_OK) return s;
+    }
+    const int n = (int)b->hs.size();
+    bool diverged = false;
+    if (compute_error) {
+        BCK(cudaStreamSynchronize(b->stream));
+        for (int q = 0; q < n; q++) b->diff_error[q] = b->h_cnt[q] ? b->h_sum[q] / (double)b->h_cnt[q] : 0.0;
+    }
+    for (int q = 0; q < n; q++) diverged |= b->diff_error[q] > 0.01;
+    for (int q = 0; q < n; q++) {
+        adi_handle *h = b->hs[q];
+        h->ta = ta;
+        h->tb = tb;
+        h->diff_error = b->diff_error[q];
+        if (!diverged) {
+            std::swap(h->cur, h->nxt);
+            h->bv_synced = false;
+        }
+    }
+    if (diverged) return bfail(b, ADI_ERR_DIVERGENCE, "a domain's divergence error is above 0.01; no domain advanced");
+    return ADI_OK;
+}
+
+void batch_free(adi_batch *b)
+{
+    batch_invalidate(b);
+    if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+    cudaFree(b->d_doms);
+    for (int d = 0; d < 3; d++) cudaFree(b->d_items[d]);
+    cudaFree(b->d_psum);
+    cudaFree(b->d_pcnt);
+    cudaFree(b->d_sum);
+    cudaFree(b->d_cnt);
+    cudaFreeHost(b->h_sum);
+    cudaFreeHost(b->h_cnt);
+}
+
+} // namespace
+
+extern "C" {
+
+adi_status adi_batch_create(adi_handle *const *handles, int n, adi_batch **out)
+{
+    if (!handles || n < 1 || !out) return ADI_ERR_BAD_ARG;
+    *out = nullptr;
+    adi_handle *h0 = handles[0];
+    for (int q = 0; q < n; q++) {
+        adi_handle *h = handles[q];
+        if (!h) return ADI_ERR_BAD_ARG;
+        adi_status s = check_ready(h);
+        if (s != ADI_OK) return s;
+        if (h->prec != h0->prec || h->device != h0->device)
+            return fail(h, ADI_ERR_BAD_ARG, "batch members must share precision and device");
+        if (h->cur != h0->cur || h->nxt != h0->nxt || h->half != h0->half || h->ta != h0->ta || h->tb != h0->tb)
+            return fail(h, ADI_ERR_STATE, "batch members must have stepped in lock step (same layer roles)");
+        for (int r = 0; r < q; r++)
+            if (handles[r] == h) return fail(h, ADI_ERR_BAD_ARG, "a handle appears twice in the batch");
+    }
+    adi_batch *b = new (std::nothrow) adi_batch();
+    if (!b) return ADI_ERR_CAPACITY;
+    b->prec = h0->prec;
+    b->hs.assign(handles, handles + n);
+    b->stream = h0->stream;
+    b->diff_error.assign(n, 0.0);
+    for (int q = 0; q < n; q++) b->diff_error[q] = handles[q]->diff_error;
+    cudaError_t e = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_psum, sizeof(double) * BATCH_DIV_BLOCKS * n);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_pcnt, sizeof(unsigned long long) * BATCH_DIV_BLOCKS * n);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_sum, sizeof(double) * n);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_cnt, sizeof(unsigned long long) * n);
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&b->h_sum, sizeof(double) * n);
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&b->h_cnt, sizeof(unsigned long long) * n);
+    adi_status s = e == cudaSuccess ? ADI_OK : ADI_ERR_CUDA;
+    if (s == ADI_OK) s = b->prec == ADI_FP64 ? batch_build<double>(b) : batch_build<float>(b);
+    if (s != ADI_OK) {
+        batch_free(b);
+        delete b;
+        cudaGetLastError();
+        return s;
+    }
+    *out = b;
+    return ADI_OK;
+}
+
+adi_status adi_batch_destroy(adi_batch *b)
+{
+    if (!b) return ADI_OK;
+    cudaStreamSynchronize(b->stream);
+    batch_free(b);
+    delete b;
+    return ADI_OK;
+}
+
+adi_status adi_batch_set_stream(adi_batch *b, void *stream)
+{
+    if (!b) return ADI_ERR_BAD_ARG;
+    b->stream = (cudaStream_t)stream;
+    for (auto *h : b->hs) h->stream = b->stream;
+    return ADI_OK;
+}
+
+adi_status adi_batch_set_graphs(adi_batch *b, int on)
+{
+    if (!b) return ADI_ERR_BAD_ARG;
+    b->graphs_on = on != 0;
+    if (!b->graphs_on) batch_invalidate(b);
+    return ADI_OK;
+}
+
+adi_status adi_batch_set_chunk(adi_batch *b, int dir, int K)
+{
+    if (!b || dir < 0 || dir > 2 || (K != 4 && K != 8)) return ADI_ERR_BAD_ARG;
+    const int old = b->K[dir];
+    b->K[dir] = K;
+    adi_status s = b->prec == ADI_FP64 ? batch_build<double>(b) : batch_build<float>(b);
+    if (s != ADI_OK) {
+        b->K[dir] = old;
+        if (b->prec == ADI_FP64) batch_build<double>(b);
+        else batch_build<float>(b);
+    }
+    return s;
+}
+
+adi_status adi_batch_get_chunk(adi_batch *b, int dir, int *K)
+{
+    if (!b || dir < 0 || dir > 2 || !K) return ADI_ERR_BAD_ARG;
+    *K = b->K[dir];
+    return ADI_OK;
+}
+
+adi_status adi_batch_step(adi_batch *b, double dt, int num_global, int num_local, int compute_error)
+{
+    if (!b) return ADI_ERR_BAD_ARG;
+    if (num_global < 1 || num_local < 1) return bfail(b, ADI_ERR_BAD_ARG, "num_global and num_local must be >= 1");
+    if (!(dt > 0) || !std::isfinite(dt)) return bfail(b, ADI_ERR_BAD_ARG, "dt must be positive and finite");
+    const adi_handle *h0 = b->hs[0];
+    for (auto *h : b->hs)
+        if (h->cur != h0->cur || h->nxt != h0->nxt || h->ta != h0->ta || h->tb != h0->tb)
+            return bfail(b, ADI_ERR_STATE, "a batch member was stepped on its own; step members only through the batch");
+    if (b->prec == ADI_FP64) return batch_step<double>(b, dt, num_global, num_local, compute_error);
+    return batch_step<float>(b, dt, num_global, num_local, compute_error);
+}
+
+adi_status adi_batch_autotune(adi_batch *b, double dt, int reps)
+{
+    if (!b || reps < 1 || !(dt > 0)) return ADI_ERR_BAD_ARG;
+    // times one sweep per direction and chunk length; the sweeps write half and the
+    // nonlinear buffers only, which every step rewrites before reading
+    cudaEvent_t e0, e1;
+    BCK(cudaEventCreate(&e0));
+    BCK(cudaEventCreate(&e1));
+    const adi_handle *h0 = b->hs[0];
+    for (int dir = 0; dir < 3; dir++) {
+        float best = 1e30f;
+        int bestK = b->K[dir];
+        for (int K : {4, 8}) {
+            b->K[dir] = K;
+            adi_status s = b->prec == ADI_FP64 ? batch_build<double>(b) : batch_build<float>(b);
+            if (s != ADI_OK) continue;
+            s = b->prec == ADI_FP64 ? batch_load_dt<double>(b, dt) : batch_load_dt<float>(b, dt);
+            if (s != ADI_OK) return s;
+            float tmin = 1e30f;
+            for (int r = 0; r < reps + 1; r++) {
+                BCK(cudaEventRecord(e0, b->stream));
+                cudaError_t e = b->prec == ADI_FP64
+                    ? launch_sweep_fast_batch<double>(dir, K, (const BatchDomain<double> *)b->d_doms, b->d_items[dir],
+                                                      b->nitems[dir], b->grid[dir], h0->cur, h0->ta, h0->half, h0->tb,
+                                                      1, b->stream)
+                    : launch_sweep_fast_batch<float>(dir, K, (const BatchDomain<float> *)b->d_doms, b->d_items[dir],
+                                                     b->nitems[dir], b->grid[dir], h0->cur, h0->ta, h0->half, h0->tb,
+                                                     1, b->stream);
+                BCK(e);
+                BCK(cudaEventRecord(e1, b->stream));
+                BCK(cudaEventSynchronize(e1));
+                float ms = 0;
+                BCK(cudaEventElapsedTime(&ms, e0, e1));
+                if (r > 0 && ms < tmin) tmin = ms;
+            }
+            if (tmin < best) { best = tmin; bestK = K; }
+        }
+        b->K[dir] = bestK;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return b->prec == ADI_FP64 ? batch_build<double>(b) : batch_build<float>(b);
+}
+
+adi_status adi_batch_time_sweeps(adi_batch *b, double dt, int reps, float *ms_out)
+{
+    if (!b || reps < 1 || !(dt > 0) || !ms_out) return ADI_ERR_BAD_ARG;
+    adi_status s = b->prec == ADI_FP64 ? batch_load_dt<double>(b, dt) : batch_load_dt<float>(b, dt);
+    if (s != ADI_OK) return s;
+    cudaEvent_t e0, e1;
+    BCK(cudaEventCreate(&e0));
+    BCK(cudaEventCreate(&e1));
+    const adi_handle *h0 = b->hs[0];
+    for (int dir = 0; dir < 3; dir++) {
+        float sum = 0.f;
+        for (int r = 0; r < reps + 1; r++) {
+            BCK(cudaEventRecord(e0, b->stream));
+            cudaError_t e = b->prec == ADI_FP64
+                ? launch_sweep_fast_batch<double>(dir, b->K[dir], (const BatchDomain<double> *)b->d_doms,
+                                                  b->d_items[dir], b->nitems[dir], b->grid[dir], h0->cur, h0->ta,
+                                                  h0->half, h0->tb, 1, b->stream)
+                : launch_sweep_fast_batch<float>(dir, b->K[dir], (const BatchDomain<float> *)b->d_doms,
+                                                 b->d_items[dir], b->nitems[dir], b->grid[dir], h0->cur, h0->ta,
+                                                 h0->half, h0->tb, 1, b->stream);
+            BCK(e);
+            BCK(cudaEventRecord(e1, b->stream));
+            BCK(cudaEventSynchronize(e1));
+            float ms = 0;
+            BCK(cudaEventElapsedTime(&ms, e0, e1));
+            if (r > 0) sum += ms;
+        }
+        ms_out[dir] = sum / reps;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return ADI_OK;
+}
+
+adi_status adi_batch_div_errors(adi_batch *b, double *out)
+{
+    if (!b || !out) return ADI_ERR_BAD_ARG;
+    for (size_t q = 0; q < b->hs.size(); q++) out[q] = b->diff_error[q];
+    return ADI_OK;
+}
+
+adi_status adi_batch_launches(adi_batch *b, int64_t *out)
+{
+    if (!b || !out) return ADI_ERR_BAD_ARG;
+    *out = b->launches;
+    return ADI_OK;
+}
+
+const char *adi_batch_last_error_string(const adi_batch *b)
+{
+    if (!b) return "null batch";
+    return b->err.c_str();
 }
 
 } // extern "C"

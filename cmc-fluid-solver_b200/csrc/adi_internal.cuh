@@ -102,6 +102,22 @@ struct DomainView {
     const R *nv[4];   // node values v.x v.y v.z T
 };
 
+// One domain of a batch (adi_batch_*), as the batched kernels see it: geometry,
+// node codes and values, the five layers, per-direction line ranges, sweep
+// constants for the batch's dt and lines-per-CTA / chunks-per-line of the batched
+// generic sweep (NL * P <= 256).
+template <typename R>
+struct BatchDomain {
+    DomainView<R> d;
+    R *L[5][4];
+    const int *lo[3];
+    const int *hi[3];
+    SweepConst<R> kc[3];
+    int NL[3], P[3];
+    int vec_ok;
+    double dx, dy, dz;
+};
+
 // ---- launchers (each returns cudaGetLastError()) ----
 template <typename R>
 cudaError_t launch_step_begin(const DomainView<R> &d, Layer<R> cur, Layer<R> next, Layer<R> ta, Layer<R> tb,
@@ -116,6 +132,15 @@ cudaError_t launch_div_error(const DomainView<R> &d, CLayer<R> l, R dx, R dy, R 
                              unsigned long long *out_cnt, cudaStream_t s);
 template <typename R>
 cudaError_t launch_fill_missing(const DomainView<R> &d, Layer<R> l, cudaStream_t s);
+// Batch versions: every domain of the batch in one launch (grid y = domain).
+// The divergence partials take nblocks * ndom slots, the results ndom each.
+template <typename R>
+cudaError_t launch_step_begin_batch(const BatchDomain<R> *doms, int ndom, long long max_cells, int cur, int nxt,
+                                   int ta, int tb, bool update_boundaries, cudaStream_t s);
+template <typename R>
+cudaError_t launch_div_error_batch(const BatchDomain<R> *doms, int ndom, int layer, int nblocks, double *psum,
+                                   unsigned long long *pcnt, double *out_sum, unsigned long long *out_cnt,
+                                   cudaStream_t s);
 // out[0] |= max |x - t|, out[1] |= max |x| over NODE_IN cells (bit patterns, atomicMax;
 // out must start at zero).
 template <typename R>
@@ -132,6 +157,11 @@ cudaError_t launch_sweep_fast(int dir, const DomainView<R> &d, const int *line_l
                               const SweepConst<R> &k, int merges, FastShape shape, cudaStream_t s);
 // Shapes the fast sweep is compiled for (K values); returns false if `shape` is not one.
 bool fast_shape_supported(int dir, FastShape shape, int len, int elem_bytes);
+// Batched generic sweep: one persistent launch over the (domain, first line) items
+// of direction dir; K in {4, 8}; 256 threads per CTA.
+template <typename R>
+cudaError_t launch_sweep_fast_batch(int dir, int K, const BatchDomain<R> *doms, const int2 *items, int nitems,
+                                    int grid, int src, int tin, int dst, int tout, int merges, cudaStream_t s);
 
 template <typename R>
 cudaError_t launch_sweep_zwarp(const DomainView<R> &d, const int *line_lo, const int *line_hi, CLayer<R> cur,

@@ -35,25 +35,51 @@ __global__ void update_boundaries_kernel(DomainView<R> d, Layer<R> cur)
 // With update_boundaries, cur[BOUND|VALVE] is first refreshed from the node values
 // (the driver calls UpdateBoundaries right before TimeStep, FluidSolver3D.cpp:241-242).
 template <typename R>
+__device__ __forceinline__ void step_begin_at(const DomainView<R> &d, const Layer<R> &cur, const Layer<R> &next,
+                                              const Layer<R> &ta, const Layer<R> &tb, bool update_boundaries,
+                                              long long i)
+{
+    bool bv = code_is_bv(d.code[i]);
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+        R x;
+        if (update_boundaries && bv) {
+            x = d.nv[v][i];
+            cur.f[v][i] = x;
+        } else {
+            x = cur.f[v][i];
+        }
+        if (bv) next.f[v][i] = x;
+        ta.f[v][i] = x;
+        tb.f[v][i] = x;
+    }
+}
+
+template <typename R>
 __global__ void step_begin_kernel(DomainView<R> d, Layer<R> cur, Layer<R> next, Layer<R> ta, Layer<R> tb,
                                   bool update_boundaries)
 {
-    for (long long i = gtid(); i < d.n; i += gstride()) {
-        bool bv = code_is_bv(d.code[i]);
+    for (long long i = gtid(); i < d.n; i += gstride()) step_begin_at(d, cur, next, ta, tb, update_boundaries, i);
+}
+
+template <typename R>
+__device__ __forceinline__ Layer<R> batch_layer(const BatchDomain<R> &bd, int l)
+{
+    Layer<R> x;
 #pragma unroll
-        for (int v = 0; v < 4; v++) {
-            R x;
-            if (update_boundaries && bv) {
-                x = d.nv[v][i];
-                cur.f[v][i] = x;
-            } else {
-                x = cur.f[v][i];
-            }
-            if (bv) next.f[v][i] = x;
-            ta.f[v][i] = x;
-            tb.f[v][i] = x;
-        }
-    }
+    for (int v = 0; v < 4; v++) x.f[v] = bd.L[l][v];
+    return x;
+}
+
+// The step start of every domain of a batch in one launch: blockIdx.y picks the
+// domain, blockIdx.x / threadIdx.x stride over its cells.
+template <typename R>
+__global__ void step_begin_batch_kernel(const BatchDomain<R> *__restrict__ doms, int cur, int nxt, int ta, int tb,
+                                        bool update_boundaries)
+{
+    const BatchDomain<R> &bd = doms[blockIdx.y];
+    const Layer<R> c = batch_layer(bd, cur), n = batch_layer(bd, nxt), a = batch_layer(bd, ta), b = batch_layer(bd, tb);
+    for (long long i = gtid(); i < bd.d.n; i += gstride()) step_begin_at(bd.d, c, n, a, b, update_boundaries, i);
 }
 
 // dest = (dest + src) / 2 where type == IN (TimeLayer3D.h:415-436).
@@ -73,35 +99,39 @@ __global__ void merge_kernel(DomainView<R> d, CLayer<R> src, Layer<R> dest)
 // and accumulated in double.  Per-block partial sums are reduced in a fixed order
 // by a second single-block kernel, so the result is deterministic; it differs from
 // the reference's sequential double sum only by summation order.
+// Adds cell id's term of the divergence error to acc / cnt (IN cells off the
+// upper faces only).
 template <typename R>
-__global__ void div_error_partial_kernel(DomainView<R> d, CLayer<R> l, R dx, R dy, R dz, double *psum,
-                                         unsigned long long *pcnt)
+__device__ __forceinline__ void div_cell(const DomainView<R> &d, const CLayer<R> &l, R dx, R dy, R dz, long long id,
+                                         double &acc, unsigned long long &cnt)
 {
     const int nx = d.nx, ny = d.ny, nz = d.nz;
     const long long sx = (long long)ny * nz, sy = nz;
-    double acc = 0.0;
-    unsigned long long cnt = 0;
     const R *U = l.f[0], *V = l.f[1], *W = l.f[2];
-    for (long long id = gtid(); id < d.n; id += gstride()) {
-        int k = (int)(id % nz);
-        long long r = id / nz;
-        int j = (int)(r % ny);
-        int i = (int)(r / ny);
-        if (i >= nx - 1 || j >= ny - 1 || k >= nz - 1) continue;
-        if (!code_is_in(d.code[id])) continue;
-        // E(i,j,k) with the offsets the reference uses; IN nodes never sit on the
-        // frame (solver contract), so i-1, j-1, k-1 >= 0.
+    int k = (int)(id % nz);
+    long long r = id / nz;
+    int j = (int)(r % ny);
+    int i = (int)(r / ny);
+    if (i >= nx - 1 || j >= ny - 1 || k >= nz - 1) return;
+    if (!code_is_in(d.code[id])) return;
+    // E(i,j,k) with the offsets the reference uses; IN nodes never sit on the
+    // frame (solver contract), so i-1, j-1, k-1 >= 0.
 #define E_(A, di, dj, dk) A[id + (di) * sx + (dj) * sy + (dk)]
-        double err_x = (double)((R)((R)((R)((R)((R)((R)((R)(E_(U, 0, 0, 0) + E_(U, 0, -1, 0)) + E_(U, 0, -1, -1)) + E_(U, 0, 0, -1)) -
-                                E_(U, -1, 0, 0)) - E_(U, -1, -1, 0)) - E_(U, -1, -1, -1)) - E_(U, -1, 0, -1)) * dz * dy) / 4.0;
-        double err_y = (double)((R)((R)((R)((R)((R)((R)((R)(E_(V, 0, 0, 0) + E_(V, -1, 0, 0)) + E_(V, -1, 0, -1)) + E_(V, 0, 0, -1)) -
-                                E_(V, 0, -1, 0)) - E_(V, -1, -1, 0)) - E_(V, -1, -1, -1)) - E_(V, 0, -1, -1)) * dx * dz) / 4.0;
-        double err_z = (double)((R)((R)((R)((R)((R)((R)((R)(E_(W, 0, 0, 0) + E_(W, 0, -1, 0)) + E_(W, -1, -1, 0)) + E_(W, -1, 0, 0)) -
-                                E_(W, 0, 0, -1)) - E_(W, 0, -1, -1)) - E_(W, -1, -1, -1)) - E_(W, -1, 0, -1)) * dx * dy) / 4.0;
+    double err_x = (double)((R)((R)((R)((R)((R)((R)((R)(E_(U, 0, 0, 0) + E_(U, 0, -1, 0)) + E_(U, 0, -1, -1)) + E_(U, 0, 0, -1)) -
+                            E_(U, -1, 0, 0)) - E_(U, -1, -1, 0)) - E_(U, -1, -1, -1)) - E_(U, -1, 0, -1)) * dz * dy) / 4.0;
+    double err_y = (double)((R)((R)((R)((R)((R)((R)((R)(E_(V, 0, 0, 0) + E_(V, -1, 0, 0)) + E_(V, -1, 0, -1)) + E_(V, 0, 0, -1)) -
+                            E_(V, 0, -1, 0)) - E_(V, -1, -1, 0)) - E_(V, -1, -1, -1)) - E_(V, 0, -1, -1)) * dx * dz) / 4.0;
+    double err_z = (double)((R)((R)((R)((R)((R)((R)((R)(E_(W, 0, 0, 0) + E_(W, 0, -1, 0)) + E_(W, -1, -1, 0)) + E_(W, -1, 0, 0)) -
+                            E_(W, 0, 0, -1)) - E_(W, 0, -1, -1)) - E_(W, -1, -1, -1)) - E_(W, -1, 0, -1)) * dx * dy) / 4.0;
 #undef E_
-        acc += fabs(err_x + err_y + err_z);
-        cnt++;
-    }
+    acc += fabs(err_x + err_y + err_z);
+    cnt++;
+}
+
+// Block sum of (acc, cnt) in a fixed tree order into psum[slot], pcnt[slot].
+__device__ __forceinline__ void block_sum_to(double acc, unsigned long long cnt, double *psum,
+                                             unsigned long long *pcnt, long long slot)
+{
     __shared__ double s_sum[256];
     __shared__ unsigned long long s_cnt[256];
     s_sum[threadIdx.x] = acc;
@@ -115,16 +145,46 @@ __global__ void div_error_partial_kernel(DomainView<R> d, CLayer<R> l, R dx, R d
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        psum[blockIdx.x] = s_sum[0];
-        pcnt[blockIdx.x] = s_cnt[0];
+        psum[slot] = s_sum[0];
+        pcnt[slot] = s_cnt[0];
     }
 }
 
-// One warp: lane l sums partials l, l+32, ... in order, then a fixed shuffle tree
-// combines the lanes, so the result does not depend on scheduling.
+template <typename R>
+__global__ void div_error_partial_kernel(DomainView<R> d, CLayer<R> l, R dx, R dy, R dz, double *psum,
+                                         unsigned long long *pcnt)
+{
+    double acc = 0.0;
+    unsigned long long cnt = 0;
+    for (long long id = gtid(); id < d.n; id += gstride()) div_cell(d, l, dx, dy, dz, id, acc, cnt);
+    block_sum_to(acc, cnt, psum, pcnt, blockIdx.x);
+}
+
+// Per-domain partial sums of a batch: blockIdx.y picks the domain; partials land
+// at [domain][blockIdx.x].
+template <typename R>
+__global__ void div_error_batch_partial_kernel(const BatchDomain<R> *__restrict__ doms, int layer, double *psum,
+                                               unsigned long long *pcnt)
+{
+    const BatchDomain<R> &bd = doms[blockIdx.y];
+    CLayer<R> l;
+#pragma unroll
+    for (int v = 0; v < 4; v++) l.f[v] = bd.L[layer][v];
+    double acc = 0.0;
+    unsigned long long cnt = 0;
+    for (long long id = gtid(); id < bd.d.n; id += gstride())
+        div_cell(bd.d, l, (R)bd.dx, (R)bd.dy, (R)bd.dz, id, acc, cnt);
+    block_sum_to(acc, cnt, psum, pcnt, (long long)blockIdx.y * gridDim.x + blockIdx.x);
+}
+
 __global__ void div_error_final_kernel(const double *psum, const unsigned long long *pcnt, int nblocks,
                                        double *out_sum, unsigned long long *out_cnt)
 {
+    // one warp per reduction: block b folds partials [b * nblocks, (b + 1) * nblocks)
+    psum += (long long)blockIdx.x * nblocks;
+    pcnt += (long long)blockIdx.x * nblocks;
+    out_sum += blockIdx.x;
+    out_cnt += blockIdx.x;
     const int lane = threadIdx.x;
     double s = 0.0;
     unsigned long long c = 0;
@@ -248,6 +308,32 @@ cudaError_t launch_fill_missing(const DomainView<R> &d, Layer<R> l, cudaStream_t
 }
 
 template <typename R>
+cudaError_t launch_step_begin_batch(const BatchDomain<R> *doms, int ndom, long long max_cells, int cur, int nxt,
+                                   int ta, int tb, bool update_boundaries, cudaStream_t s)
+{
+    if (ndom == 0) return cudaSuccess;
+    long long per = (max_cells + 255) / 256;
+    long long cap = (148LL * 16 + ndom - 1) / ndom;   // about 16 blocks per SM overall
+    if (cap < 8) cap = 8;
+    const int bx = (int)(per < cap ? (per < 1 ? 1 : per) : cap);
+    step_begin_batch_kernel<R><<<dim3(bx, ndom), 256, 0, s>>>(doms, cur, nxt, ta, tb, update_boundaries);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_div_error_batch(const BatchDomain<R> *doms, int ndom, int layer, int nblocks, double *psum,
+                                   unsigned long long *pcnt, double *out_sum, unsigned long long *out_cnt,
+                                   cudaStream_t s)
+{
+    if (ndom == 0) return cudaSuccess;
+    div_error_batch_partial_kernel<R><<<dim3(nblocks, ndom), 256, 0, s>>>(doms, layer, psum, pcnt);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    div_error_final_kernel<<<ndom, 32, 0, s>>>(psum, pcnt, nblocks, out_sum, out_cnt);
+    return cudaGetLastError();
+}
+
+template <typename R>
 cudaError_t launch_residual(const DomainView<R> &d, CLayer<R> x, CLayer<R> t, unsigned long long *out, cudaStream_t s)
 {
     residual_kernel<R><<<DIV_BLOCKS, 256, 0, s>>>(d, x, t, out);
@@ -255,6 +341,11 @@ cudaError_t launch_residual(const DomainView<R> &d, CLayer<R> x, CLayer<R> t, un
 }
 
 #define INST(R)                                                                                                  \
+    template cudaError_t launch_step_begin_batch<R>(const BatchDomain<R> *, int, long long, int, int, int, int,  \
+                                                    bool, cudaStream_t);                                          \
+    template cudaError_t launch_div_error_batch<R>(const BatchDomain<R> *, int, int, int, double *,               \
+                                                   unsigned long long *, double *, unsigned long long *,          \
+                                                   cudaStream_t);                                                 \
     template cudaError_t launch_residual<R>(const DomainView<R> &, CLayer<R>, CLayer<R>, unsigned long long *,   \
                                             cudaStream_t);                                                        \
     template cudaError_t launch_update_boundaries<R>(const DomainView<R> &, Layer<R>, cudaStream_t);            \

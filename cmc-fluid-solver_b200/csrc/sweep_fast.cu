@@ -118,24 +118,33 @@ __device__ __forceinline__ int slot(int li, int c, int q, int NL, int P)
 
 } // namespace
 
+// One CTA's work: NL lines starting at line0, P chunks of K rows each, threads
+// t < NL*P live.  Threads beyond NL*P (a batch item narrower than the block) keep
+// every barrier but load and write nothing global and share one spare slot; each
+// buffer holds buf_elems >= NL*P*8 (+ 8 when such threads exist) values.
 template <typename R, int DIR, int K>
-__global__ void __launch_bounds__(256)
-    sweep_fast_kernel(DomainView<R> d, LineGeom g, int NL, int P, const int *__restrict__ line_lo,
-                      const int *__restrict__ line_hi, CLayer<R> cur, CLayer<R> tin, Layer<R> next, Layer<R> tout,
-                      SweepConst<R> kc, int merges, int vec_ok)
+__device__ __forceinline__ void sweep_fast_block(unsigned char *smem_raw, int buf_elems, const DomainView<R> &d,
+                                                 const LineGeom &g, int NL, int P, int line0,
+                                                 const int *__restrict__ line_lo, const int *__restrict__ line_hi,
+                                                 CLayer<R> cur, CLayer<R> tin, Layer<R> next, Layer<R> tout,
+                                                 const SweepConst<R> &kc, int merges, int vec_ok)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     R *buf0 = reinterpret_cast<R *>(smem_raw);
-    R *buf1 = buf0 + (size_t)NL * P * 8;
+    R *buf1 = buf0 + buf_elems;
 
     const int t = threadIdx.x;
     int li, ch;
     if (DIR == 2) { li = t / P; ch = t - li * P; }
     else { ch = t / NL; li = t - ch * NL; }
-    const int line = blockIdx.x * NL + li;
+    const bool live = t < NL * P;
+    // Shared-memory slot of value q of chunk c of line li.  A thread beyond NL*P
+    // (batch items narrower than the block) uses one spare slot past the live ones:
+    // it keeps the barriers but its values are never read by a live thread.
+    auto slot_of = [&](int li_, int c_, int q_) { return live ? slot<DIR>(li_, c_, q_, NL, P) : NL * P * 8 + q_; };
+    const int line = line0 + li;
     int lo = INT_MAX, hi = -1;
     long long base = 0;
-    if (line < g.nlines) {
+    if (live && line < g.nlines) {
         const int a = line_lo[line];
         if (a >= 0) { lo = a; hi = line_hi[line]; }
         base = line_base(DIR, g, line);
@@ -348,23 +357,23 @@ __global__ void __launch_bounds__(256)
     // ---------------- 3. reduced system of the line ----------------
     // (a) one cyclic-reduction step: remove x_last of chunks ch-1 and ch from the
     //     chunk-first row of chunk ch.
-    buf0[slot<DIR>(li, ch, 0, NL, P)] = Al[0];
-    buf0[slot<DIR>(li, ch, 1, NL, P)] = Cl[0];
-    buf0[slot<DIR>(li, ch, 2, NL, P)] = Al[1];
-    buf0[slot<DIR>(li, ch, 3, NL, P)] = Cl[1];
+    buf0[slot_of(li, ch, 0)] = Al[0];
+    buf0[slot_of(li, ch, 1)] = Cl[0];
+    buf0[slot_of(li, ch, 2)] = Al[1];
+    buf0[slot_of(li, ch, 3)] = Cl[1];
 #pragma unroll
-    for (int v = 0; v < 4; v++) buf0[slot<DIR>(li, ch, 4 + v, NL, P)] = Dl[v];
+    for (int v = 0; v < 4; v++) buf0[slot_of(li, ch, 4 + v)] = Dl[v];
     __syncthreads();
     R ea_[2], ec_[2], ed[4];  // the chunk-first row after the reduction, normalised
     {
         R pA[2] = {R(0), R(0)}, pC[2] = {R(0), R(0)}, pD[4] = {R(0), R(0), R(0), R(0)};
         if (ch > 0) {
-            pA[0] = buf0[slot<DIR>(li, ch - 1, 0, NL, P)];
-            pC[0] = buf0[slot<DIR>(li, ch - 1, 1, NL, P)];
-            pA[1] = buf0[slot<DIR>(li, ch - 1, 2, NL, P)];
-            pC[1] = buf0[slot<DIR>(li, ch - 1, 3, NL, P)];
+            pA[0] = buf0[slot_of(li, ch - 1, 0)];
+            pC[0] = buf0[slot_of(li, ch - 1, 1)];
+            pA[1] = buf0[slot_of(li, ch - 1, 2)];
+            pC[1] = buf0[slot_of(li, ch - 1, 3)];
 #pragma unroll
-            for (int v = 0; v < 4; v++) pD[v] = buf0[slot<DIR>(li, ch - 1, 4 + v, NL, P)];
+            for (int v = 0; v < 4; v++) pD[v] = buf0[slot_of(li, ch - 1, 4 + v)];
         }
 #pragma unroll
         for (int m = 0; m < 2; m++) {
@@ -387,32 +396,32 @@ __global__ void __launch_bounds__(256)
     int nstep = 0;
     for (int s = 1; s < P; s <<= 1, nstep++) {
         R *bw = (nstep & 1) ? buf0 : buf1;
-        bw[slot<DIR>(li, ch, 0, NL, P)] = ea_[0];
-        bw[slot<DIR>(li, ch, 1, NL, P)] = ec_[0];
-        bw[slot<DIR>(li, ch, 2, NL, P)] = ea_[1];
-        bw[slot<DIR>(li, ch, 3, NL, P)] = ec_[1];
+        bw[slot_of(li, ch, 0)] = ea_[0];
+        bw[slot_of(li, ch, 1)] = ec_[0];
+        bw[slot_of(li, ch, 2)] = ea_[1];
+        bw[slot_of(li, ch, 3)] = ec_[1];
 #pragma unroll
-        for (int v = 0; v < 4; v++) bw[slot<DIR>(li, ch, 4 + v, NL, P)] = ed[v];
+        for (int v = 0; v < 4; v++) bw[slot_of(li, ch, 4 + v)] = ed[v];
         __syncthreads();
         R mA[2] = {R(0), R(0)}, mC[2] = {R(0), R(0)}, mD[4] = {R(0), R(0), R(0), R(0)};
         R pA[2] = {R(0), R(0)}, pC[2] = {R(0), R(0)}, pD[4] = {R(0), R(0), R(0), R(0)};
         if (ch - s >= 0) {
 #pragma unroll
             for (int m = 0; m < 2; m++) {
-                mA[m] = bw[slot<DIR>(li, ch - s, 2 * m, NL, P)];
-                mC[m] = bw[slot<DIR>(li, ch - s, 2 * m + 1, NL, P)];
+                mA[m] = bw[slot_of(li, ch - s, 2 * m)];
+                mC[m] = bw[slot_of(li, ch - s, 2 * m + 1)];
             }
 #pragma unroll
-            for (int v = 0; v < 4; v++) mD[v] = bw[slot<DIR>(li, ch - s, 4 + v, NL, P)];
+            for (int v = 0; v < 4; v++) mD[v] = bw[slot_of(li, ch - s, 4 + v)];
         }
         if (ch + s < P) {
 #pragma unroll
             for (int m = 0; m < 2; m++) {
-                pA[m] = bw[slot<DIR>(li, ch + s, 2 * m, NL, P)];
-                pC[m] = bw[slot<DIR>(li, ch + s, 2 * m + 1, NL, P)];
+                pA[m] = bw[slot_of(li, ch + s, 2 * m)];
+                pC[m] = bw[slot_of(li, ch + s, 2 * m + 1)];
             }
 #pragma unroll
-            for (int v = 0; v < 4; v++) pD[v] = bw[slot<DIR>(li, ch + s, 4 + v, NL, P)];
+            for (int v = 0; v < 4; v++) pD[v] = bw[slot_of(li, ch + s, 4 + v)];
         }
 #pragma unroll
         for (int m = 0; m < 2; m++) {
@@ -431,14 +440,14 @@ __global__ void __launch_bounds__(256)
     // (c) x_first of this chunk is ed; x_last from its own row and x_first(ch+1)
     R *bx = (nstep & 1) ? buf0 : buf1;
 #pragma unroll
-    for (int v = 0; v < 4; v++) bx[slot<DIR>(li, ch, v, NL, P)] = ed[v];
+    for (int v = 0; v < 4; v++) bx[slot_of(li, ch, v)] = ed[v];
     __syncthreads();
     R xf[4], xl[4];
     {
         R nf[4] = {R(0), R(0), R(0), R(0)};
         if (ch + 1 < P) {
 #pragma unroll
-            for (int v = 0; v < 4; v++) nf[v] = bx[slot<DIR>(li, ch + 1, v, NL, P)];
+            for (int v = 0; v < 4; v++) nf[v] = bx[slot_of(li, ch + 1, v)];
         }
 #pragma unroll
         for (int v = 0; v < 4; v++) {
@@ -482,6 +491,68 @@ __global__ void __launch_bounds__(256)
         }
     }
 }
+
+template <typename R, int DIR, int K>
+__global__ void __launch_bounds__(256)
+    sweep_fast_kernel(DomainView<R> d, LineGeom g, int NL, int P, const int *__restrict__ line_lo,
+                      const int *__restrict__ line_hi, CLayer<R> cur, CLayer<R> tin, Layer<R> next, Layer<R> tout,
+                      SweepConst<R> kc, int merges, int vec_ok)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    sweep_fast_block<R, DIR, K>(smem_raw, NL * P * 8, d, g, NL, P, blockIdx.x * NL, line_lo, line_hi, cur, tin,
+                                next, tout, kc, merges, vec_ok);
+}
+
+// Many domains in one persistent launch: CTA b takes items b, b + gridDim.x, ...
+// of the direction's work list (domain, first line); every item runs with the
+// domain's own geometry, constants and lines-per-CTA.  Layer roles are indices
+// into each domain's five layers, the same for every domain of the batch.
+template <typename R, int DIR, int K>
+__global__ void __launch_bounds__(256, K == 4 ? 2 : 1)
+    sweep_fast_batch_kernel(const BatchDomain<R> *__restrict__ doms, const int2 *__restrict__ items, int nitems,
+                            int src, int tin, int dst, int tout, int merges)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const int2 w = items[it];
+        const BatchDomain<R> &bd = doms[w.x];
+        const DomainView<R> d = bd.d;
+        const LineGeom g = line_geom(DIR, d.nx, d.ny, d.nz);
+        CLayer<R> c, ti;
+        Layer<R> nx, to;
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            c.f[v] = bd.L[src][v];
+            ti.f[v] = bd.L[tin][v];
+            nx.f[v] = bd.L[dst][v];
+            to.f[v] = bd.L[tout][v];
+        }
+        sweep_fast_block<R, DIR, K>(smem_raw, blockDim.x * 8, d, g, bd.NL[DIR], bd.P[DIR], w.y, bd.lo[DIR], bd.hi[DIR],
+                                    c, ti, nx, to, bd.kc[DIR], merges, bd.vec_ok);
+        __syncthreads();   // the shared buffers are reused by the next item
+    }
+}
+
+template <typename R>
+cudaError_t launch_sweep_fast_batch(int dir, int K, const BatchDomain<R> *doms, const int2 *items, int nitems,
+                                    int grid, int src, int tin, int dst, int tout, int merges, cudaStream_t s)
+{
+    if (nitems == 0) return cudaSuccess;
+    const size_t smem = (size_t)2 * 256 * 8 * sizeof(R);
+#define FB(DD, KK)                                                                                                 \
+    if (dir == DD && K == KK) {                                                                                    \
+        sweep_fast_batch_kernel<R, DD, KK><<<grid, 256, smem, s>>>(doms, items, nitems, src, tin, dst, tout, merges); \
+        return cudaGetLastError();                                                                                 \
+    }
+    FB(0, 4) FB(0, 8) FB(1, 4) FB(1, 8) FB(2, 4) FB(2, 8)
+#undef FB
+    return cudaErrorInvalidConfiguration;
+}
+
+template cudaError_t launch_sweep_fast_batch<float>(int, int, const BatchDomain<float> *, const int2 *, int, int, int,
+                                                    int, int, int, int, cudaStream_t);
+template cudaError_t launch_sweep_fast_batch<double>(int, int, const BatchDomain<double> *, const int2 *, int, int,
+                                                     int, int, int, int, int, cudaStream_t);
 
 bool fast_shape_supported(int dir, FastShape s, int len, int elem_bytes)
 {

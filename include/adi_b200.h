@@ -252,6 +252,52 @@ adi_status adi_get_profile(adi_handle *h, adi_profile *out, int reset);
  * boundary values. */
 adi_status adi_device_pointers(adi_handle *h, void *out8[8]);
 
+/* ---- batches of domains ------------------------------------------------ */
+
+/* Many independent domains stepped together (no counterpart in the reference,
+ * which steps one domain per process).  Each member is an ordinary handle (created,
+ * masked and segmented as usual; its own fluid parameters and grid); the batch
+ * borrows them, so they must outlive it.  A batch step runs, for all members at
+ * once: one step-start launch, one persistent launch per sweep (the generic
+ * chunked sweep over a work list of (domain, first line) items in longest-first
+ * order, K rows per thread and 256 threads per CTA, lines per CTA fitted to each
+ * domain), and the per-domain divergence errors; the whole step is replayed as a
+ * CUDA graph.  Members step in lock step: all start with the same layer roles
+ * (e.g. freshly set up) and must not be stepped on their own while batched. */
+typedef struct adi_batch adi_batch;
+
+/* Builds the batch's descriptors and work lists.  All handles: same precision and
+ * device, mask and segments set, solver contract satisfied.  The batch uses the
+ * first handle's stream. */
+adi_status adi_batch_create(adi_handle *const *handles, int n, adi_batch **out);
+adi_status adi_batch_destroy(adi_batch *b);
+adi_status adi_batch_set_stream(adi_batch *b, void *cuda_stream);
+
+/* adi_step for every member: boundary update, num_global x (Z, Y, X sweeps,
+ * num_local each), divergence errors when compute_error.  If any member's
+ * (last computed) divergence error exceeds 0.01 the call returns
+ * ADI_ERR_DIVERGENCE and no member advances. */
+adi_status adi_batch_step(adi_batch *b, double dt, int num_global, int num_local, int compute_error);
+
+/* Last computed divergence error of each member (n values). */
+adi_status adi_batch_div_errors(adi_batch *b, double *out);
+
+/* Chunk length K in {4, 8} of the batched sweep per direction (segment-to-thread
+ * binning), and the autotuner that times both per direction at dt. */
+adi_status adi_batch_set_chunk(adi_batch *b, int dir, int K);
+adi_status adi_batch_get_chunk(adi_batch *b, int dir, int *K);
+adi_status adi_batch_autotune(adi_batch *b, double dt, int reps);
+
+/* Mean time in ms of one batched sweep launch per direction X, Y, Z (reps timed
+ * launches after one untimed, at dt; the launches write half and the nonlinear
+ * buffers only, which every step rewrites before reading). */
+adi_status adi_batch_time_sweeps(adi_batch *b, double dt, int reps, float *ms_out3);
+
+/* Graph replay on (default) or off; kernel launches issued so far. */
+adi_status adi_batch_set_graphs(adi_batch *b, int on);
+adi_status adi_batch_launches(adi_batch *b, int64_t *out);
+const char *adi_batch_last_error_string(const adi_batch *b);
+
 /* ---- allocation-free sweep ----------------------------------------------- */
 
 /* This entry point has no counterpart in the reference: it exists for callers

@@ -1,0 +1,129 @@
+"""GPU checks of batched stepping (adi_batch_*).
+
+A batch runs every member through the generic chunked sweep with the batch's
+chunk length K and lines-per-CTA max(1, 256 // P), so each member must come out
+bit for bit as the same domain stepped alone with that fast-sweep shape; one member
+is also compared with the FP64 oracle at float tolerance (2e-6 of the field scale).
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from adi_b200 import geometry as G
+from golden_util import fluid_params_tuple, non_out
+
+pytestmark = pytest.mark.gpu
+
+
+def _domains(seed, n=5, lo=18, hi=44):
+    rng = np.random.default_rng(seed)
+    out = []
+    for q in range(n):
+        dims = tuple(int(x) for x in rng.integers(lo, hi + 1, size=3))
+        d = G.random_domain(*dims, seed=seed * 100 + q, shell=bool(q % 2), n_obstacles=4, rmax=3.5)
+        d.meta["Re"] = float(rng.uniform(60.0, 300.0))
+        out.append(d)
+    return out
+
+
+def _member(adi_lib, d, solver=None, precision=None):
+    from adi_b200 import _abi
+    fp = adi_lib.fluid_params_normalized(d.meta["Re"], 0.72, 1.4)
+    s = adi_lib.AdiSolver3D(d, params=fp, precision=precision or _abi.ADI_FP32,
+                            solver=_abi.ADI_SOLVER_EXACT if solver is None else solver)
+    s.CreateSegments()
+    return s
+
+
+def _alone(adi_lib, d, K):
+    """The same domain stepped by itself with the batch's generic-sweep shape."""
+    from adi_b200 import _abi
+    s = _member(adi_lib, d, solver=_abi.ADI_SOLVER_FAST)
+    for dr in range(3):
+        P = -(-d.shape[dr] // K[dr])
+        s.set_fast_shape(dr, K[dr], max(1, 256 // P))
+    return s
+
+
+@pytest.mark.parametrize("K", [(4, 4, 4), (8, 8, 8), (4, 8, 4)])
+def test_batch_matches_members_stepped_alone(adi_lib, K):
+    ds = _domains(7)
+    members = [_member(adi_lib, d) for d in ds]
+    b = adi_lib.AdiBatch(members)
+    for dr in range(3):
+        b.set_chunk(dr, K[dr])
+    assert b.chunks() == list(K)
+    alone = [_alone(adi_lib, d, K) for d in ds]
+    for i in range(4):
+        ce = i in (0, 3)           # the last step's errors are those of the final state
+        assert b.step(6e-4, 2, 2, ce) == 0, b.last_error()
+        for s in alone:
+            assert s.step(6e-4, 2, 2, ce) == 0
+    for q, (m, s) in enumerate(zip(members, alone)):
+        for f in range(4):
+            assert np.array_equal(m.fields(0)[f], s.fields(0)[f]), (q, f)
+    errs = b.div_errors()
+    for q, s in enumerate(alone):
+        # same cells, summed in a different block order
+        assert abs(errs[q] - s.div_error()) <= 1e-12 * max(1.0, abs(errs[q]))
+
+
+def test_batch_member_against_oracle(adi_lib):
+    ds = _domains(8, n=3)
+    members = [_member(adi_lib, d) for d in ds]
+    b = adi_lib.AdiBatch(members)
+    orc = O.OracleSolver(ds[1], precision=8, params=fluid_params_tuple(("normalized", (ds[1].meta["Re"], 0.72, 1.4))))
+    for i in range(3):
+        assert b.step(7e-4, 3, 2, True) == 0
+        assert orc.step(7e-4, 3, 2, True) == 0
+    m = non_out(ds[1])
+    got, want = members[1].fields(0), orc.fields(0)
+    vs = max(np.max(np.abs(want[f][m])) for f in range(3))
+    for f in range(4):
+        scale = vs if f < 3 else np.max(np.abs(want[3][m]))
+        assert np.max(np.abs(got[f][m].astype(np.float64) - want[f][m])) / scale < 2e-6, f
+    assert abs(b.div_errors()[1] - orc.div_error()) < 1e-6
+
+
+def test_batch_graph_replay_and_autotune(adi_lib):
+    ds = _domains(9, n=4)
+    ma = [_member(adi_lib, d) for d in ds]
+    mb = [_member(adi_lib, d) for d in ds]
+    a, b = adi_lib.AdiBatch(ma), adi_lib.AdiBatch(mb)
+    a.autotune(6e-4, 2)
+    assert all(k in (4, 8) for k in a.chunks())
+    for dr, k in enumerate(a.chunks()):
+        b.set_chunk(dr, k)
+    b.set_graphs(False)
+    l0a, l0b = a.launches(), b.launches()
+    for i in range(5):
+        assert a.step(6e-4, 2, 2, i == 4) == b.step(6e-4, 2, 2, i == 4) == 0
+    for x, y in zip(ma, mb):
+        for f in range(4):
+            assert np.array_equal(x.fields(0)[f], y.fields(0)[f])
+    assert a.launches() - l0a == b.launches() - l0b == 5 * (1 + 2 * 2 * 3) + 2
+
+
+def test_batch_divergence_guard_and_lock_step(adi_lib):
+    from adi_b200 import _abi
+    ds = _domains(10, n=3)
+    members = [_member(adi_lib, d) for d in ds]
+    b = adi_lib.AdiBatch(members)
+    before = [m.fields(0) for m in members]
+    # a wild state in one member trips its divergence guard: nobody advances
+    rng = np.random.default_rng(0)
+    wild = [(a + 100.0 * rng.standard_normal(a.shape)).astype(np.float32) for a in members[2].fields(0)]
+    members[2].set_state(*wild)
+    assert b.step(6e-4, 1, 1, True) == _abi.ADI_ERR_DIVERGENCE
+    assert b.div_errors()[2] > 0.01
+    for m, f0 in zip(members[:2], before[:2]):
+        for f in range(4):
+            assert np.array_equal(m.fields(0)[f], f0[f])
+    # a member stepped on its own leaves the batch out of lock step
+    members[2].set_state(*before[2])
+    members[2].step(6e-4, 1, 1, True)
+    assert b.step(6e-4, 1, 1, False) == _abi.ADI_ERR_STATE
+    # mixed precisions cannot form a batch
+    m64 = _member(adi_lib, ds[0], precision=_abi.ADI_FP64)
+    with pytest.raises(_abi.AdiError):
+        adi_lib.AdiBatch([members[0], m64])
