@@ -104,6 +104,22 @@ class AdiSolver3D:
     def run(self, dt, num_global, num_local, n_steps, err_every=10):
         self._check(self.lib.adi_run(self.h, dt, num_global, num_local, n_steps, err_every))
 
+    def adjoint_run(self, dt, num_global, num_local, n_steps, ckpt_every, box_lo, box_hi):
+        """Discrete adjoint of n_steps steps for J = 1/2 sum_{IN in box} |u|^2 at the end.
+        Returns (J, dJ/d node values [4, nx, ny, nz], dJ/d initial state)."""
+        lo = (C.c_int * 3)(*box_lo)
+        hi = (C.c_int * 3)(*box_hi)
+        J = C.c_double(0.0)
+        gnv = np.zeros((4,) + tuple(self.shape), self.dtype)
+        gst = np.zeros((4,) + tuple(self.shape), self.dtype)
+        self._check(self.lib.adi_adjoint_run(self.h, dt, num_global, num_local, n_steps, ckpt_every, lo, hi,
+                                             C.byref(J), _ptr(gnv), _ptr(gst)))
+        return J.value, gnv, gst
+
+    def set_node_values(self, vx, vy, vz, T):
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (vx, vy, vz, T)]
+        self._check(self.lib.adi_set_node_values(self.h, *[_ptr(a) for a in arrs]))
+
     def step_tol(self, dt, max_global, num_local, tol, compute_error=False):
         """UpdateBoundaries + TimeStep in tolerance mode; returns (status, iterations, residual)."""
         it, res = C.c_int(0), C.c_double(0.0)

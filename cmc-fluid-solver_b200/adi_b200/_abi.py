@@ -32,7 +32,8 @@ EXPORTED = [
     "adi_sweep_exact_static", "adi_static_scratch_bytes", "adi_step_tol", "adi_set_graphs",
     "adi_batch_create", "adi_batch_destroy", "adi_batch_set_stream", "adi_batch_step", "adi_batch_div_errors",
     "adi_batch_set_chunk", "adi_batch_get_chunk", "adi_batch_autotune", "adi_batch_set_graphs",
-    "adi_batch_launches", "adi_batch_last_error_string", "adi_batch_time_sweeps",
+    "adi_batch_launches", "adi_batch_last_error_string", "adi_batch_time_sweeps", "adi_adjoint_run",
+    "adi_set_node_values",
 ]
 
 K_NUM = 7
@@ -111,6 +112,8 @@ def load() -> C.CDLL:
         "adi_batch_set_graphs": [vp, i],
         "adi_batch_launches": [vp, C.POINTER(C.c_int64)],
         "adi_batch_time_sweeps": [vp, d, i, vp],
+        "adi_adjoint_run": [vp, d, i, i, i, i, vp, vp, C.POINTER(d), vp, vp],
+        "adi_set_node_values": [vp, vp, vp, vp, vp],
         "adi_get_state": [vp, i, vp, vp, vp, vp],
         "adi_set_state": [vp, vp, vp, vp, vp],
         "adi_get_layer": [vp, i, i, i, vp, vp],

@@ -35,6 +35,7 @@ SOURCES = [
     ("sweep_zwarp.cu", []),
     ("sweep_xytma.cu", []),
     ("sweep_xypair.cu", []),
+    ("adjoint.cu", []),
 ]
 
 

@@ -313,7 +313,7 @@ cudaError_t launch_fast(adi_handle *h, int dir, CLayer<R> cur, CLayer<R> tin, La
 // into the nonlinear layer; the last X sweep merges twice (the extra merge after
 // X).  The two nonlinear buffers swap roles after every sweep.
 template <typename R>
-adi_status enqueue_global_iteration(adi_handle *h, R dt, int num_local)
+adi_status enqueue_global_iteration(adi_handle *h, R dt, int num_local, void *const *tape = nullptr)
 {
     const DomainView<R> d = view<R>(h);
     const int order[3] = {2, 1, 0};
@@ -328,6 +328,11 @@ adi_status enqueue_global_iteration(adi_handle *h, R dt, int num_local)
         const int cls = dir == 0 ? ADI_K_SWEEP_X : (dir == 1 ? ADI_K_SWEEP_Y : ADI_K_SWEEP_Z);
         for (int l = 0; l < num_local; l++) {
             const int merges = (dir == 0 && l == num_local - 1) ? 2 : 1;
+            const size_t fb = (size_t)h->n * sizeof(R);
+            if (tape) {   // the nonlinear layer this sweep reads
+                for (int v = 0; v < 4; v++)
+                    CK(cudaMemcpyAsync(tape[v], h->d_L[h->ta][v], fb, cudaMemcpyDeviceToDevice, h->stream));
+            }
             CK(timed(h, cls, bytes, [&] {
                 if (h->solver == ADI_SOLVER_FAST)
                     return launch_fast<R>(h, dir, clayer<R>(h, src[q]), clayer<R>(h, h->ta), layer<R>(h, dst[q]),
@@ -336,6 +341,11 @@ adi_status enqueue_global_iteration(adi_handle *h, R dt, int num_local)
                                              clayer<R>(h, h->ta), layer<R>(h, dst[q]), layer<R>(h, h->tb),
                                              (R *)h->d_scratch, k, merges, h->stream);
             }));
+            if (tape) {   // the layer it wrote
+                for (int v = 0; v < 4; v++)
+                    CK(cudaMemcpyAsync(tape[4 + v], h->d_L[dst[q]][v], fb, cudaMemcpyDeviceToDevice, h->stream));
+                tape += 8;
+            }
             std::swap(h->ta, h->tb);
         }
     }
@@ -641,6 +651,153 @@ adi_status time_step_tol(adi_handle *h, double dt, int max_global, int num_local
         if (s != ADI_OK) return s;
     }
     return finish_step(h, compute_error);
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint: dJ/d(node values) and dJ/d(initial state) of n_steps adi_step calls,
+// J the kinetic energy in a box at the end.  Checkpoints the state every
+// ckpt_every steps; each window is recomputed with a tape (per sweep: the
+// nonlinear layer read and the layer written) and run backward.
+// ---------------------------------------------------------------------------
+
+struct DevBuffers {
+    std::vector<void *> ptrs;
+    ~DevBuffers()
+    {
+        for (void *p : ptrs) cudaFree(p);
+    }
+    void *get(size_t bytes, cudaError_t &e)
+    {
+        void *p = nullptr;
+        if (e == cudaSuccess) e = cudaMalloc(&p, bytes);
+        if (e == cudaSuccess) ptrs.push_back(p);
+        return p;
+    }
+};
+
+template <typename R>
+Layer<R> layer_of(void *const *f)
+{
+    Layer<R> x;
+    for (int v = 0; v < 4; v++) x.f[v] = (R *)f[v];
+    return x;
+}
+
+template <typename R>
+CLayer<R> clayer_of(void *const *f)
+{
+    CLayer<R> x;
+    for (int v = 0; v < 4; v++) x.f[v] = (const R *)f[v];
+    return x;
+}
+
+template <typename R>
+adi_status adjoint_run(adi_handle *h, double dt, int ng, int nl, int n_steps, int ck, const int lo[3], const int hi[3],
+                       double *J, void *nv_grad, void *state_grad)
+{
+    const size_t fb = (size_t)h->n * sizeof(R);
+    const int S = ng * nl * 3;
+    const int nck = (n_steps + ck - 1) / ck;
+    const int win = ck < n_steps ? ck : n_steps;
+    DevBuffers mem;
+    cudaError_t e = cudaSuccess;
+    auto layer4 = [&](void **out) {
+        for (int v = 0; v < 4; v++) out[v] = mem.get(fb, e);
+    };
+    std::vector<void *> ckpt((size_t)nck * 4), fin(4), cb(4), nb(4), hb(4), tb(4), nvb(4);
+    for (int c = 0; c < nck; c++) layer4(&ckpt[(size_t)c * 4]);
+    layer4(fin.data()); layer4(cb.data()); layer4(nb.data()); layer4(hb.data()); layer4(tb.data());
+    layer4(nvb.data());
+    R *ga = (R *)mem.get(fb, e), *gbp = (R *)mem.get(fb, e);
+    double *psum = (double *)mem.get(sizeof(double) * DIV_BLOCKS, e), *dJ = (double *)mem.get(sizeof(double), e);
+    std::vector<void *> tape((size_t)win * S * 8);
+    for (auto &p : tape) p = mem.get(fb, e);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(h, e == cudaErrorMemoryAllocation ? ADI_ERR_CAPACITY : ADI_ERR_CUDA,
+                    "adjoint buffers: " + std::string(cudaGetErrorString(e)));
+    }
+    auto copy4 = [&](void *const *dst, void *const *src) -> adi_status {
+        for (int v = 0; v < 4; v++) CK(cudaMemcpyAsync(dst[v], src[v], fb, cudaMemcpyDeviceToDevice, h->stream));
+        return ADI_OK;
+    };
+    auto zero4 = [&](void *const *dst) -> adi_status {
+        for (int v = 0; v < 4; v++) CK(cudaMemsetAsync(dst[v], 0, fb, h->stream));
+        return ADI_OK;
+    };
+    adi_status st;
+    const R dtr = (R)dt;
+    // ---- forward, keeping checkpoints ----
+    for (int t = 0; t < n_steps; t++) {
+        if (t % ck == 0 && (st = copy4(&ckpt[(size_t)(t / ck) * 4], h->d_L[h->cur])) != ADI_OK) return st;
+        h->bv_synced = true;
+        if (h->graphs_on && !h->prof_on) st = step_graph<R>(h, dtr, ng, nl, 0, true);
+        else st = enqueue_step<R>(h, dtr, ng, nl, 0, true);
+        if (st != ADI_OK) return st;
+        std::swap(h->cur, h->nxt);
+        h->bv_synced = false;
+    }
+    if ((st = copy4(fin.data(), h->d_L[h->cur])) != ADI_OK) return st;
+    CK(launch_objective<R>(view<R>(h), clayer_of<R>(fin.data()), lo, hi, layer_of<R>(cb.data()), psum, DIV_BLOCKS, dJ,
+                           h->stream));
+    if ((st = zero4(nvb.data())) != ADI_OK) return st;
+    const DomainView<R> dv = view<R>(h);
+    // ---- backward, one checkpoint window at a time ----
+    for (int w = nck - 1; w >= 0; w--) {
+        const int t0 = w * ck, t1 = t0 + ck < n_steps ? t0 + ck : n_steps;
+        if ((st = copy4(h->d_L[h->cur], &ckpt[(size_t)w * 4])) != ADI_OK) return st;
+        for (int t = t0; t < t1; t++) {
+            h->bv_synced = true;
+            CK(timed(h, ADI_K_STEP_BEGIN, (int64_t)h->n * (1 + 8 * (int64_t)sizeof(R)), [&] {
+                return launch_step_begin<R>(view<R>(h), layer<R>(h, h->cur), layer<R>(h, h->nxt), layer<R>(h, h->ta),
+                                            layer<R>(h, h->tb), true, h->stream);
+            }));
+            void *const *tp = &tape[(size_t)(t - t0) * S * 8];
+            for (int it = 0; it < ng; it++) {
+                st = enqueue_global_iteration<R>(h, dtr, nl, tp + (size_t)it * nl * 3 * 8);
+                if (st != ADI_OK) return st;
+            }
+            std::swap(h->cur, h->nxt);
+            h->bv_synced = false;
+        }
+        for (int t = t1 - 1; t >= t0; t--) {
+            void *const *tp = &tape[(size_t)(t - t0) * S * 8];
+            if ((st = copy4(nb.data(), cb.data())) != ADI_OK) return st;
+            if ((st = zero4(cb.data())) != ADI_OK) return st;
+            if ((st = zero4(hb.data())) != ADI_OK) return st;
+            if ((st = zero4(tb.data())) != ADI_OK) return st;
+            int q = S - 1;
+            for (int it = ng - 1; it >= 0; it--)
+                for (int dir = 0; dir < 3; dir++) {
+                    void *const *sb = dir == 2 ? cb.data() : (dir == 1 ? nb.data() : hb.data());
+                    void *const *db = dir == 1 ? hb.data() : nb.data();
+                    const SweepConst<R> k = sweep_const<R>(h, dir, dtr);
+                    for (int l = nl - 1; l >= 0; l--, q--) {
+                        const int merges = (dir == 0 && l == nl - 1) ? 2 : 1;
+                        CK(timed(h, ADI_K_OTHER, 0, [&] {
+                            return launch_adjoint_sweep<R>(dir, dv, h->d_line_lo[dir], h->d_line_hi[dir],
+                                                           clayer_of<R>(tp + (size_t)q * 8),
+                                                           clayer_of<R>(tp + (size_t)q * 8 + 4), layer_of<R>(sb),
+                                                           layer_of<R>(db), layer_of<R>(tb.data()),
+                                                           layer_of<R>(nvb.data()), ga, gbp, (R *)h->d_scratch, k,
+                                                           merges, h->stream);
+                        }));
+                    }
+                }
+            CK(launch_adjoint_step_start<R>(dv, layer_of<R>(cb.data()), layer_of<R>(nb.data()), layer_of<R>(tb.data()),
+                                            layer_of<R>(nvb.data()), h->stream));
+        }
+    }
+    if ((st = copy4(h->d_L[h->cur], fin.data())) != ADI_OK) return st;
+    CK(cudaMemcpyAsync(J, dJ, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    for (int v = 0; v < 4; v++) {
+        if (nv_grad)
+            CK(cudaMemcpyAsync((char *)nv_grad + (size_t)v * fb, nvb[v], fb, cudaMemcpyDeviceToHost, h->stream));
+        if (state_grad)
+            CK(cudaMemcpyAsync((char *)state_grad + (size_t)v * fb, cb[v], fb, cudaMemcpyDeviceToHost, h->stream));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    return check_device_flag(h);
 }
 
 adi_status check_ready(adi_handle *h)
@@ -972,6 +1129,46 @@ adi_status adi_step_tol(adi_handle *h, double dt, int max_global, int num_local,
     if (h->prec == ADI_FP64)
         return time_step_tol<double>(h, dt, max_global, num_local, tol, compute_error, true, iters_used, residual);
     return time_step_tol<float>(h, dt, max_global, num_local, tol, compute_error, true, iters_used, residual);
+}
+
+adi_status adi_adjoint_run(adi_handle *h, double dt, int num_global, int num_local, int n_steps, int ckpt_every,
+                           const int box_lo[3], const int box_hi[3], double *J, void *nv_grad, void *state_grad)
+{
+    adi_status s = check_ready(h);
+    if (s != ADI_OK) return s;
+    if (!J || !box_lo || !box_hi || n_steps < 1 || ckpt_every < 1 || num_global < 1 || num_local < 1)
+        return fail(h, ADI_ERR_BAD_ARG, "adjoint: bad arguments");
+    if (!(dt > 0) || !std::isfinite(dt)) return fail(h, ADI_ERR_BAD_ARG, "dt must be positive and finite");
+    const int dims[3] = {h->nx, h->ny, h->nz};
+    int lo[3], hi[3];
+    for (int a = 0; a < 3; a++) {
+        lo[a] = box_lo[a] < 0 ? 0 : box_lo[a];
+        hi[a] = box_hi[a] > dims[a] ? dims[a] : box_hi[a];
+    }
+    if (h->prec == ADI_FP64) return adjoint_run<double>(h, dt, num_global, num_local, n_steps, ckpt_every, lo, hi, J,
+                                                        nv_grad, state_grad);
+    return adjoint_run<float>(h, dt, num_global, num_local, n_steps, ckpt_every, lo, hi, J, nv_grad, state_grad);
+}
+
+adi_status adi_set_node_values(adi_handle *h, const double *vx, const double *vy, const double *vz, const double *T)
+{
+    if (!h || !vx || !vy || !vz || !T) return ADI_ERR_BAD_ARG;
+    if (!h->mask_set) return fail(h, ADI_ERR_STATE, "adi_set_mask has not been called");
+    const double *src[4] = {vx, vy, vz, T};
+    const size_t fb = (size_t)h->n * esize(h);
+    if (h->prec == ADI_FP64) {
+        for (int v = 0; v < 4; v++) CK(cudaMemcpyAsync(h->d_nv[v], src[v], fb, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    } else {
+        std::vector<float> tmp(h->n);
+        for (int v = 0; v < 4; v++) {
+            for (long long i = 0; i < h->n; i++) tmp[i] = (float)src[v][i];
+            CK(cudaMemcpyAsync(h->d_nv[v], tmp.data(), fb, cudaMemcpyHostToDevice, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+        }
+    }
+    h->bv_synced = false;
+    return ADI_OK;
 }
 
 adi_status adi_set_graphs(adi_handle *h, int on)

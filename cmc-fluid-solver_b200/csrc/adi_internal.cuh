@@ -184,6 +184,26 @@ cudaError_t launch_segment_scan(int dir, int nx, int ny, int nz, const uint8_t *
 cudaError_t launch_segment_write(int dir, int nx, int ny, int nz, const uint8_t *code,
                                  const long long *line_offset, int32_t *out7, cudaStream_t s);
 
+// ---- adjoint (adjoint.cu) ----
+// Adjoint of one sweep of direction dir with its tape (ti: the nonlinear layer
+// the sweep read, xs: the layer it wrote): dbar consumed on the segment nodes,
+// tbar turned from the adjoint of the written temp into that of the read temp,
+// sbar and nvbar accumulated; ga, gb are two full-size work planes.
+template <typename R>
+cudaError_t launch_adjoint_sweep(int dir, const DomainView<R> &d, const int *lo, const int *hi, CLayer<R> ti,
+                                 CLayer<R> xs, Layer<R> sbar, Layer<R> dbar, Layer<R> tbar, Layer<R> nvbar, R *ga, R *gb,
+                                 R *scratch, const SweepConst<R> &k, int merges, cudaStream_t s);
+// Adjoint of the step start and UpdateBoundaries (cbar: in, adjoint of cur after
+// them; out, before them).
+template <typename R>
+cudaError_t launch_adjoint_step_start(const DomainView<R> &d, Layer<R> cbar, Layer<R> nbar, Layer<R> tbar,
+                                      Layer<R> nvbar, cudaStream_t s);
+// Kinetic energy of the NODE_IN cells of the box [lo, hi) of x into *out, and its
+// gradient into cbar (psum: nblocks doubles of scratch).
+template <typename R>
+cudaError_t launch_objective(const DomainView<R> &d, CLayer<R> x, const int lo[3], const int hi[3], Layer<R> cbar,
+                             double *psum, int nblocks, double *out, cudaStream_t s);
+
 constexpr int DIV_BLOCKS = 592;  // 4 x 148 SMs
 
 } // namespace adi

@@ -252,6 +252,27 @@ adi_status adi_get_profile(adi_handle *h, adi_profile *out, int reset);
  * boundary values. */
 adi_status adi_device_pointers(adi_handle *h, void *out8[8]);
 
+/* ---- adjoint --------------------------------------------------------------- */
+
+/* Discrete adjoint of n_steps adi_step calls (no counterpart in the reference).
+ * Runs the steps from the current state (no divergence guard), evaluates
+ *   J = 1/2 sum over NODE_IN cells of the box [box_lo, box_hi) of u^2 + v^2 + w^2
+ * on the final state, and returns dJ/d(node values) (nv_grad: 4 fields, handle
+ * precision, [i][j][k]; the inflow, wall and outflow data are node values) and
+ * dJ/d(initial state) (state_grad), either may be NULL.  The backward pass runs
+ * the sweeps in reverse order, each as a transposed tridiagonal solve over the same
+ * segments, recomputing the steps of each window of ckpt_every steps from a
+ * stored state.  Device memory: (n_steps/ckpt_every + 12) layers plus the tape of
+ * one window, ckpt_every * num_global * num_local * 3 * 8 fields.  The handle ends
+ * at the final state. */
+adi_status adi_adjoint_run(adi_handle *h, double dt, int num_global, int num_local, int n_steps, int ckpt_every,
+                           const int box_lo[3], const int box_hi[3], double *J, void *nv_grad, void *state_grad);
+
+/* Replaces the node values (the boundary data of every node; Grid3D node v, T)
+ * without touching the state; the next adi_step applies them. */
+adi_status adi_set_node_values(adi_handle *h, const double *vx, const double *vy, const double *vz,
+                               const double *T);
+
 /* ---- batches of domains ------------------------------------------------ */
 
 /* Many independent domains stepped together (no counterpart in the reference,

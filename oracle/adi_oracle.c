@@ -107,6 +107,8 @@ static int build_lists(const uint8_t *type, int nx, int ny, int nz, seg_list out
 #undef REAL
 #undef SFX
 
+#include "adi_oracle_adjoint.h"
+
 /* ------------------------------------------------------------------------ */
 /* C ABI used by the tests (ctypes).                                          */
 /* ------------------------------------------------------------------------ */
@@ -243,6 +245,80 @@ double oracle_last_div_error(void *vh)
     oracle_h *h = (oracle_h *)vh;
     if (h->precision == 8) return ((solver_f64 *)h->s)->diff_error;
     return ((solver_f32 *)h->s)->diff_error;
+}
+
+/* FP64 discrete adjoint of n_steps adi_step calls from the current state:
+ * J = 1/2 sum over NODE_IN cells of the box [lo, hi) of u^2 + v^2 + w^2 after the
+ * steps; nv_grad = dJ/d(node values), state_grad = dJ/d(initial state), each 4
+ * fields [i][j][k].  The handle ends at the final state.  No divergence guard.
+ * Returns 0, or -1 for a float handle. */
+int oracle_adjoint_run(void *vh, double dt, int num_global, int num_local, int n_steps, const int *lo,
+                       const int *hi, double *J, double *nv_grad, double *state_grad)
+{
+    oracle_h *h = (oracle_h *)vh;
+    if (h->precision != 8) return -1;
+    solver_f64 *s = h->s;
+    size_t n = adj_n(s);
+    int S = num_global * num_local * 3;
+    layer_f64 *states = calloc((size_t)n_steps + 1, sizeof(layer_f64));
+    for (int t = 0; t <= n_steps; t++) adj_alloc(&states[t], n);
+    for (int t = 0; t < n_steps; t++) {
+        adj_copy(&states[t], &s->L[s->cur], n);
+        step_f64(s, dt, num_global, num_local, 0, 1);
+    }
+    adj_copy(&states[n_steps], &s->L[s->cur], n);
+    layer_f64 cbar, nvbar, nbar, hbar, tbar, xb;
+    adj_alloc(&cbar, n); adj_alloc(&nvbar, n); adj_alloc(&nbar, n);
+    adj_alloc(&hbar, n); adj_alloc(&tbar, n); adj_alloc(&xb, n);
+    double acc = 0.0;
+    for (int i = lo[0]; i < hi[0]; i++)
+        for (int j = lo[1]; j < hi[1]; j++)
+            for (int k = lo[2]; k < hi[2]; k++) {
+                size_t id = ((size_t)i * s->ny + j) * s->nz + k;
+                if (s->type[id] != NODE_IN_) continue;
+                for (int v = 0; v < 3; v++) {
+                    double x = states[n_steps].f[v][id];
+                    acc += x * x;
+                    cbar.f[v][id] = x;
+                }
+            }
+    *J = 0.5 * acc;
+    layer_f64 *Ti = calloc((size_t)S, sizeof(layer_f64)), *X = calloc((size_t)S, sizeof(layer_f64));
+    for (int q = 0; q < S; q++) { adj_alloc(&Ti[q], n); adj_alloc(&X[q], n); }
+    for (int t = n_steps - 1; t >= 0; t--) {
+        adj_copy(&s->L[s->cur], &states[t], n);
+        adj_step_with_tape(s, dt, num_global, num_local, Ti, X);
+        adj_step(s, dt, num_global, num_local, Ti, X, &cbar, &nvbar, &nbar, &hbar, &tbar, &xb);
+    }
+    adj_copy(&s->L[s->cur], &states[n_steps], n);
+    for (int v = 0; v < 4; v++) {
+        memcpy(nv_grad + (size_t)v * n, nvbar.f[v], n * sizeof(double));
+        memcpy(state_grad + (size_t)v * n, cbar.f[v], n * sizeof(double));
+    }
+    for (int q = 0; q < S; q++) { adj_free(&Ti[q]); adj_free(&X[q]); }
+    free(Ti); free(X);
+    for (int t = 0; t <= n_steps; t++) adj_free(&states[t]);
+    free(states);
+    adj_free(&cbar); adj_free(&nvbar); adj_free(&nbar); adj_free(&hbar); adj_free(&tbar); adj_free(&xb);
+    return 0;
+}
+
+/* Replaces the node values (boundary data) of a handle; the state is unchanged. */
+int oracle_set_node_values(void *vh, const double *vx, const double *vy, const double *vz, const double *T_)
+{
+    oracle_h *h = (oracle_h *)vh;
+    const double *src[4] = {vx, vy, vz, T_};
+    if (h->precision == 8) {
+        solver_f64 *s = h->s;
+        size_t n = (size_t)s->nx * s->ny * s->nz;
+        for (int v = 0; v < 4; v++) memcpy(s->nv[v], src[v], n * sizeof(double));
+    } else {
+        solver_f32 *s = h->s;
+        size_t n = (size_t)s->nx * s->ny * s->nz;
+        for (int v = 0; v < 4; v++)
+            for (size_t q = 0; q < n; q++) s->nv[v][q] = (float)src[v][q];
+    }
+    return 0;
 }
 
 #define FREE_SOLVER(T)                                                              \

@@ -73,6 +73,9 @@ def _load_oracle():
         lib.oracle_step_tol.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int,
                                         C.POINTER(C.c_int), C.POINTER(C.c_double)]
         lib.oracle_get_fields.argtypes = [C.c_void_p, C.c_int] + [_f64p] * 4
+        lib.oracle_adjoint_run.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                           C.c_void_p, C.POINTER(C.c_double), _f64p, _f64p]
+        lib.oracle_set_node_values.argtypes = [C.c_void_p] + [_f64p] * 4
         lib.oracle_set_state.argtypes = [C.c_void_p] + [_f64p] * 4
         lib.oracle_div_error.restype = C.c_double
         lib.oracle_div_error.argtypes = [C.c_void_p]
@@ -182,6 +185,23 @@ class OracleSolver:
     def time_step(self, dt, num_global, num_local, compute_error=True) -> int:
         """TimeStep without UpdateBoundaries."""
         return self.lib.oracle_time_step(self.h, dt, num_global, num_local, int(compute_error))
+
+    def adjoint_run(self, dt, num_global, num_local, n_steps, box_lo, box_hi):
+        """FP64 discrete adjoint of n_steps steps for J = 1/2 sum_{IN in box} |u|^2 at the
+        end; returns (J, dJ/d node values [4, nx, ny, nz], dJ/d initial state)."""
+        lo = (C.c_int * 3)(*box_lo)
+        hi = (C.c_int * 3)(*box_hi)
+        J = C.c_double(0.0)
+        gnv = np.zeros((4,) + tuple(self.shape), np.float64)
+        gst = np.zeros((4,) + tuple(self.shape), np.float64)
+        rc = self.lib.oracle_adjoint_run(self.h, dt, num_global, num_local, n_steps, lo, hi, C.byref(J), gnv, gst)
+        if rc != 0:
+            raise ValueError("the oracle adjoint needs a double-precision handle")
+        return J.value, gnv, gst
+
+    def set_node_values(self, vx, vy, vz, T):
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (vx, vy, vz, T)]
+        self.lib.oracle_set_node_values(self.h, *arrs)
 
     def step_tol(self, dt, max_global, num_local, tol, compute_error=False):
         """Tolerance-mode step; returns (status, iterations, residual)."""
