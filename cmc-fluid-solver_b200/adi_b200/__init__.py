@@ -15,7 +15,7 @@ from . import _abi
 from ._abi import ADI_FP32, ADI_FP64, ADI_SOLVER_EXACT, ADI_SOLVER_FAST, AdiError  # noqa: F401
 
 __all__ = ["AdiSolver3D", "AdiError", "fluid_params_normalized", "ADI_FP32", "ADI_FP64",
-           "ADI_SOLVER_EXACT", "ADI_SOLVER_FAST", "library_path", "AdiBatch"]
+           "ADI_SOLVER_EXACT", "ADI_SOLVER_FAST", "library_path", "AdiBatch", "AdiSolver2D"]
 
 
 def library_path() -> str:
@@ -262,6 +262,78 @@ class AdiBatch:
         if self.b:
             self.lib.adi_batch_destroy(self.b)
             self.b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class AdiSolver2D:
+    """The reference's 2D ADI solver on the GPU (adi2d_*), Solver2D surface:
+    Init (constructor), UpdateBoundaries, TimeStep, GetLayer, SetLayer."""
+
+    def __init__(self, domain, Re: float = 100.0, Pr: float = 0.72, lam: float = 1.4,
+                 precision: int = _abi.ADI_FP64, stream=None, params=None):
+        self.lib = _abi.load()
+        self.shape = domain.shape
+        self.dtype = np.float64 if precision == _abi.ADI_FP64 else np.float32
+        self.params = params if params is not None else fluid_params_normalized(Re, Pr, lam)
+        self.h = C.c_void_p()
+        _abi.check(self.lib.adi2d_create(domain.nx, domain.ny, domain.dx, domain.dy, precision,
+                                         C.byref(self.params), C.byref(self.h)))
+        if stream is not None:
+            handle = stream if isinstance(stream, int) else getattr(stream, "cuda_stream", stream)
+            self._check(self.lib.adi2d_set_stream(self.h, C.c_void_p(handle)))
+        arrs = [np.ascontiguousarray(domain.type, np.uint8), np.ascontiguousarray(domain.bct, np.uint8)]
+        f = [np.ascontiguousarray(a, np.float64) for a in (domain.vx, domain.vy, domain.T)]
+        self._check(self.lib.adi2d_set_grid(self.h, *[_ptr(a) for a in arrs + f], float(domain.startT)))
+
+    def _check(self, status):
+        if status != _abi.ADI_OK:
+            raw = self.lib.adi2d_last_error_string(self.h) if self.h else b""
+            raise _abi.AdiError(status, raw.decode() if raw else "")
+
+    def UpdateBoundaries(self):
+        self._check(self.lib.adi2d_update_boundaries(self.h))
+
+    def TimeStep(self, dt, num_global, num_local) -> int:
+        it = C.c_int(0)
+        self._check(self.lib.adi2d_time_step(self.h, dt, num_global, num_local, C.byref(it)))
+        return it.value
+
+    def step(self, dt, num_global, num_local):
+        """UpdateBoundaries + TimeStep; returns (status, global iterations)."""
+        it = C.c_int(0)
+        rc = self.lib.adi2d_step(self.h, dt, num_global, num_local, C.byref(it))
+        return rc, it.value
+
+    def fields(self, which: int = 0):
+        out = [np.zeros(self.shape, self.dtype) for _ in range(3)]
+        self._check(self.lib.adi2d_get_state(self.h, which, *[_ptr(a) for a in out]))
+        return out
+
+    def SetLayer(self, u, v, T):
+        arrs = [np.ascontiguousarray(a, self.dtype) for a in (u, v, T)]
+        self._check(self.lib.adi2d_set_state(self.h, *[_ptr(a) for a in arrs]))
+
+    def GetLayer(self, outdimx=0, outdimy=0):
+        ox, oy = outdimx or self.shape[0], outdimy or self.shape[1]
+        vel = np.zeros((ox, oy, 2))
+        T = np.zeros((ox, oy))
+        self._check(self.lib.adi2d_get_layer(self.h, outdimx, outdimy, _ptr(vel), _ptr(T)))
+        return vel, T
+
+    def last_error(self):
+        e, it = C.c_double(), C.c_int()
+        self._check(self.lib.adi2d_last_error(self.h, C.byref(e), C.byref(it)))
+        return e.value, it.value
+
+    def close(self):
+        if self.h:
+            self.lib.adi2d_destroy(self.h)
+            self.h = C.c_void_p()
 
     def __del__(self):
         try:

@@ -273,6 +273,53 @@ adi_status adi_adjoint_run(adi_handle *h, double dt, int num_global, int num_loc
 adi_status adi_set_node_values(adi_handle *h, const double *vx, const double *vy, const double *vz,
                                const double *T);
 
+/* ---- 2D solver ------------------------------------------------------------ */
+
+/* The reference's 2D ADI solver (FluidSolver2D/AdiSolver2D.cpp) on the GPU, with
+ * its own semantics, which differ from the 3D solver's: one segment per grid row /
+ * column spanning every interior obstacle, 1/dt in the rows, FREE rows x0 - x1 = 0,
+ * temp_local copy-then-merge per local iteration, a global loop that runs
+ * num_global iterations and then continues while the divergence error exceeds 0.1,
+ * layer copies that skip the last row and column.  Float results equal the
+ * reference's bit for bit.  Surface: Solver2D / AdiSolver2D (Solver2D.h:23-44). */
+typedef struct adi2d_handle adi2d_handle;
+
+/* Replaces AdiSolver2D::Init's allocation (AdiSolver2D.cpp:20-33). */
+adi_status adi2d_create(int nx, int ny, double dx, double dy, int precision, const adi_fluid_params *params,
+                        adi2d_handle **out);
+adi_status adi2d_destroy(adi2d_handle *h);
+adi_status adi2d_set_stream(adi2d_handle *h, void *cuda_stream);
+
+/* Grid2D node data as arrays [i][j] (j fastest): cell type, BC type, velocity,
+ * temperature (CondData2D, Grid2D.h:31-45); startT is Grid2D::startT.  The state
+ * starts at the node data (AdiSolver2D::Init, AdiSolver2D.cpp:35-47); the segments
+ * are built here (CreateSegments, :228-277). */
+adi_status adi2d_set_grid(adi2d_handle *h, const uint8_t *node_type, const uint8_t *bc_type, const double *vx,
+                          const double *vy, const double *T, double startT);
+
+/* Solver2D::UpdateBoundaries (Solver2D.cpp:40-54). */
+adi_status adi2d_update_boundaries(adi2d_handle *h);
+
+/* AdiSolver2D::TimeStep (AdiSolver2D.cpp:279-323); *iters_used (may be NULL) gets
+ * the global iterations run.  Where the reference calls exit(1) this returns
+ * ADI_ERR_DIVERGENCE (error above 1.0) or ADI_ERR_NOT_CONVERGED (over 100
+ * iterations) and leaves the state unspecified. */
+adi_status adi2d_time_step(adi2d_handle *h, double dt, int num_global, int num_local, int *iters_used);
+
+/* adi2d_update_boundaries + adi2d_time_step (FluidSolver2D.cpp:131-132). */
+adi_status adi2d_step(adi2d_handle *h, double dt, int num_global, int num_local, int *iters_used);
+
+/* which 0: cur (the state), 1: next; handle precision, [i][j]. */
+adi_status adi2d_get_state(adi2d_handle *h, int which, void *u, void *v, void *T);
+/* Solver2D::SetLayer (Solver2D.cpp:30-38): the state. */
+adi_status adi2d_set_state(adi2d_handle *h, const void *u, const void *v, const void *T);
+/* Solver2D::GetLayer (Solver2D.cpp:19-29): next point-sampled on outdimx x outdimy
+ * (0 = full); vel2 gets interleaved (x, y) doubles, T doubles. */
+adi_status adi2d_get_layer(adi2d_handle *h, int outdimx, int outdimy, double *vel2, double *T);
+/* Divergence error and global iterations of the last step. */
+adi_status adi2d_last_error(adi2d_handle *h, double *err, int *iters);
+const char *adi2d_last_error_string(const adi2d_handle *h);
+
 /* ---- batches of domains ------------------------------------------------ */
 
 /* Many independent domains stepped together (no counterpart in the reference,

@@ -235,3 +235,128 @@ class OracleSolver:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------
+# 2D: the restatement (liboracle_adi2d.so) and the reference's own 2D solver
+# (_ref/libref2d.so)
+# ---------------------------------------------------------------------------
+ORACLE2D_LIB = os.path.join(HERE, "liboracle_adi2d.so")
+REF2D_LIB = os.path.join(HERE, "_ref", "libref2d.so")
+_orc2d = None
+_ref2d = None
+
+
+def have_ref2d() -> bool:
+    return os.path.exists(REF2D_LIB)
+
+
+def _load_oracle2d():
+    global _orc2d
+    if _orc2d is None:
+        lib = C.CDLL(ORACLE2D_LIB)
+        lib.oracle2d_create.restype = C.c_void_p
+        lib.oracle2d_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                        _u8p, _u8p, _f64p, _f64p, _f64p]
+        lib.oracle2d_set_params.argtypes = [C.c_void_p] + [C.c_double] * 4
+        lib.oracle2d_step.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int]
+        lib.oracle2d_get_fields.argtypes = [C.c_void_p, C.c_int, _f64p, _f64p, _f64p]
+        lib.oracle2d_last_err.restype = C.c_double
+        lib.oracle2d_last_err.argtypes = [C.c_void_p]
+        lib.oracle2d_segments.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+        lib.oracle2d_destroy.argtypes = [C.c_void_p]
+        _orc2d = lib
+    return _orc2d
+
+
+def _load_ref2d():
+    global _ref2d
+    if _ref2d is None:
+        lib = C.CDLL(REF2D_LIB)
+        lib.ref2d_create.restype = C.c_void_p
+        lib.ref2d_create.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _u8p, _u8p,
+                                     _f64p, _f64p, _f64p, C.c_double, C.c_double, C.c_double]
+        lib.ref2d_step.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int]
+        lib.ref2d_get_fields.argtypes = [C.c_void_p, C.c_int, _f64p, _f64p, _f64p]
+        lib.ref2d_destroy.argtypes = [C.c_void_p]
+        _ref2d = lib
+    return _ref2d
+
+
+def fluid_params2d(Re, Pr, lam, precision):
+    """FluidParams(Re, Pr, lambda) rounded to the working precision (Geometry.h:545-552)."""
+    vals = [1.0, 1.0 / Re, 1.0 / (Re * Pr), (lam - 1) / (lam * Re)]
+    if precision == 4:
+        vals = [float(np.float32(v)) for v in vals]
+    return vals
+
+
+class Oracle2D:
+    """The 2D restatement; precision 4 reproduces the reference float build."""
+
+    def __init__(self, d, precision=8, Re=100.0, Pr=0.72, lam=1.4):
+        self.lib = _load_oracle2d()
+        self.shape = d.shape
+        arrs = [np.ascontiguousarray(a) for a in (d.type.astype(np.uint8), d.bct.astype(np.uint8))]
+        f = [np.ascontiguousarray(a, np.float64) for a in (d.vx, d.vy, d.T)]
+        self.h = self.lib.oracle2d_create(precision, d.nx, d.ny, d.dx, d.dy, d.startT, *arrs, *f)
+        self.lib.oracle2d_set_params(self.h, *fluid_params2d(Re, Pr, lam, precision))
+
+    def step(self, dt, num_global, num_local) -> int:
+        return self.lib.oracle2d_step(self.h, dt, num_global, num_local)
+
+    def fields(self, which=0):
+        out = [np.zeros(self.shape) for _ in range(3)]
+        self.lib.oracle2d_get_fields(self.h, which, *out)
+        return out
+
+    def last_err(self) -> float:
+        return self.lib.oracle2d_last_err(self.h)
+
+    def segments(self) -> np.ndarray:
+        n = self.lib.oracle2d_segments(self.h, None, 0)
+        out = np.zeros((max(n, 1), 6), np.int32)
+        self.lib.oracle2d_segments(self.h, out.ctypes.data, n)
+        return out[:n]
+
+    def close(self):
+        if self.h:
+            self.lib.oracle2d_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Ref2D:
+    """The reference's own AdiSolver2D (float), driven like its driver loop."""
+
+    def __init__(self, d, Re=100.0, Pr=0.72, lam=1.4):
+        self.lib = _load_ref2d()
+        self.shape = d.shape
+        arrs = [np.ascontiguousarray(a) for a in (d.type.astype(np.uint8), d.bct.astype(np.uint8))]
+        f = [np.ascontiguousarray(a, np.float64) for a in (d.vx, d.vy, d.T)]
+        self._keep = (arrs, f)
+        self.h = self.lib.ref2d_create(d.nx, d.ny, d.dx, d.dy, d.startT, *arrs, *f, Re, Pr, lam)
+
+    def step(self, dt, num_global, num_local):
+        self.lib.ref2d_step(self.h, dt, num_global, num_local)
+
+    def fields(self, which=0):
+        out = [np.zeros(self.shape) for _ in range(3)]
+        self.lib.ref2d_get_fields(self.h, which, *out)
+        return out
+
+    def close(self):
+        if self.h:
+            self.lib.ref2d_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
