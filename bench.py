@@ -80,6 +80,16 @@ CONFIGS = {
                       desc="batched: 64 independent 3D FP32 domains, axes U{64..160} (seed 2), 10-60 solid spheres "
                            "each (radii U[4,12]), Re U[50,400], dt=5e-4, num_global=4, num_local=2; all domains "
                            "in one persistent launch per sweep, step replayed as a CUDA graph"),
+    "adjoint128": dict(make=_spheres128, adjoint=True, Re=200.0, Pr=0.72, lam=1.4, dt=5e-4, ng=4, nl=2,
+                       n_steps=40, ckpt=8, box=((80, 48, 48), (112, 80, 80)), near_box=((2, 48, 48), (34, 80, 80)),
+                       desc="adjoint: 128^3 FP32, 40 spheres (seed 0), Re=200, dt=5e-4, num_global=4, num_local=2, "
+                            "40 forward steps checkpointed every 8; J = kinetic energy of the fluid in the 32^3 box "
+                            "x in [80,112), y, z in [48,80); gradient w.r.t. 16 sine-product coefficients of the "
+                            "inflow profile"),
+    "channel2d": dict(make=None, two_d=True, Re=100.0, Pr=0.72, lam=1.4, dt=1e-3, ng=4, nl=1, n_steps=100,
+                      desc="plain 2D ADI: 256x128 FP64 channel, dx=dy=1/128, disc radius 12 at (64,64), parabolic "
+                           "inflow (max 1.0), no-slip walls, BC_FREE outflow, Re=100, dt=1e-3, num_global=4 "
+                           "(the reference's loop continues while its divergence error exceeds 0.1), num_local=1"),
     "spheres64": dict(make=_spheres64, Re=200.0, Pr=0.72, lam=1.4, dt=5e-4, ng=4, nl=2,
                       desc="small case for profiling: 64^3 FP32, 10 spheres, Re=200, dt=5e-4, "
                            "num_global=4, num_local=2"),
@@ -212,6 +222,31 @@ def run_reference(args):
     if rank != 0:
         return 0
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+    if cfg.get("two_d"):
+        import oracle as O
+        from adi_b200 import geometry2d as G2
+        d = G2.channel_disc()
+        r = O.Ref2D(d, Re=cfg["Re"], Pr=cfg["Pr"], lam=cfg["lam"])
+        with stdout_to_stderr():
+            for _ in range(min(args.warmup, 1)):
+                r.step(cfg["dt"], cfg["ng"], cfg["nl"])
+            t0 = time.perf_counter()
+            done = 0
+            while done < args.steps and time.perf_counter() - t0 < args.ref_budget:
+                r.step(cfg["dt"], cfg["ng"], cfg["nl"])
+                done += 1
+            el = time.perf_counter() - t0
+        value = d.cells * done / el
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+            "steps": done, "warmup": args.warmup, "ms_per_step": 1e3 * el / done, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{args.config}: {cfg['desc']}", "cells": d.cells},
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": 1, "kind": "reference",
+                             "sample": f"{done} steps ({el:.1f} s), the reference 2D solver (single-threaded)"},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }), flush=True)
+        return 0
     if cfg.get("batch"):
         domains = cfg["make"]()
         with stdout_to_stderr():
@@ -573,6 +608,202 @@ def run_batch(args):
     return 0
 
 
+def inflow_basis(ny, nz, n=4):
+    y = np.arange(ny) / (ny - 1)
+    z = np.arange(nz) / (nz - 1)
+    return np.stack([np.outer(np.sin((a + 1) * np.pi * y), np.sin((b + 1) * np.pi * z))
+                     for a in range(n) for b in range(n)])
+
+
+def run_adjoint(args):
+    """Adjoint workload: forward time of n_steps steps, time of the adjoint run
+    (forward with checkpoints + recomputation + backward), their ratio, and the
+    theta-gradient against FP64 central differences of the GPU FP64 forward."""
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    import adi_b200
+    cfg = CONFIGS[args.config]
+    d = cfg["make"]()
+    stream = torch.cuda.current_stream()
+    dt, ng, nl, ns, ck = cfg["dt"], cfg["ng"], cfg["nl"], cfg["n_steps"], cfg["ckpt"]
+    s = adi_b200.AdiSolver3D(d, Re=cfg["Re"], Pr=cfg["Pr"], lam=cfg["lam"], precision=adi_b200.ADI_FP32,
+                             stream=stream.cuda_stream)
+    s.CreateSegments()
+    init = [a.copy() for a in s.fields(0)]
+    phi = inflow_basis(d.ny, d.nz)
+
+    def theta_grad(gnv):
+        return np.tensordot(phi[:, 1:-1, 1:-1], gnv[0][0, 1:-1, 1:-1].astype(np.float64), axes=([1, 2], [0, 1]))
+
+    # warm-up: one short forward and one short adjoint
+    for i in range(args.warmup):
+        s.step(dt, ng, nl, False)
+    s.set_state(*init)
+    s.adjoint_run(dt, ng, nl, 2, 1, *cfg["box"])
+    s.set_state(*init)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(ns):
+        rc = s.step(dt, ng, nl, False)
+        if rc != 0:
+            raise RuntimeError(f"adi_step failed with status {rc}")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fwd_ms = e0.elapsed_time(e1)
+    s.set_state(*init)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    J, gnv, _ = s.adjoint_run(dt, ng, nl, ns, ck, *cfg["box"])
+    adj_ms = 1e3 * (time.perf_counter() - t0)
+    clk = clocks.stop()
+    g_far = theta_grad(gnv)
+
+    # gradient check: the same run with the box next to the inflow (the 32^3 box at
+    # x >= 80 is beyond the reach of 40 steps at dt = 5e-4, so its gradient is zero)
+    s.set_state(*init)
+    Jn, gnv_n, _ = s.adjoint_run(dt, ng, nl, ns, ck, *cfg["near_box"])
+    g_near = theta_grad(gnv_n)
+    s64 = adi_b200.AdiSolver3D(d, Re=cfg["Re"], Pr=cfg["Pr"], lam=cfg["lam"], precision=adi_b200.ADI_FP64,
+                               stream=stream.cuda_stream)
+    s64.CreateSegments()
+    lo, hi = cfg["near_box"]
+    m = np.zeros(d.shape, bool)
+    m[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] = True
+    m &= d.type == G.NODE_IN
+
+    def J64(th):
+        vx = d.vx.copy()
+        vx[0, 1:-1, 1:-1] = (1.0 + np.tensordot(th, phi, axes=1))[1:-1, 1:-1]
+        s64.set_node_values(vx, d.vy, d.vz, d.T)
+        s64.set_state(*init)
+        for _ in range(ns):
+            s64.step(dt, ng, nl, False)
+        u = s64.fields(0)
+        return 0.5 * sum(float(np.sum(u[f][m] ** 2)) for f in range(3))
+
+    fd = np.zeros(16)
+    for q in range(16):
+        e = np.zeros(16)
+        e[q] = 1e-3
+        fd[q] = (J64(e) - J64(-e)) / 2e-3
+    rel = float(np.max(np.abs(g_near - fd)) / max(np.max(np.abs(fd)), 1e-300))
+    step_bytes = 0
+    line = {
+        "metric": METRIC, "value": d.cells * ns / (adj_ms / 1e3), "unit": METRIC, "n_gpus": 1, "steps": ns,
+        "warmup": args.warmup, "ms_per_step": adj_ms / ns, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{args.config}: {cfg['desc']}", "cells": d.cells, "checkpoint_every": ck,
+                   "l2": "working set (tape of 8 steps, 12 GB) far above L2"},
+        "adjoint_over_forward": adj_ms / fwd_ms, "forward_ms": fwd_ms, "adjoint_ms": adj_ms,
+        "J": J, "grad_theta_far_box_max_abs": float(np.max(np.abs(g_far))),
+        "grad_check": {"box": cfg["near_box"], "J": Jn, "max_rel_err_vs_fp64_central_fd": rel, "fd_h": 1e-3,
+                       "grad": [float(x) for x in g_near], "fd": [float(x) for x in fd]},
+        "e2e": {"value": d.cells * ns / (adj_ms / 1e3), "unit": METRIC, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0, "note": "the adjoint call is the public API; its host wall time is the value"},
+        "gpu_launches": None,
+        "clocks": clk,
+    }
+    del step_bytes
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    s.close()
+    s64.close()
+    return 0
+
+
+def run_2d(args):
+    """2D workload (the reference's AdiSolver2D semantics), FP64."""
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    import adi_b200
+    from adi_b200 import geometry2d as G2
+    cfg = CONFIGS[args.config]
+    d = G2.channel_disc()
+    stream = torch.cuda.current_stream()
+    g = adi_b200.AdiSolver2D(d, Re=cfg["Re"], Pr=cfg["Pr"], lam=cfg["lam"], stream=stream.cuda_stream)
+    dt, ng, nl = cfg["dt"], cfg["ng"], cfg["nl"]
+    steps = args.steps if args.steps else cfg["n_steps"]
+    for i in range(args.warmup):
+        assert g.step(dt, ng, nl)[0] == 0
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    iters = []
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for i in range(steps):
+        ev[i][0].record(stream)
+        rc, it = g.step(dt, ng, nl)
+        ev[i][1].record(stream)
+        if rc != 0:
+            raise RuntimeError(f"adi2d_step failed with status {rc}")
+        iters.append(it)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    total_ms = float(sum(a.elapsed_time(b) for a, b in ev))
+    value = world * d.cells * steps / (total_ms / 1e3)
+    # end to end with host buffers
+    pinned = [torch.empty(d.shape, dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)]
+    for a, b in zip(pinned, g.fields(0)):
+        a[...] = b
+    e2e_steps = max(1, min(steps, 20))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(e2e_steps):
+        g.SetLayer(*pinned)
+        g.step(dt, ng, nl)
+        g._check(g.lib.adi2d_get_state(g.h, 0, *[p.ctypes.data for p in pinned]))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_value = d.cells * e2e_steps / (e0.elapsed_time(e1) / 1e3)
+    # algorithmic bytes of one global iteration's two sweeps: per node read cur and
+    # temp_local (3 fields each) and write next_local (3 fields), 8-byte values
+    peak, peak_kind = measured_peaks()
+    mean_iters = float(np.mean(iters))
+    step_bytes = mean_iters * 2 * nl * d.cells * 9 * 8
+    achieved = step_bytes / (total_ms / steps / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.config}: {cfg['desc']}", "cells": d.cells,
+                   "global_iterations_per_step": mean_iters,
+                   "l2": "the whole 2D state (under 3 MB) stays in L2; each step is one graph launch and one "
+                         "read of the iteration errors"},
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 3 * 8 * d.cells,
+                "d2h_bytes_per_step": 3 * 8 * d.cells, "steps": e2e_steps},
+        "gpu_launches": None,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if peak else None, "traffic": None, "kernel": "whole 2D step",
+                     "peak_source": peak_kind,
+                     "note": "32K cells: latency- and launch-bound, not bandwidth-bound"},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle as O
+        if not O.have_ref2d():
+            O.build()
+        r = O.Ref2D(d, Re=cfg["Re"], Pr=cfg["Pr"], lam=cfg["lam"])
+        with stdout_to_stderr():
+            t0 = time.perf_counter()
+            done = 0
+            while done < steps and time.perf_counter() - t0 < args.cpu_budget:
+                r.step(dt, ng, nl)
+                done += 1
+            el = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": d.cells * done / el, "unit": METRIC, "cores": 1, "kind": "reference",
+                                "sample": f"{done} steps ({el:.1f} s) of the reference's 2D solver (float build, "
+                                          f"single-threaded as written)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    g.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -596,6 +827,10 @@ def main():
         return run_reference(args)
     if CONFIGS[args.config].get("batch"):
         return run_batch(args)
+    if CONFIGS[args.config].get("adjoint"):
+        return run_adjoint(args)
+    if CONFIGS[args.config].get("two_d"):
+        return run_2d(args)
     return run_ours(args)
 
 
