@@ -120,6 +120,9 @@ class AdiSolver3D:
         arrs = [np.ascontiguousarray(a, np.float64) for a in (vx, vy, vz, T)]
         self._check(self.lib.adi_set_node_values(self.h, *[_ptr(a) for a in arrs]))
 
+    def set_adjoint_chunk(self, K: int):
+        self._check(self.lib.adi_set_adjoint_chunk(self.h, K))
+
     def step_tol(self, dt, max_global, num_local, tol, compute_error=False):
         """UpdateBoundaries + TimeStep in tolerance mode; returns (status, iterations, residual)."""
         it, res = C.c_int(0), C.c_double(0.0)

@@ -33,7 +33,7 @@ EXPORTED = [
     "adi_batch_create", "adi_batch_destroy", "adi_batch_set_stream", "adi_batch_step", "adi_batch_div_errors",
     "adi_batch_set_chunk", "adi_batch_get_chunk", "adi_batch_autotune", "adi_batch_set_graphs",
     "adi_batch_launches", "adi_batch_last_error_string", "adi_batch_time_sweeps", "adi_adjoint_run",
-    "adi_set_node_values", "adi2d_create", "adi2d_destroy", "adi2d_set_stream", "adi2d_set_grid",
+    "adi_set_node_values", "adi_set_adjoint_chunk", "adi2d_create", "adi2d_destroy", "adi2d_set_stream", "adi2d_set_grid",
     "adi2d_update_boundaries", "adi2d_time_step", "adi2d_step", "adi2d_get_state", "adi2d_set_state",
     "adi2d_get_layer", "adi2d_last_error", "adi2d_last_error_string",
 ]
@@ -116,6 +116,7 @@ def load() -> C.CDLL:
         "adi_batch_time_sweeps": [vp, d, i, vp],
         "adi_adjoint_run": [vp, d, i, i, i, i, vp, vp, C.POINTER(d), vp, vp],
         "adi_set_node_values": [vp, vp, vp, vp, vp],
+        "adi_set_adjoint_chunk": [vp, i],
         "adi2d_create": [i, i, d, d, i, C.POINTER(FluidParams), C.POINTER(vp)],
         "adi2d_destroy": [vp],
         "adi2d_set_stream": [vp, vp],

@@ -36,6 +36,7 @@ SOURCES = [
     ("sweep_xytma.cu", []),
     ("sweep_xypair.cu", []),
     ("adjoint.cu", []),
+    ("adjoint_fast.cu", []),
     ("adi2d.cu", ["--fmad=false"]),
 ]
 

@@ -91,6 +91,7 @@ struct adi_handle {
     std::vector<GraphEntry> graphs;
     bool graphs_on = true;
     cudaStream_t cap_stream = nullptr;
+    int adjoint_K = 4;   // chunk length of the adjoint sweep; 0: one thread per line
     std::string contract_msg;
     std::string err;
     double diff_error = 0.0;
@@ -660,17 +661,20 @@ adi_status time_step_tol(adi_handle *h, double dt, int max_global, int num_local
 // nonlinear layer read and the layer written) and run backward.
 // ---------------------------------------------------------------------------
 
-struct DevBuffers {
-    std::vector<void *> ptrs;
-    ~DevBuffers()
-    {
-        for (void *p : ptrs) cudaFree(p);
-    }
+// One device allocation carved into 256-byte aligned pieces (thousands of tape
+// fields would otherwise cost a cudaMalloc each).
+struct DevArena {
+    char *base = nullptr;
+    size_t cap = 0, used = 0;
+    ~DevArena() { cudaFree(base); }
+    cudaError_t reserve(size_t bytes) { cap = bytes; return cudaMalloc((void **)&base, bytes); }
     void *get(size_t bytes, cudaError_t &e)
     {
-        void *p = nullptr;
-        if (e == cudaSuccess) e = cudaMalloc(&p, bytes);
-        if (e == cudaSuccess) ptrs.push_back(p);
+        const size_t b = (bytes + 255) / 256 * 256;
+        if (e != cudaSuccess) return nullptr;
+        if (used + b > cap) { e = cudaErrorMemoryAllocation; return nullptr; }
+        void *p = base + used;
+        used += b;
         return p;
     }
 };
@@ -699,8 +703,9 @@ adi_status adjoint_run(adi_handle *h, double dt, int ng, int nl, int n_steps, in
     const int S = ng * nl * 3;
     const int nck = (n_steps + ck - 1) / ck;
     const int win = ck < n_steps ? ck : n_steps;
-    DevBuffers mem;
-    cudaError_t e = cudaSuccess;
+    const size_t fbr = (fb + 255) / 256 * 256;
+    DevArena mem;
+    cudaError_t e = mem.reserve(fbr * ((size_t)nck * 4 + 4 * 6 + 2 + (size_t)win * S * 8) + 256 * (DIV_BLOCKS + 16));
     auto layer4 = [&](void **out) {
         for (int v = 0; v < 4; v++) out[v] = mem.get(fb, e);
     };
@@ -780,7 +785,7 @@ adi_status adjoint_run(adi_handle *h, double dt, int ng, int nl, int n_steps, in
                                                            clayer_of<R>(tp + (size_t)q * 8 + 4), layer_of<R>(sb),
                                                            layer_of<R>(db), layer_of<R>(tb.data()),
                                                            layer_of<R>(nvb.data()), ga, gbp, (R *)h->d_scratch, k,
-                                                           merges, h->stream);
+                                                           merges, h->adjoint_K, h->stream);
                         }));
                     }
                 }
@@ -1148,6 +1153,13 @@ adi_status adi_adjoint_run(adi_handle *h, double dt, int num_global, int num_loc
     if (h->prec == ADI_FP64) return adjoint_run<double>(h, dt, num_global, num_local, n_steps, ckpt_every, lo, hi, J,
                                                         nv_grad, state_grad);
     return adjoint_run<float>(h, dt, num_global, num_local, n_steps, ckpt_every, lo, hi, J, nv_grad, state_grad);
+}
+
+adi_status adi_set_adjoint_chunk(adi_handle *h, int K)
+{
+    if (!h || (K != 0 && K != 4 && K != 8)) return ADI_ERR_BAD_ARG;
+    h->adjoint_K = K;
+    return ADI_OK;
 }
 
 adi_status adi_set_node_values(adi_handle *h, const double *vx, const double *vy, const double *vz, const double *T)

@@ -311,20 +311,27 @@ __global__ void objective_final_kernel(const double *psum, int nblocks, double *
 template <typename R>
 cudaError_t launch_adjoint_sweep(int dir, const DomainView<R> &d, const int *lo, const int *hi, CLayer<R> ti,
                                  CLayer<R> xs, Layer<R> sbar, Layer<R> dbar, Layer<R> tbar, Layer<R> nvbar, R *ga, R *gb,
-                                 R *scratch, const SweepConst<R> &k, int merges, cudaStream_t s)
+                                 R *scratch, const SweepConst<R> &k, int merges, int chunk_K, cudaStream_t s)
 {
     const LineGeom g = line_geom(dir, d.nx, d.ny, d.nz);
     cudaError_t e = cudaMemsetAsync(ga, 0, sizeof(R) * d.n, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(gb, 0, sizeof(R) * d.n, s);
     if (e != cudaSuccess) return e;
+    int NL = 0, P = 0;
+    const bool chunked = chunk_K > 0 && adjoint_chunk_supported(g.len, chunk_K, (int)sizeof(R), NL, P);
     const int blocks = (g.nlines + 127) / 128;
     long long gb_ = (d.n + 255) / 256;
     const int gblocks = (int)(gb_ > 148 * 16 ? 148 * 16 : gb_);
 #define AS(DD)                                                                                                   \
     if (dir == DD) {                                                                                             \
-        adjoint_sweep_kernel<R, DD><<<blocks, 128, 0, s>>>(d, g, lo, hi, ti, xs, sbar, dbar, tbar, nvbar, ga, gb,  \
-                                                           scratch, k, merges);                                   \
-        e = cudaGetLastError();                                                                                  \
+        if (chunked)                                                                                             \
+            e = launch_adjoint_chunk<R>(DD, chunk_K, d, lo, hi, ti, xs, sbar, dbar, tbar, nvbar, ga, gb, k,       \
+                                        merges, s);                                                              \
+        else {                                                                                                   \
+            adjoint_sweep_kernel<R, DD><<<blocks, 128, 0, s>>>(d, g, lo, hi, ti, xs, sbar, dbar, tbar, nvbar, ga, \
+                                                               gb, scratch, k, merges);                          \
+            e = cudaGetLastError();                                                                              \
+        }                                                                                                        \
         if (e != cudaSuccess) return e;                                                                          \
         adjoint_gather_kernel<R, DD><<<gblocks, 256, 0, s>>>(d, tbar.f[DD], ga, gb, k);                          \
         return cudaGetLastError();                                                                               \
@@ -359,7 +366,7 @@ cudaError_t launch_objective(const DomainView<R> &d, CLayer<R> x, const int lo[3
 #define INST(R)                                                                                                     \
     template cudaError_t launch_adjoint_sweep<R>(int, const DomainView<R> &, const int *, const int *, CLayer<R>,   \
                                                  CLayer<R>, Layer<R>, Layer<R>, Layer<R>, Layer<R>, R *, R *, R *,  \
-                                                 const SweepConst<R> &, int, cudaStream_t);                         \
+                                                 const SweepConst<R> &, int, int, cudaStream_t);                    \
     template cudaError_t launch_adjoint_step_start<R>(const DomainView<R> &, Layer<R>, Layer<R>, Layer<R>, Layer<R>, \
                                                       cudaStream_t);                                                \
     template cudaError_t launch_objective<R>(const DomainView<R> &, CLayer<R>, const int *, const int *, Layer<R>,  \

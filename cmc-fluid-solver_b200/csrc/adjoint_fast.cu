@@ -1,0 +1,352 @@
+// Chunked adjoint sweep: the transposed tridiagonal solve of adjoint.cu with the
+// parallel structure of the fast forward sweep (sweep_fast.cu).
+//
+// Each thread owns K consecutive rows of one line.  It builds its rows of A^T
+// (sub-diagonal: row p-1's c, diagonal: row p's b, super-diagonal: row p+1's a,
+// for the velocity and the temperature matrix) and the right-hand sides xbar (the
+// destination's adjoint on segment rows plus the merge's share of the temp
+// adjoint), eliminates its interior rows (eliminate_abc), and the chunk-first /
+// chunk-last unknowns of the line's P chunks are solved by one cyclic-reduction
+// step and parallel cyclic reduction through shared memory, as in the forward.
+// The accumulations then happen per owned row; the contributions a row makes to
+// its neighbours p-1 and p+1 (pressure term, along-line dissipation terms) stay
+// in the thread or cross one chunk boundary through shared memory, so every
+// cell of tbar has one writer.  Off-line dissipation terms go through the two
+// planes that adjoint_gather_kernel (adjoint.cu) folds in afterwards.
+#include "adi_internal.cuh"
+#include "sweep_common.cuh"
+
+#include <climits>
+
+namespace adi {
+
+namespace {
+
+enum : int { Q_NONE = 0, Q_START = 1, Q_IN = 2, Q_END = 3, Q_SHARED = 4 };
+
+__device__ __forceinline__ int qkind(bool inm, bool in0, bool inp)
+{
+    if (in0) return Q_IN;
+    if (inm && inp) return Q_SHARED;
+    if (inp) return Q_START;
+    if (inm) return Q_END;
+    return Q_NONE;
+}
+
+// Entries (a, b, c) of forward row p for matrix m from its kind, BC code and
+// advection term r.
+template <typename R>
+__device__ __forceinline__ void fwd_entries(int kind, uint8_t code, int m, R r, const SweepConst<R> &k, R &a, R &b,
+                                            R &c)
+{
+    const R vis = m == 0 ? k.vis_v : k.vis_t;
+    const bool fr = m == 0 ? (code & CODE_VEL_FREE) != 0 : (code & CODE_TEMP_FREE) != 0;
+    if (kind == Q_IN) {
+        a = -r - vis;
+        b = m == 0 ? k.b_v : k.b_t;
+        c = r - vis;
+    } else if (kind == Q_START) {
+        a = R(0);
+        b = fr ? R(2) : R(1);
+        c = fr ? R(-1) : R(0);
+    } else if (kind == Q_END) {
+        a = fr ? R(-1) : R(0);
+        b = fr ? R(2) : R(1);
+        c = R(0);
+    } else {   // SHARED (Dirichlet by the solver contract) and NONE
+        a = R(0);
+        b = R(1);
+        c = R(0);
+    }
+}
+
+template <int DIR>
+__device__ __forceinline__ int aslot(int li, int c, int q, int NL, int P)
+{
+    if (DIR == 2) return (li * 8 + q) * P + c;
+    return (c * 8 + q) * NL + li;
+}
+
+} // namespace
+
+template <typename R, int DIR, int K>
+__global__ void __launch_bounds__(256)
+    adjoint_chunk_kernel(DomainView<R> d, LineGeom g, int NL, int P, const int *__restrict__ line_lo,
+                         const int *__restrict__ line_hi, CLayer<R> ti, CLayer<R> xs, Layer<R> sbar, Layer<R> dbar,
+                         Layer<R> tbar, Layer<R> nvbar, R *__restrict__ ga, R *__restrict__ gb, SweepConst<R> kc,
+                         int merges)
+{
+    using namespace sweep;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R *buf0 = reinterpret_cast<R *>(smem_raw);
+    R *buf1 = buf0 + (size_t)NL * P * 8;
+    const int t = threadIdx.x;
+    int li, ch;
+    if (DIR == 2) { li = t / P; ch = t - li * P; }
+    else { ch = t / NL; li = t - ch * NL; }
+    const int line = blockIdx.x * NL + li;
+    int lo = INT_MAX, hi = -1;
+    long long base = 0;
+    if (line < g.nlines) {
+        const int a = line_lo[line];
+        if (a >= 0) { lo = a; hi = line_hi[line]; }
+        base = line_base(DIR, g, line);
+    }
+    const long long sl = g.stride;
+    const long long sx = (long long)g.ny * g.nz, sy = g.nz;
+    const long long so1 = DIR == 0 ? sy : sx;
+    const long long so2 = DIR == 2 ? sy : 1;
+    const R h1 = DIR == 0 ? kc.inv_two_dy : kc.inv_two_dx;
+    const R h2 = DIR == 2 ? kc.inv_two_dy : kc.inv_two_dz;
+    const int p0 = ch * K;
+    const bool active = p0 <= hi && p0 + K - 1 >= lo;
+    const R mx = merges == 2 ? R(0.75) : R(0.5);
+    const R mt = merges == 2 ? R(0.25) : R(0.5);
+
+    // ---------------- rows: kinds, window values, A^T and xbar ----------------
+    uint8_t cc[K + 4];   // codes of rows p0-2 .. p0+K+1 (OUT outside the segment range)
+#pragma unroll
+    for (int q = 0; q < K + 4; q++) {
+        const int p = p0 - 2 + q;
+        cc[q] = (active && p >= lo && p <= hi) ? d.code[base + (long long)p * sl] : uint8_t(NODE_OUT);
+    }
+    int kd[K + 2];   // kinds of rows p0-1 .. p0+K
+#pragma unroll
+    for (int q = 0; q < K + 2; q++) kd[q] = qkind(code_is_in(cc[q]), code_is_in(cc[q + 1]), code_is_in(cc[q + 2]));
+    R wv[K + 2];     // advecting temp at window rows (IN rows only)
+    R xw[4][K + 2];  // the sweep's output x at window rows (segment rows)
+#pragma unroll
+    for (int q = 0; q < K + 2; q++) {
+        const long long off = base + (long long)(p0 - 1 + q) * sl;
+        wv[q] = kd[q] == Q_IN ? ti.f[DIR][off] : R(0);
+#pragma unroll
+        for (int v = 0; v < 4; v++) xw[v][q] = kd[q] != Q_NONE ? xs.f[v][off] : R(0);
+    }
+    R A[2][K], B[2][K], C[2][K], xb[4][K], tob[4][K];
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        const int q = i + 1;
+        const long long off = base + (long long)(p0 + i) * sl;
+#pragma unroll
+        for (int m = 0; m < 2; m++) {
+            R a0, b0, c0, am, bm, cm, ap, bp, cp;
+            fwd_entries<R>(kd[q], cc[q + 1], m, wv[q] * kc.inv_two_h, kc, a0, b0, c0);
+            fwd_entries<R>(kd[q - 1], cc[q], m, wv[q - 1] * kc.inv_two_h, kc, am, bm, cm);
+            fwd_entries<R>(kd[q + 1], cc[q + 2], m, wv[q + 1] * kc.inv_two_h, kc, ap, bp, cp);
+            A[m][i] = cm;   // A^T[p][p-1] = A[p-1][p]
+            B[m][i] = b0;
+            C[m][i] = ap;   // A^T[p][p+1] = A[p+1][p]
+            (void)a0; (void)c0; (void)bm; (void)am; (void)bp; (void)cp;
+        }
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            const R db = kd[q] != Q_NONE ? dbar.f[v][off] : R(0);
+            const R to = kd[q] != Q_NONE ? tbar.f[v][off] : R(0);
+            tob[v][i] = to;
+            xb[v][i] = db + (kd[q] == Q_IN ? mx * to : R(0));
+        }
+    }
+
+    // ---------------- chunk elimination of A^T ----------------
+    R ea[2][K], ec[2][K];
+    Reduced<R> red;
+    eliminate_abc<R, K>(A, B, C, xb, ea, ec, red);
+
+    // ---------------- reduced system: one CR step + PCR (as in sweep_fast.cu) ----------------
+    buf0[aslot<DIR>(li, ch, 0, NL, P)] = red.Al[0];
+    buf0[aslot<DIR>(li, ch, 1, NL, P)] = red.Cl[0];
+    buf0[aslot<DIR>(li, ch, 2, NL, P)] = red.Al[1];
+    buf0[aslot<DIR>(li, ch, 3, NL, P)] = red.Cl[1];
+#pragma unroll
+    for (int v = 0; v < 4; v++) buf0[aslot<DIR>(li, ch, 4 + v, NL, P)] = red.Dl[v];
+    __syncthreads();
+    R ea_[2], ec_[2], ed[4];
+    {
+        R pv[8] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};
+        if (ch > 0) {
+#pragma unroll
+            for (int q = 0; q < 8; q++) pv[q] = buf0[aslot<DIR>(li, ch - 1, q, NL, P)];
+        }
+        cr_step<R>(red, pv, ea_, ec_, ed);
+    }
+    int nstep = 0;
+    for (int s = 1; s < P; s <<= 1, nstep++) {
+        R *bw = (nstep & 1) ? buf0 : buf1;
+        bw[aslot<DIR>(li, ch, 0, NL, P)] = ea_[0];
+        bw[aslot<DIR>(li, ch, 1, NL, P)] = ec_[0];
+        bw[aslot<DIR>(li, ch, 2, NL, P)] = ea_[1];
+        bw[aslot<DIR>(li, ch, 3, NL, P)] = ec_[1];
+#pragma unroll
+        for (int v = 0; v < 4; v++) bw[aslot<DIR>(li, ch, 4 + v, NL, P)] = ed[v];
+        __syncthreads();
+        R mv[8] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};
+        R pv[8] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};
+        if (ch - s >= 0) {
+#pragma unroll
+            for (int q = 0; q < 8; q++) mv[q] = bw[aslot<DIR>(li, ch - s, q, NL, P)];
+        }
+        if (ch + s < P) {
+#pragma unroll
+            for (int q = 0; q < 8; q++) pv[q] = bw[aslot<DIR>(li, ch + s, q, NL, P)];
+        }
+        pcr_update<R>(mv, pv, ea_, ec_, ed);
+    }
+    R *bx = (nstep & 1) ? buf0 : buf1;
+#pragma unroll
+    for (int v = 0; v < 4; v++) bx[aslot<DIR>(li, ch, v, NL, P)] = ed[v];
+    __syncthreads();
+    R lf[4], ll[4];
+    {
+        R nf[4] = {R(0), R(0), R(0), R(0)};
+        if (ch + 1 < P) {
+#pragma unroll
+            for (int v = 0; v < 4; v++) nf[v] = bx[aslot<DIR>(li, ch + 1, v, NL, P)];
+        }
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            const int m = v < 3 ? 0 : 1;
+            lf[v] = ed[v];
+            ll[v] = red.Dl[v] - red.Al[m] * lf[v] - red.Cl[m] * nf[v];
+        }
+    }
+
+    // ---------------- accumulations per owned row ----------------
+    R up[4][K], dn[4][K];   // contributions of row i to rows p+1 (up) and p-1 (dn): u, v, w, T
+    R wb[K];
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        const int q = i + 1;
+        const long long off = base + (long long)(p0 + i) * sl;
+        R lam[4];
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            const int m = v < 3 ? 0 : 1;
+            lam[v] = i == 0 ? lf[v] : (i == K - 1 ? ll[v] : xb[v][i] - ea[m][i] * lf[v] - ec[m][i] * ll[v]);
+        }
+#pragma unroll
+        for (int v = 0; v < 4; v++) { up[v][i] = R(0); dn[v][i] = R(0); }
+        wb[i] = R(0);
+        if (!active || kd[q] == Q_NONE) continue;
+#pragma unroll
+        for (int v = 0; v < 4; v++) dbar.f[v][off] = R(0);   // the sweep overwrote the destination here
+        if (kd[q] != Q_IN) {
+            const uint8_t c = cc[q + 1];
+            const bool shared = kd[q] == Q_SHARED;
+            const bool vf = !shared && (c & CODE_VEL_FREE) != 0, tf = !shared && (c & CODE_TEMP_FREE) != 0;
+            if (!vf) {
+#pragma unroll
+                for (int v = 0; v < 3; v++) nvbar.f[v][off] += lam[v];
+            }
+            if (!tf) nvbar.f[3][off] += lam[3];
+            continue;
+        }
+#pragma unroll
+        for (int v = 0; v < 4; v++) sbar.f[v][off] += kc.three_dt * lam[v];
+        R w = R(0);
+#pragma unroll
+        for (int v = 0; v < 4; v++) w += lam[v] * (xw[v][q - 1] - xw[v][q + 1]);
+        wb[i] = w * kc.inv_two_h;
+        const R pt = kc.v_T * lam[DIR] * kc.inv_two_h;
+        up[3][i] = -pt;
+        dn[3][i] = pt;
+        const R gl = kc.t_phi * lam[3];
+        const R *U = ti.f[0], *V = ti.f[1], *Wt = ti.f[2];
+        const R ua = (U[off + sl] - U[off - sl]) * kc.inv_two_h;
+        const R va = (V[off + sl] - V[off - sl]) * kc.inv_two_h;
+        const R wa = (Wt[off + sl] - Wt[off - sl]) * kc.inv_two_h;
+        const R *Fd = ti.f[DIR];
+        const R f1 = (Fd[off + so1] - Fd[off - so1]) * h1;
+        const R f2 = (Fd[off + so2] - Fd[off - so2]) * h2;
+        R gu, gv, gw, g1, g2;
+        if (DIR == 0) {
+            gu = R(4) * ua; gv = R(2) * va + f1; gw = R(2) * wa + f2; g1 = va; g2 = wa;
+        } else if (DIR == 1) {
+            gu = R(2) * ua + f1; gv = R(4) * va; gw = R(2) * wa + f2; g1 = ua; g2 = wa;
+        } else {
+            gu = R(2) * ua + f1; gv = R(2) * va + f2; gw = R(4) * wa; g1 = ua; g2 = va;
+        }
+        const R s_h = gl * kc.inv_two_h;
+        up[0][i] = gu * s_h; dn[0][i] = -gu * s_h;
+        up[1][i] = gv * s_h; dn[1][i] = -gv * s_h;
+        up[2][i] = gw * s_h; dn[2][i] = -gw * s_h;
+        ga[off] = gl * g1;
+        gb[off] = gl * g2;
+    }
+    // chunk-boundary neighbours: the previous chunk's last row sends up, the next
+    // chunk's first row sends down
+    R *bz = (nstep & 1) ? buf1 : buf0;   // not bx: stage (c) may still be reading it
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+        bz[aslot<DIR>(li, ch, v, NL, P)] = up[v][K - 1];
+        bz[aslot<DIR>(li, ch, 4 + v, NL, P)] = dn[v][0];
+    }
+    __syncthreads();
+    if (!active) return;
+    R upp[4] = {R(0), R(0), R(0), R(0)}, dnn[4] = {R(0), R(0), R(0), R(0)};
+    if (ch > 0) {
+#pragma unroll
+        for (int v = 0; v < 4; v++) upp[v] = bz[aslot<DIR>(li, ch - 1, v, NL, P)];
+    }
+    if (ch + 1 < P) {
+#pragma unroll
+        for (int v = 0; v < 4; v++) dnn[v] = bz[aslot<DIR>(li, ch + 1, 4 + v, NL, P)];
+    }
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        const int q = i + 1;
+        if (kd[q] == Q_NONE) continue;
+        const long long off = base + (long long)(p0 + i) * sl;
+        const bool in = kd[q] == Q_IN;
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            R x = (in ? mt : R(1)) * tob[v][i];
+            if (v == DIR) x += wb[i];
+            x += i > 0 ? up[v][i - 1] : upp[v];
+            x += i < K - 1 ? dn[v][i + 1] : dnn[v];
+            tbar.f[v][off] = x;
+        }
+    }
+}
+
+bool adjoint_chunk_supported(int len, int K, int elem_bytes, int &NL, int &P)
+{
+    if (K != 4 && K != 8) return false;
+    P = (len + K - 1) / K;
+    if (P < 1 || P > 256) return false;
+    NL = 256 / P;
+    if (NL < 1) return false;
+    return (size_t)2 * NL * P * 8 * elem_bytes <= 48 * 1024;
+}
+
+template <typename R>
+cudaError_t launch_adjoint_chunk(int dir, int K, const DomainView<R> &d, const int *lo, const int *hi, CLayer<R> ti,
+                                 CLayer<R> xs, Layer<R> sbar, Layer<R> dbar, Layer<R> tbar, Layer<R> nvbar, R *ga, R *gb,
+                                 const SweepConst<R> &k, int merges, cudaStream_t s)
+{
+    const LineGeom g = line_geom(dir, d.nx, d.ny, d.nz);
+    int NL = 0, P = 0;
+    if (!adjoint_chunk_supported(g.len, K, (int)sizeof(R), NL, P)) return cudaErrorInvalidConfiguration;
+    const int threads = NL * P;
+    const int blocks = (g.nlines + NL - 1) / NL;
+    const size_t smem = (size_t)2 * NL * P * 8 * sizeof(R);
+#define AC(DD, KK)                                                                                                 \
+    if (dir == DD && K == KK) {                                                                                    \
+        adjoint_chunk_kernel<R, DD, KK><<<blocks, threads, smem, s>>>(d, g, NL, P, lo, hi, ti, xs, sbar, dbar,   \
+                                                                     tbar, nvbar, ga, gb, k, merges);             \
+        return cudaGetLastError();                                                                                 \
+    }
+    AC(0, 4) AC(0, 8) AC(1, 4) AC(1, 8) AC(2, 4) AC(2, 8)
+#undef AC
+    return cudaErrorInvalidConfiguration;
+}
+
+template cudaError_t launch_adjoint_chunk<float>(int, int, const DomainView<float> &, const int *, const int *,
+                                                 CLayer<float>, CLayer<float>, Layer<float>, Layer<float>, Layer<float>,
+                                                 Layer<float>, float *, float *, const SweepConst<float> &, int,
+                                                 cudaStream_t);
+template cudaError_t launch_adjoint_chunk<double>(int, int, const DomainView<double> &, const int *, const int *,
+                                                  CLayer<double>, CLayer<double>, Layer<double>, Layer<double>,
+                                                  Layer<double>, Layer<double>, double *, double *,
+                                                  const SweepConst<double> &, int, cudaStream_t);
+
+} // namespace adi

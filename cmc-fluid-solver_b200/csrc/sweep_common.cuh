@@ -137,6 +137,67 @@ __device__ __forceinline__ void eliminate(const int (&kind)[K], const R (&rr)[K]
     }
 }
 
+// eliminate() for explicitly given rows: A, B, C per matrix m (sub-diagonal,
+// diagonal, super-diagonal of each of the chunk's K rows), right-hand sides dv
+// (velocity columns 0-2 use m = 0, column 3 uses m = 1).  Used by the adjoint,
+// whose transposed rows are not of the BuildMatrix / ApplyBC form.
+template <typename R, int K>
+__device__ __forceinline__ void eliminate_abc(const R (&A)[2][K], const R (&B)[2][K], const R (&C)[2][K],
+                                              R (&dv)[4][K], R (&ea)[2][K], R (&ec)[2][K], Reduced<R> &red)
+{
+    static_assert(K >= 3, "chunks of at least three rows");
+#pragma unroll
+    for (int m = 0; m < 2; m++) {
+        {
+            const R r = rcp<R>(B[m][1]);
+            ea[m][1] = A[m][1] * r;
+            ec[m][1] = C[m][1] * r;
+            if (m == 0) { dv[0][1] *= r; dv[1][1] *= r; dv[2][1] *= r; }
+            else dv[3][1] *= r;
+        }
+#pragma unroll
+        for (int i = 2; i <= K - 2; i++) {
+            const R r = rcp<R>(B[m][i] - A[m][i] * ec[m][i - 1]);
+            if (m == 0) {
+#pragma unroll
+                for (int v = 0; v < 3; v++) dv[v][i] = (dv[v][i] - A[m][i] * dv[v][i - 1]) * r;
+            } else {
+                dv[3][i] = (dv[3][i] - A[m][i] * dv[3][i - 1]) * r;
+            }
+            ea[m][i] = -A[m][i] * ea[m][i - 1] * r;
+            ec[m][i] = C[m][i] * r;
+        }
+#pragma unroll
+        for (int i = K - 3; i >= 1; i--) {
+            const R ci = ec[m][i];
+            ea[m][i] -= ci * ea[m][i + 1];
+            if (m == 0) {
+#pragma unroll
+                for (int v = 0; v < 3; v++) dv[v][i] -= ci * dv[v][i + 1];
+            } else {
+                dv[3][i] -= ci * dv[3][i + 1];
+            }
+            ec[m][i] = -ci * ec[m][i + 1];
+        }
+        const R rf = rcp<R>(B[m][0] - C[m][0] * ea[m][1]);
+        red.Af[m] = A[m][0] * rf;
+        red.Cf[m] = -C[m][0] * ec[m][1] * rf;
+        const R rl = rcp<R>(B[m][K - 1] - A[m][K - 1] * ec[m][K - 2]);
+        red.Al[m] = -A[m][K - 1] * ea[m][K - 2] * rl;
+        red.Cl[m] = C[m][K - 1] * rl;
+        if (m == 0) {
+#pragma unroll
+            for (int v = 0; v < 3; v++) {
+                red.Df[v] = (dv[v][0] - C[m][0] * dv[v][1]) * rf;
+                red.Dl[v] = (dv[v][K - 1] - A[m][K - 1] * dv[v][K - 2]) * rl;
+            }
+        } else {
+            red.Df[3] = (dv[3][0] - C[m][0] * dv[3][1]) * rf;
+            red.Dl[3] = (dv[3][K - 1] - A[m][K - 1] * dv[3][K - 2]) * rl;
+        }
+    }
+}
+
 // Cyclic-reduction step on the chunk-first row, given the previous chunk's last
 // row (pv: Al[0] Cl[0] Al[1] Cl[1] Dl[0..3], zeros for the first chunk).  Returns
 // the row of x(first) coupled to x(first) of the neighbouring chunks, normalised.
