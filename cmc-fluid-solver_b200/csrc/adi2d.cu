@@ -282,6 +282,125 @@ __global__ void sweep2_kernel(int nx, int ny, const Seg *__restrict__ segs, int 
     }
 }
 
+// Row coefficients of one segment row p (BC rows at the ends, BuildMatrix rows
+// inside), the reference's operand order.  Shared by both 2D sweep kernels.
+template <typename R>
+__device__ __forceinline__ void row2(const Seg &g, int p, int n, long long id, int ny, const uint8_t *__restrict__ bct,
+                                     const L2<R> &data, const L2<R> &cur, const L2<R> &tl, const Consts<R> &k, R &au,
+                                     R &bu, R &cu, R &at, R &bt, R &ct, R &d0, R &d1, R &d2)
+{
+    const R *TU = tl.f[0], *TV = tl.f[1], *TT = tl.f[2];
+    const R two = R(2);
+    if (p == 0 || p == n - 1) {   // ApplyBC0 / ApplyBC1
+        const bool fr = bct[id] == BC_FREE;
+        if (p == 0) {
+            au = at = R(0);
+            bu = bt = R(1);
+            cu = ct = fr ? R(-1) : R(0);
+        } else {
+            au = at = fr ? R(1) : R(0);
+            bu = bt = fr ? R(-1) : R(1);
+            cu = ct = R(0);   // c[n-1] = 0 (Algorithms.h:23)
+        }
+        d0 = fr ? R(0) : data.f[0][id];
+        d1 = fr ? R(0) : data.f[1][id];
+        d2 = fr ? R(0) : data.f[2][id];
+    } else if (g.dir == 0) {
+        const R vu = k.v_vis / (k.dx * k.dx), vt = k.t_vis / (k.dx * k.dx);
+        const R w = TU[id];
+        au = -w / (two * k.dx) - vu;
+        bu = R(1) / k.dt + two * vu;
+        cu = w / (two * k.dx) - vu;
+        at = -w / (two * k.dx) - vt;
+        bt = R(1) / k.dt + two * vt;
+        ct = w / (two * k.dx) - vt;
+        const R Tx = (TT[id + ny] - TT[id - ny]) / (two * k.dx);
+        d0 = cur.f[0][id] / k.dt - k.v_T * Tx;
+        d1 = cur.f[1][id] / k.dt;
+        const R ux = (TU[id + ny] - TU[id - ny]) / (two * k.dx);
+        const R vx = (TV[id + ny] - TV[id - ny]) / (two * k.dx);
+        const R uy = (TU[id + 1] - TU[id - 1]) / (two * k.dy);
+        d2 = cur.f[2][id] / k.dt + k.t_phi * (two * ux * ux + vx * vx + uy * vx);
+    } else {
+        const R vu = k.v_vis / (k.dy * k.dy), vt = k.t_vis / (k.dy * k.dy);
+        const R w = TV[id];
+        au = -w / (two * k.dy) - vu;
+        bu = R(1) / k.dt + two * vu;
+        cu = w / (two * k.dy) - vu;
+        at = -w / (two * k.dy) - vt;
+        bt = R(1) / k.dt + two * vt;
+        ct = w / (two * k.dy) - vt;
+        const R Ty = (TT[id + 1] - TT[id - 1]) / (two * k.dy);
+        d0 = cur.f[0][id] / k.dt;
+        d1 = cur.f[1][id] / k.dt - k.v_T * Ty;
+        const R vx = (TV[id + ny] - TV[id - ny]) / (two * k.dx);
+        const R uy = (TU[id + 1] - TU[id - 1]) / (two * k.dy);
+        const R vy = (TV[id + 1] - TV[id - 1]) / (two * k.dy);
+        d2 = cur.f[2][id] / k.dt + k.t_phi * (uy * uy + two * vy * vy + vx * uy);
+    }
+}
+
+// One CTA per segment: all threads build the rows into shared memory, lanes 0-2
+// run the Thomas recurrences of U, V and T side by side (the same instructions on
+// their own arrays; U and V each recompute the shared c'), all threads write the
+// solution back.  Bit-identical to sweep2_kernel; latency per row is a shared-
+// memory round trip instead of a global one.
+template <typename R>
+__global__ void sweep2_smem_kernel(int nx, int ny, const Seg *__restrict__ segs, const uint8_t *__restrict__ bct,
+                                   L2<R> data, L2<R> cur, L2<R> tl, L2<R> nl, Consts<R> k)
+{
+    extern __shared__ __align__(16) unsigned char sm2[];
+    const Seg g = segs[blockIdx.x];
+    const int n = g.size;
+    const long long st = g.dir == 0 ? ny : 1;
+    const long long id0 = (long long)g.posx * ny + g.posy;
+    // arrays of n: a, b, c for U/V and T (6), d for U, V, T (3), c' for U, V, T (3)
+    R *A = reinterpret_cast<R *>(sm2);
+    R *a_uv = A, *b_uv = A + n, *c_uv = A + 2 * n, *a_t = A + 3 * n, *b_t = A + 4 * n, *c_t = A + 5 * n;
+    R *dd = A + 6 * n;    // [3][n]
+    R *cpr = A + 9 * n;   // [3][n]
+    for (int p = threadIdx.x; p < n; p += blockDim.x) {
+        R au, bu, cu, at, bt, ct, d0, d1, d2;
+        row2<R>(g, p, n, id0 + (long long)p * st, ny, bct, data, cur, tl, k, au, bu, cu, at, bt, ct, d0, d1, d2);
+        a_uv[p] = au; b_uv[p] = bu; c_uv[p] = cu;
+        a_t[p] = at; b_t[p] = bt; c_t[p] = ct;
+        dd[p] = d0; dd[n + p] = d1; dd[2 * n + p] = d2;
+    }
+    __syncthreads();
+    const int v = threadIdx.x;
+    if (v < 3) {
+        const R *a = v < 2 ? a_uv : a_t, *b = v < 2 ? b_uv : b_t, *c = v < 2 ? c_uv : c_t;
+        R *d = dd + v * n, *cp = cpr + v * n;
+        // Thomas (Algorithms.h:21-39) in the reference's operand order
+        R cprev = c[0] / b[0];
+        R dprev = d[0] / b[0];
+        cp[0] = cprev;
+        d[0] = dprev;
+        for (int p = 1; p < n; p++) {
+            const R ap = a[p], bp = b[p];
+            const R cc = c[p] / (bp - ap * cprev);
+            const R dv = (d[p] - dprev * ap) / (bp - ap * cprev);
+            cp[p] = cc;
+            d[p] = dv;
+            cprev = cc;
+            dprev = dv;
+        }
+        R x = dprev;   // x[n-1] = d'[n-1]
+        for (int p = n - 2; p >= 0; p--) {
+            x = d[p] - cp[p] * x;
+            d[p] = x;
+        }
+    }
+    __syncthreads();
+    for (int p = threadIdx.x; p < n; p += blockDim.x) {
+        const long long id = id0 + (long long)p * st;
+        nl.f[0][id] = dd[p];
+        nl.f[1][id] = dd[n + p];
+        nl.f[2][id] = dd[2 * n + p];
+    }
+    (void)nx;
+}
+
 } // namespace d2
 } // namespace adi
 
@@ -398,8 +517,20 @@ adi_status solve_dir(adi2d_handle *h, double dt, int num_local, const Seg *segs,
     if (s != ADI_OK) return s;
     L2<R> data;
     for (int v = 0; v < 3; v++) data.f[v] = (R *)h->d_data[v];
+    // longest possible segment of this list: the extent along its axis
+    const int len = (nseg > 0 && segs == h->d_segy) ? h->nx : h->ny;
+    const size_t smem = (size_t)12 * len * sizeof(R);
     for (int it = 0; it < num_local; it++) {
-        if (nseg > 0) {
+        if (nseg > 0 && smem <= 200 * 1024) {
+            static size_t smem_set = 0;
+            if (smem > 48 * 1024 && smem > smem_set) {
+                CK2(cudaFuncSetAttribute(sweep2_smem_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                smem_set = smem;
+            }
+            sweep2_smem_kernel<R><<<nseg, 128, smem, h->stream>>>(h->nx, h->ny, segs, h->d_bct, data, lay<R>(h, cur),
+                                                                  lay<R>(h, TLOC), lay<R>(h, NLOC), consts<R>(h, dt));
+            CK2(cudaGetLastError());
+        } else if (nseg > 0) {
             sweep2_kernel<R><<<(nseg + 127) / 128, 128, 0, h->stream>>>(h->nx, h->ny, segs, nseg, h->d_bct, data,
                                                                         lay<R>(h, cur), lay<R>(h, TLOC),
                                                                         lay<R>(h, NLOC), (R *)h->d_scratch,
