@@ -70,7 +70,7 @@ __device__ __forceinline__ int aslot(int li, int c, int q, int NL, int P)
 } // namespace
 
 template <typename R, int DIR, int K>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 2)
     adjoint_chunk_kernel(DomainView<R> d, LineGeom g, int NL, int P, const int *__restrict__ line_lo,
                          const int *__restrict__ line_hi, CLayer<R> ti, CLayer<R> xs, Layer<R> sbar, Layer<R> dbar,
                          Layer<R> tbar, Layer<R> nvbar, R *__restrict__ ga, R *__restrict__ gb, SweepConst<R> kc,
@@ -114,15 +114,12 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int q = 0; q < K + 2; q++) kd[q] = qkind(code_is_in(cc[q]), code_is_in(cc[q + 1]), code_is_in(cc[q + 2]));
     R wv[K + 2];     // advecting temp at window rows (IN rows only)
-    R xw[4][K + 2];  // the sweep's output x at window rows (segment rows)
 #pragma unroll
     for (int q = 0; q < K + 2; q++) {
         const long long off = base + (long long)(p0 - 1 + q) * sl;
         wv[q] = kd[q] == Q_IN ? ti.f[DIR][off] : R(0);
-#pragma unroll
-        for (int v = 0; v < 4; v++) xw[v][q] = kd[q] != Q_NONE ? xs.f[v][off] : R(0);
     }
-    R A[2][K], B[2][K], C[2][K], xb[4][K], tob[4][K];
+    R A[2][K], B[2][K], C[2][K], xb[4][K];
 #pragma unroll
     for (int i = 0; i < K; i++) {
         const int q = i + 1;
@@ -141,9 +138,8 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
         for (int v = 0; v < 4; v++) {
             const R db = kd[q] != Q_NONE ? dbar.f[v][off] : R(0);
-            const R to = kd[q] != Q_NONE ? tbar.f[v][off] : R(0);
-            tob[v][i] = to;
-            xb[v][i] = db + (kd[q] == Q_IN ? mx * to : R(0));
+            const R to = kd[q] == Q_IN ? tbar.f[v][off] : R(0);
+            xb[v][i] = db + mx * to;
         }
     }
 
@@ -244,7 +240,7 @@ __global__ void __launch_bounds__(256)
         for (int v = 0; v < 4; v++) sbar.f[v][off] += kc.three_dt * lam[v];
         R w = R(0);
 #pragma unroll
-        for (int v = 0; v < 4; v++) w += lam[v] * (xw[v][q - 1] - xw[v][q + 1]);
+        for (int v = 0; v < 4; v++) w += lam[v] * (xs.f[v][off - sl] - xs.f[v][off + sl]);
         wb[i] = w * kc.inv_two_h;
         const R pt = kc.v_T * lam[DIR] * kc.inv_two_h;
         up[3][i] = -pt;
@@ -299,7 +295,7 @@ __global__ void __launch_bounds__(256)
         const bool in = kd[q] == Q_IN;
 #pragma unroll
         for (int v = 0; v < 4; v++) {
-            R x = (in ? mt : R(1)) * tob[v][i];
+            R x = (in ? mt : R(1)) * tbar.f[v][off];   // not yet rewritten: this thread owns the row
             if (v == DIR) x += wb[i];
             x += i > 0 ? up[v][i - 1] : upp[v];
             x += i < K - 1 ? dn[v][i + 1] : dnn[v];
