@@ -62,6 +62,15 @@ def _spheres64():
     return G.spheres_channel(n=64, n_spheres=10, rmin=3.0, rmax=7.0, seed=0)
 
 
+def _batched8():
+    return G.batch_of_domains(n_domains=8, seed=2, size_lo=64, size_hi=96, spheres=(10, 30), rmin=4.0, rmax=10.0,
+                              re=(50.0, 400.0))
+
+
+def _spheres64_adj():
+    return G.spheres_channel(n=64, n_spheres=10, rmin=3.0, rmax=7.0, seed=0)
+
+
 def _batched64():
     return G.batch_of_domains(n_domains=64, seed=2, size_lo=64, size_hi=160, spheres=(10, 60), rmin=4.0, rmax=12.0,
                               re=(50.0, 400.0))
@@ -90,6 +99,12 @@ CONFIGS = {
                       desc="plain 2D ADI: 256x128 FP64 channel, dx=dy=1/128, disc radius 12 at (64,64), parabolic "
                            "inflow (max 1.0), no-slip walls, BC_FREE outflow, Re=100, dt=1e-3, num_global=4 "
                            "(the reference's loop continues while its divergence error exceeds 0.1), num_local=1"),
+    "batched8": dict(make=_batched8, batch=True, Pr=0.72, lam=1.4, dt=5e-4, ng=4, nl=2,
+                     desc="small batch for profiling: 8 domains, axes U{64..96} (seed 2), 10-30 spheres, "
+                          "Re U[50,400], dt=5e-4, num_global=4, num_local=2"),
+    "adjoint64": dict(make=_spheres64_adj, adjoint=True, Re=200.0, Pr=0.72, lam=1.4, dt=5e-4, ng=4, nl=2,
+                      n_steps=8, ckpt=4, box=((40, 16, 16), (56, 48, 48)), near_box=((2, 16, 16), (18, 48, 48)),
+                      desc="small adjoint for profiling: 64^3 FP32, 10 spheres, 8 steps checkpointed every 4"),
     "spheres64": dict(make=_spheres64, Re=200.0, Pr=0.72, lam=1.4, dt=5e-4, ng=4, nl=2,
                       desc="small case for profiling: 64^3 FP32, 10 spheres, Re=200, dt=5e-4, "
                            "num_global=4, num_local=2"),
