@@ -282,7 +282,8 @@ int line_len(const adi_handle *h, int dir) { return dir == 0 ? h->nx : (dir == 1
 bool shape_ok(const adi_handle *h, int dir, const FastShape &s)
 {
     if (s.mode == 1) return dir == 2 && zwarp_supported(h->nz, s.K, (int)esize(h));
-    if (s.mode == 2) return dir < 2 && xytma_supported(dir, h->nx, h->ny, h->nz, s.K, (int)esize(h));
+    if (s.mode == 2 || s.mode == 4)
+        return dir < 2 && xytma_supported(dir, h->nx, h->ny, h->nz, s.K, s.mode == 2 ? 16 : 8, (int)esize(h));
     if (s.mode == 3) return dir < 2 && xypair_supported(dir, h->nx, h->ny, h->nz, s.K, (int)esize(h));
     return s.mode == 0 && fast_shape_supported(dir, s, line_len(h, dir), (int)esize(h));
 }
@@ -296,9 +297,9 @@ cudaError_t launch_fast(adi_handle *h, int dir, CLayer<R> cur, CLayer<R> tin, La
     if (s.mode == 1)
         return launch_sweep_zwarp<R>(d, h->d_line_lo[2], h->d_line_hi[2], cur, tin, next, tout, k, merges, s.K,
                                      h->stream);
-    if (s.mode == 2)
-        return launch_sweep_xytma<R>(dir, d, h->d_line_lo[dir], cur, tin, next, tout, k, merges, s.K, h->d_err,
-                                     h->stream);
+    if (s.mode == 2 || s.mode == 4)
+        return launch_sweep_xytma<R>(dir, d, h->d_line_lo[dir], cur, tin, next, tout, k, merges, s.K,
+                                     s.mode == 2 ? 16 : 8, h->d_err, h->stream);
     if (s.mode == 3) {
         if constexpr (std::is_same<R, float>::value)
             return launch_sweep_xypair(dir, d, h->d_line_lo[dir], cur, tin, next, tout, k, merges, s.K, h->d_err,
@@ -367,9 +368,11 @@ std::vector<FastShape> shape_candidates(const adi_handle *h, int dir)
             FastShape s{K, 32, len / K, 3};
             if (shape_ok(h, dir, s)) out.push_back(s);
         }
-        for (int K : {8, 16}) {
+        for (int K : {4, 8, 16}) {
             FastShape s{K, 16, len / K, 2};
             if (shape_ok(h, dir, s)) out.push_back(s);
+            FastShape s8{K, 8, len / K, 4};
+            if (shape_ok(h, dir, s8)) out.push_back(s8);
         }
     }
     for (int K : {4, 8, 12, 16})
@@ -400,7 +403,10 @@ adi_status autotune(adi_handle *h, int reps)
                 return launch_fast<R>(h, dir, clayer<R>(h, h->cur), clayer<R>(h, h->ta), layer<R>(h, h->half),
                                       layer<R>(h, h->tb), k, 1, s);
             };
-            CK(go());
+            // a tensor map the driver will not encode rules the candidate out before any launch
+            const cudaError_t e0 = go();
+            if (e0 == cudaErrorInvalidValue && (s.mode == 2 || s.mode == 3 || s.mode == 4)) continue;
+            CK(e0);
             float tmin = 1e30f;
             for (int r = 0; r < reps; r++) {
                 CK(cudaEventRecord(a, h->stream));
@@ -1047,7 +1053,7 @@ adi_status adi_get_fast_shape(adi_handle *h, int dir, int *K, int *NL, int *P)
     if (!h || dir < 0 || dir > 2) return ADI_ERR_BAD_ARG;
     const FastShape s = h->shape[dir];
     if (K) *K = s.K;
-    if (NL) *NL = s.mode == 1 ? 0 : (s.mode == 2 ? -16 : (s.mode == 3 ? -32 : s.NL));
+    if (NL) *NL = s.mode == 1 ? 0 : (s.mode == 2 ? -16 : (s.mode == 3 ? -32 : (s.mode == 4 ? -8 : s.NL)));
     if (P) *P = (line_len(h, dir) + s.K - 1) / s.K;
     return ADI_OK;
 }
@@ -1056,8 +1062,10 @@ adi_status adi_set_fast_shape(adi_handle *h, int dir, int K, int NL)
 {
     if (!h || dir < 0 || dir > 2 || K <= 0) return ADI_ERR_BAD_ARG;
     const int len = line_len(h, dir);
-    if (NL < 0 && NL != -16 && NL != -32) return fail(h, ADI_ERR_BAD_ARG, "unsupported fast-sweep shape");
-    FastShape s{K, NL < 0 ? -NL : NL, (len + K - 1) / K, NL == 0 ? 1 : (NL == -16 ? 2 : (NL == -32 ? 3 : 0))};
+    if (NL < 0 && NL != -8 && NL != -16 && NL != -32)
+        return fail(h, ADI_ERR_BAD_ARG, "unsupported fast-sweep shape");
+    const int mode = NL == 0 ? 1 : (NL == -16 ? 2 : (NL == -32 ? 3 : (NL == -8 ? 4 : 0)));
+    FastShape s{K, NL < 0 ? -NL : NL, (len + K - 1) / K, mode};
     if (!shape_ok(h, dir, s)) return fail(h, ADI_ERR_BAD_ARG, "unsupported fast-sweep shape");
     h->shape[dir] = s;
     h->tuned = true;

@@ -89,8 +89,9 @@ struct SweepConst {
 struct FastShape {
     int K, NL, P;
     int mode;   // 0: generic chunked kernel; 1: warp-resident Z lines (sweep_zwarp.cu);
-                // 2: TMA-fed X/Y tiles (sweep_xytma.cu); 3: persistent double-buffered
-                // X/Y tiles, two lines per thread (sweep_xypair.cu, FP32)
+                // 2: TMA-fed X/Y tiles of NL = 16 lines (sweep_xytma.cu); 3: persistent
+                // double-buffered X/Y tiles, two lines per thread (sweep_xypair.cu, FP32);
+                // 4: TMA-fed X/Y tiles of NL = 8 lines (sweep_xytma.cu)
 };
 
 // Device-side description of one domain, passed by value to kernels.
@@ -170,9 +171,9 @@ cudaError_t launch_sweep_zwarp(const DomainView<R> &d, const int *line_lo, const
 bool zwarp_supported(int nz, int K, int elem_bytes);
 template <typename R>
 cudaError_t launch_sweep_xytma(int dir, const DomainView<R> &d, const int *line_lo, CLayer<R> cur, CLayer<R> tin,
-                               Layer<R> next, Layer<R> tout, const SweepConst<R> &k, int merges, int K,
+                               Layer<R> next, Layer<R> tout, const SweepConst<R> &k, int merges, int K, int nlt,
                                int *err_flag, cudaStream_t s);
-bool xytma_supported(int dir, int nx, int ny, int nz, int K, int elem_bytes);
+bool xytma_supported(int dir, int nx, int ny, int nz, int K, int nlt, int elem_bytes);
 cudaError_t launch_sweep_xypair(int dir, const DomainView<float> &d, const int *line_lo, CLayer<float> cur,
                                 CLayer<float> tin, Layer<float> next, Layer<float> tout, const SweepConst<float> &k,
                                 int merges, int K, int *err_flag, cudaStream_t s);

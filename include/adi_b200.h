@@ -200,9 +200,11 @@ adi_status adi_div_error(adi_handle *h, double *out);
 /* Launch shape of the fast sweep for one direction: each thread owns K
  * consecutive rows of a line, a CTA holds NL lines, P = ceil(len/K) chunks per
  * line.  NL = 0 selects the warp-resident Z kernel (Z only; dimz = P*K with P in
- * {4, 8, 16, 32}, K in {4, 8}); NL = -16 selects the TMA-fed X/Y kernel (16 lines
- * per CTA; dimz a multiple of 16, line length <= 256, even and a multiple of K,
- * K in {8, 16}); NL = -32 selects the persistent, double-buffered X/Y kernel with
+ * {4, 8, 16, 32}, K in {4, 8}); NL = -16 and NL = -8 select the TMA-fed X/Y
+ * kernel with 16 or 8 lines per CTA (dimz a multiple of 16, K in {4, 8, 16},
+ * line length = P K with P in {4, 8, 16} or P = 32 at K = 4, at most 512 threads,
+ * tiles within the shared memory of the CTAs per SM the shape is compiled for);
+ * NL = -32 selects the persistent, double-buffered X/Y kernel with
  * two lines per thread (FP32 only; dimz a multiple of 16, K in {4, 8}, 2 <= P <= 32,
  * both tile buffers within 227 KB of shared memory, e.g. line length <= 136 at
  * K = 4).  adi_build_segments times the candidate shapes on

@@ -95,7 +95,7 @@ def test_autotuner_picks_supported_shapes(adi_lib):
         if NL == 0:
             assert dr == 2 and P * K == d.shape[2]          # warp-resident Z lines
         elif NL < 0:
-            assert dr < 2 and NL in (-16, -32) and P * K == d.shape[dr]   # TMA-fed X/Y tiles
+            assert dr < 2 and NL in (-8, -16, -32) and P * K == d.shape[dr]   # TMA-fed X/Y tiles
         else:
             assert 32 <= NL * P <= 256
     with pytest.raises(_abi.AdiError):
@@ -144,16 +144,18 @@ def test_zwarp_kernel(adi_lib, zK, precision):
     assert max(errs_n) < (1e-11 if precision == "fp64" else 2e-6), errs_n
 
 
-@pytest.mark.parametrize("xK", [8, 16])
+@pytest.mark.parametrize("xK,nl", [(8, -16), (16, -16), (8, -8), (4, -8), (4, -16)])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_xytma_kernel(adi_lib, xK, precision):
-    """TMA-fed X/Y kernel (NL = -16): dimz a multiple of 16, lines a multiple of K."""
+def test_xytma_kernel(adi_lib, xK, nl, precision):
+    """TMA-fed X/Y kernel with 16 (NL = -16) or 8 (NL = -8) lines per CTA and
+    chunk-major tiles: dimz a multiple of 16, lines of 4, 8 or 16 chunks of K rows
+    (X: 64 rows, Y: 32 rows)."""
     from adi_b200 import _abi
-    d = G.random_domain(48, 40, 32, seed=81, shell=True, n_obstacles=8, rmax=4.5)
+    d = G.random_domain(64, 32, 32, seed=81, shell=True, n_obstacles=8, rmax=4.5)
     params = (130.0, 0.72, 1.4)
     prec = _abi.ADI_FP64 if precision == "fp64" else _abi.ADI_FP32
-    s = solver(adi_lib, d, params, precision=prec, shapes=[(xK, -16), (8, -16), (4, 0)])
-    assert s.fast_shapes()[0][1] == -16 and s.fast_shapes()[1][1] == -16
+    s = solver(adi_lib, d, params, precision=prec, shapes=[(xK, nl), (min(xK, 8), nl), (4, 0)])
+    assert s.fast_shapes()[0][1] == nl and s.fast_shapes()[1][1] == nl
     orc = O.OracleSolver(d, precision=8, params=fluid_params_tuple(("normalized", params)))
     m = non_out(d)
     for _ in range(3):
@@ -201,6 +203,23 @@ def test_xypair_kernel(adi_lib, xK, slab):
     assert max(errs) < 2e-6, errs
     errs_n = rel_errors(s.fields(1), orc.fields(1), m)
     assert max(errs_n) < 2e-6, errs_n
+
+
+@pytest.mark.parametrize("nl", [-16, -8])
+def test_xytma_empty_tiles(adi_lib, nl):
+    """TMA-fed X/Y kernel on a domain whose first tiles of every X and Y plane hold
+    no segment: those CTAs leave before any load; the rest match the FP64 oracle."""
+    d = _slab_domain(128, 64, 48, seed=88)
+    params = (150.0, 0.72, 1.4)
+    s = solver(adi_lib, d, params, shapes=[(8, nl), (8, nl), (8, 8)])
+    assert s.fast_shapes()[0][1] == nl and s.fast_shapes()[1][1] == nl
+    orc = O.OracleSolver(d, precision=8, params=fluid_params_tuple(("normalized", params)))
+    m = non_out(d)
+    for _ in range(2):
+        assert s.step(6e-4, 4, 2, True) == 0
+        assert orc.step(6e-4, 4, 2, True) == 0
+    errs = rel_errors(s.fields(0), orc.fields(0), m)
+    assert max(errs) < 2e-6, errs
 
 
 def test_xypair_rejects_fp64_and_bad_shapes(adi_lib):
