@@ -298,6 +298,11 @@ class AdiSolver2D:
             raw = self.lib.adi2d_last_error_string(self.h) if self.h else b""
             raise _abi.AdiError(status, raw.decode() if raw else "")
 
+    def set_segment_mode(self, mode: int):
+        """0: the reference's row-spanning segments (default); 1: masked segments
+        (runs of IN nodes, the 3D solver's segmentation)."""
+        self._check(self.lib.adi2d_set_segments(self.h, mode))
+
     def UpdateBoundaries(self):
         self._check(self.lib.adi2d_update_boundaries(self.h))
 

@@ -36,6 +36,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <algorithm>
 #include <vector>
 
 struct adi2d_handle;
@@ -428,6 +429,8 @@ struct adi2d_handle {
     std::string msg;
     cudaGraphExec_t graph = nullptr;
     uint64_t graph_key[2] = {0, 0};
+    int seg_mode = 0;             // 0: row-spanning (the reference), 1: masked segments
+    size_t scratch_bytes = 0;
 };
 
 namespace {
@@ -658,9 +661,39 @@ adi_status time_step(adi2d_handle *h, double dt, int num_global, int num_local, 
     return ADI_OK;
 }
 
-// AdiSolver2D::CreateSegments (AdiSolver2D.cpp:228-277).
+// Masked segments: the 3D solver's segmentation (Grid3D::GenerateListSegments,
+// Grid3D.cpp:47-127) on the 2D grid's columns and rows -- every maximal run of IN
+// nodes, with the non-IN node on each side as its boundary rows; a run reaching the
+// last node of a line has no closing node and is dropped, as there.
+void build_segments_masked(const adi2d_handle *h, std::vector<Seg> &cols, std::vector<Seg> &rows)
+{
+    const int nx = h->nx, ny = h->ny;
+    for (int dir = 1; dir >= 0; dir--) {
+        const int nlines = dir == 1 ? nx : ny, len = dir == 1 ? ny : nx;
+        for (int l = 0; l < nlines; l++) {
+            int open = -1;
+            for (int p = 0; p + 1 < len; p++) {
+                const size_t nxt = dir == 1 ? (size_t)l * ny + (p + 1) : (size_t)(p + 1) * ny + l;
+                const bool in_next = h->h_type[nxt] == NODE_IN;
+                if (open < 0 && in_next) {
+                    open = p;
+                } else if (open >= 0 && !in_next) {
+                    if (dir == 1) cols.push_back(Seg{l, open, p + 2 - open, 1});
+                    else rows.push_back(Seg{open, l, p + 2 - open, 0});
+                    open = -1;
+                }
+            }
+        }
+    }
+}
+
+// AdiSolver2D::CreateSegments (AdiSolver2D.cpp:228-277), or the masked segments.
 void build_segments(const adi2d_handle *h, std::vector<Seg> &cols, std::vector<Seg> &rows)
 {
+    if (h->seg_mode == 1) {
+        build_segments_masked(h, cols, rows);
+        return;
+    }
     const int nx = h->nx, ny = h->ny;
     auto T = [&](int i, int j) { return h->h_type[(size_t)i * ny + j]; };
     for (int i = 0; i < nx; i++) {
@@ -735,6 +768,7 @@ adi_status adi2d_create(int nx, int ny, double dx, double dy, int precision, con
             if (e == cudaSuccess) e = cudaMemset(h->d_L[l][v], 0, fb);
         }
     if (e == cudaSuccess) e = cudaMalloc(&h->d_scratch, 5 * fb);
+    if (e == cudaSuccess) h->scratch_bytes = 5 * fb;
     if (e == cudaSuccess) e = cudaMalloc((void **)&h->d_psum, sizeof(double) * D2_BLOCKS);
     if (e == cudaSuccess) e = cudaMalloc((void **)&h->d_pcnt, sizeof(unsigned long long) * D2_BLOCKS);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking);
@@ -764,6 +798,40 @@ adi_status adi2d_set_stream(adi2d_handle *h, void *stream)
     return ADI_OK;
 }
 
+// Builds the segment lists of the handle's mode from its node types and uploads
+// them; the per-segment scratch of sweep2_kernel (5 values per row of every
+// segment, laid out by the list's longest line) grows to fit.  Drops the graph.
+static adi_status upload_segments(adi2d_handle *h)
+{
+    std::vector<Seg> cols, rows;
+    build_segments(h, cols, rows);
+    const size_t es = es2(h);
+    const size_t need = 5 * es * std::max((size_t)h->ny * cols.size(), (size_t)h->nx * rows.size());
+    if (need > h->scratch_bytes) {
+        cudaFree(h->d_scratch);
+        h->d_scratch = nullptr;
+        h->scratch_bytes = 0;
+        CK2(cudaMalloc(&h->d_scratch, need));
+        h->scratch_bytes = need;
+    }
+    cudaFree(h->d_segx);
+    cudaFree(h->d_segy);
+    h->d_segx = h->d_segy = nullptr;
+    h->nsegx = (int)cols.size();
+    h->nsegy = (int)rows.size();
+    if (!cols.empty()) {
+        CK2(cudaMalloc((void **)&h->d_segx, sizeof(Seg) * cols.size()));
+        CK2(cudaMemcpy(h->d_segx, cols.data(), sizeof(Seg) * cols.size(), cudaMemcpyHostToDevice));
+    }
+    if (!rows.empty()) {
+        CK2(cudaMalloc((void **)&h->d_segy, sizeof(Seg) * rows.size()));
+        CK2(cudaMemcpy(h->d_segy, rows.data(), sizeof(Seg) * rows.size(), cudaMemcpyHostToDevice));
+    }
+    if (h->graph) cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+    return ADI_OK;
+}
+
 adi_status adi2d_set_grid(adi2d_handle *h, const uint8_t *type, const uint8_t *bc_type, const double *vx,
                           const double *vy, const double *T, double startT)
 {
@@ -788,25 +856,22 @@ adi_status adi2d_set_grid(adi2d_handle *h, const uint8_t *type, const uint8_t *b
         // AdiSolver2D::Init: cur = node data everywhere (AdiSolver2D.cpp:35-47)
         CK2(cudaMemcpy(h->d_L[CUR][v], p, fb, cudaMemcpyHostToDevice));
     }
-    std::vector<Seg> cols, rows;
-    build_segments(h, cols, rows);
-    cudaFree(h->d_segx);
-    cudaFree(h->d_segy);
-    h->d_segx = h->d_segy = nullptr;
-    h->nsegx = (int)cols.size();
-    h->nsegy = (int)rows.size();
-    if (!cols.empty()) {
-        CK2(cudaMalloc((void **)&h->d_segx, sizeof(Seg) * cols.size()));
-        CK2(cudaMemcpy(h->d_segx, cols.data(), sizeof(Seg) * cols.size(), cudaMemcpyHostToDevice));
-    }
-    if (!rows.empty()) {
-        CK2(cudaMalloc((void **)&h->d_segy, sizeof(Seg) * rows.size()));
-        CK2(cudaMemcpy(h->d_segy, rows.data(), sizeof(Seg) * rows.size(), cudaMemcpyHostToDevice));
-    }
-    if (h->graph) cudaGraphExecDestroy(h->graph);
-    h->graph = nullptr;
+    adi_status st = upload_segments(h);
+    if (st != ADI_OK) return st;
     h->grid_set = true;
     return ADI_OK;
+}
+
+adi_status adi2d_set_segments(adi2d_handle *h, int mode)
+{
+    if (!h || (mode != 0 && mode != 1)) return ADI_ERR_BAD_ARG;
+    if (!h->grid_set) return f2(h, ADI_ERR_STATE, "adi2d_set_grid has not been called");
+    CK2(cudaStreamSynchronize(h->stream));
+    const int old = h->seg_mode;
+    h->seg_mode = mode;
+    const adi_status st = upload_segments(h);
+    if (st != ADI_OK) h->seg_mode = old;
+    return st;
 }
 
 adi_status adi2d_update_boundaries(adi2d_handle *h)

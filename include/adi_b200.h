@@ -304,6 +304,17 @@ adi_status adi2d_set_stream(adi2d_handle *h, void *cuda_stream);
 adi_status adi2d_set_grid(adi2d_handle *h, const uint8_t *node_type, const uint8_t *bc_type, const double *vx,
                           const double *vy, const double *T, double startT);
 
+/* Segmentation of the 2D sweeps.  mode 0 (the default): the reference's, one
+ * segment per row / column spanning every interior obstacle
+ * (AdiSolver2D::CreateSegments, AdiSolver2D.cpp:228-277).  mode 1: masked
+ * segments, the 3D solver's segmentation (Grid3D::GenerateListSegments,
+ * Grid3D.cpp:47-127) applied to 2D lines -- each maximal run of IN nodes with the
+ * non-IN node on each side as its boundary rows, so solid cells are never solved
+ * as fluid; everything else (rows, 1/dt, merges, the error loop) is unchanged.
+ * The reference has no mode 1.  Rebuilds the segment lists from the node types
+ * of adi2d_set_grid (ADI_ERR_STATE before it); the state is kept. */
+adi_status adi2d_set_segments(adi2d_handle *h, int mode);
+
 /* Solver2D::UpdateBoundaries (Solver2D.cpp:40-54). */
 adi_status adi2d_update_boundaries(adi2d_handle *h);
 

@@ -37,10 +37,9 @@ static double absr_f64(double x) { return fabs(x); }
 
 /* AdiSolver2D::CreateSegments (AdiSolver2D.cpp:228-277): listX holds one
  * Y-direction segment per column i, listY one X-direction segment per row j. */
-static int make_segments(const uint8_t *type, int nx, int ny, seg2_t **segx, seg2_t **segy)
+static void make_segments_row_spanning(const uint8_t *type, int nx, int ny, seg2_t *segx, seg2_t *segy, int *ncx,
+                                       int *ncy)
 {
-    *segx = calloc((size_t)nx, sizeof(seg2_t));
-    *segy = calloc((size_t)ny, sizeof(seg2_t));
     int cx = 0, cy = 0;
 #define T_(i, j) type[(size_t)(i) * ny + (j)]
     for (int i = 0; i < nx; i++) {
@@ -58,7 +57,7 @@ static int make_segments(const uint8_t *type, int nx, int ny, seg2_t **segx, seg
         g.size = j - g.posy + 1;
         g.endx = i;
         g.endy = j;
-        (*segx)[cx++] = g;
+        segx[cx++] = g;
     }
     for (int j = 0; j < ny; j++) {
         seg2_t g;
@@ -75,10 +74,53 @@ static int make_segments(const uint8_t *type, int nx, int ny, seg2_t **segx, seg
         g.size = i - g.posx + 1;
         g.endx = i;
         g.endy = j;
-        (*segy)[cy++] = g;
+        segy[cy++] = g;
     }
 #undef T_
-    return cx * 65536 + cy;
+    *ncx = cx;
+    *ncy = cy;
+}
+
+/* Masked segments, the 3D solver's segmentation (Grid3D::GenerateListSegments,
+ * Grid3D.cpp:47-127) applied to the 2D grid's columns and rows: every maximal run
+ * of IN nodes with the non-IN node on each side as its boundary rows, so solid
+ * cells inside the box are never solved as fluid.  A run that reaches the last
+ * node of a line has no closing node and is dropped, as there. */
+static void make_segments_masked(const uint8_t *type, int nx, int ny, seg2_t *segx, seg2_t *segy, int *ncx, int *ncy)
+{
+    int cx = 0, cy = 0;
+    for (int dir = 1; dir >= 0; dir--) {
+        const int nlines = dir == 1 ? nx : ny, len = dir == 1 ? ny : nx;
+        for (int l = 0; l < nlines; l++) {
+            int open = -1;
+            for (int p = 0; p + 1 < len; p++) {
+                const size_t nxt = dir == 1 ? (size_t)l * ny + (p + 1) : (size_t)(p + 1) * ny + l;
+                const int in_next = type[nxt] == NODE_IN_;
+                if (open < 0 && in_next) open = p;
+                else if (open >= 0 && !in_next) {
+                    seg2_t g;
+                    g.dir = dir;
+                    g.size = p + 1 - open + 1;
+                    if (dir == 1) { g.posx = g.endx = l; g.posy = open; g.endy = p + 1; segx[cx++] = g; }
+                    else { g.posy = g.endy = l; g.posx = open; g.endx = p + 1; segy[cy++] = g; }
+                    open = -1;
+                }
+            }
+        }
+    }
+    *ncx = cx;
+    *ncy = cy;
+}
+
+/* mode 0: the reference's row-spanning segments; mode 1: masked segments. */
+static void make_segments(const uint8_t *type, int nx, int ny, int mode, seg2_t **segx, seg2_t **segy, int *ncx,
+                          int *ncy)
+{
+    /* a line of n nodes holds at most n / 2 masked segments */
+    *segx = calloc((size_t)nx * (ny / 2 + 1), sizeof(seg2_t));
+    *segy = calloc((size_t)ny * (nx / 2 + 1), sizeof(seg2_t));
+    if (mode == 1) make_segments_masked(type, nx, ny, *segx, *segy, ncx, ncy);
+    else make_segments_row_spanning(type, nx, ny, *segx, *segy, ncx, ncy);
 }
 
 typedef struct {
@@ -101,8 +143,7 @@ typedef struct {
         l2_alloc##SUF(&s->temp, n); l2_alloc##SUF(&s->next_local, n);                     \
         /* AdiSolver2D::Init: cur = node data everywhere (AdiSolver2D.cpp:35-47) */        \
         for (size_t q = 0; q < n; q++) { s->cur.u[q] = s->du[q]; s->cur.v[q] = s->dv[q]; s->cur.t[q] = s->dt_[q]; } \
-        int c = make_segments(t, nx, ny, &s->segx, &s->segy);                             \
-        s->nsegx = c / 65536; s->nsegy = c % 65536;                                       \
+        make_segments(t, nx, ny, 0, &s->segx, &s->segy, &s->nsegx, &s->nsegy);            \
         h->s = s;                                                                         \
     } while (0)
 
@@ -165,6 +206,25 @@ double oracle2d_last_err(void *vh)
 {
     oracle2d_h *h = vh;
     return h->precision == 8 ? ((solver2_f64 *)h->s)->last_err : ((solver2_f32 *)h->s)->last_err;
+}
+
+/* Rebuilds the segment lists: mode 0 the reference's row-spanning segments
+ * (the default), mode 1 masked segments.  Returns the segment count, -1 on a bad
+ * mode. */
+int oracle2d_set_segments(void *vh, int mode)
+{
+    oracle2d_h *h = vh;
+    if (mode != 0 && mode != 1) return -1;
+    if (h->precision == 8) {
+        solver2_f64 *s = h->s;
+        free(s->segx); free(s->segy);
+        make_segments(s->type, s->nx, s->ny, mode, &s->segx, &s->segy, &s->nsegx, &s->nsegy);
+        return s->nsegx + s->nsegy;
+    }
+    solver2_f32 *s = h->s;
+    free(s->segx); free(s->segy);
+    make_segments(s->type, s->nx, s->ny, mode, &s->segx, &s->segy, &s->nsegx, &s->nsegy);
+    return s->nsegx + s->nsegy;
 }
 
 /* Segments as int32 [posx posy endx endy size dir] rows: listX then listY. */

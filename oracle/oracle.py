@@ -264,6 +264,7 @@ def _load_oracle2d():
         lib.oracle2d_last_err.restype = C.c_double
         lib.oracle2d_last_err.argtypes = [C.c_void_p]
         lib.oracle2d_segments.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+        lib.oracle2d_set_segments.argtypes = [C.c_void_p, C.c_int]
         lib.oracle2d_destroy.argtypes = [C.c_void_p]
         _orc2d = lib
     return _orc2d
@@ -301,6 +302,14 @@ class Oracle2D:
         f = [np.ascontiguousarray(a, np.float64) for a in (d.vx, d.vy, d.T)]
         self.h = self.lib.oracle2d_create(precision, d.nx, d.ny, d.dx, d.dy, d.startT, *arrs, *f)
         self.lib.oracle2d_set_params(self.h, *fluid_params2d(Re, Pr, lam, precision))
+
+    def set_segment_mode(self, mode: int) -> int:
+        """0: the reference's row-spanning segments; 1: masked segments.  Returns
+        the segment count."""
+        n = self.lib.oracle2d_set_segments(self.h, mode)
+        if n < 0:
+            raise ValueError(f"bad segment mode {mode}")
+        return n
 
     def step(self, dt, num_global, num_local) -> int:
         return self.lib.oracle2d_step(self.h, dt, num_global, num_local)
