@@ -780,6 +780,24 @@ def run_2d(args):
     torch.cuda.synchronize()
     m_ms = m0.elapsed_time(m1)
     gm.close()
+    # the configuration's nonlinear-iteration rule: up to 4 global iterations per
+    # step until the iterate changes by at most 1e-6 (tolerance mode)
+    gt = adi_b200.AdiSolver2D(d, Re=cfg["Re"], Pr=cfg["Pr"], lam=cfg["lam"], stream=stream.cuda_stream)
+    for i in range(args.warmup):
+        assert gt.step_tol(dt, ng, nl, 1e-6)[0] == 0
+    t_iters, t_res = [], []
+    t0e, t1e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0e.record(stream)
+    for i in range(steps):
+        rc, it, res = gt.step_tol(dt, ng, nl, 1e-6)
+        if rc != 0:
+            raise RuntimeError(f"adi2d_step_tol failed with status {rc}")
+        t_iters.append(it)
+        t_res.append(res)
+    t1e.record(stream)
+    torch.cuda.synchronize()
+    t_ms = t0e.elapsed_time(t1e)
+    gt.close()
     # end to end with host buffers
     pinned = [torch.empty(d.shape, dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)]
     for a, b in zip(pinned, g.fields(0)):
@@ -815,6 +833,12 @@ def run_2d(args):
                      "frac": achieved / peak if peak else None, "traffic": None, "kernel": "whole 2D step",
                      "peak_source": peak_kind,
                      "note": "32K cells: latency- and launch-bound, not bandwidth-bound"},
+        "tolerance_mode": {"value": world * d.cells * steps / (t_ms / 1e3), "unit": METRIC,
+                           "ms_per_step": t_ms / steps, "tol": 1e-6, "max_global": ng,
+                           "global_iterations_per_step": float(np.mean(t_iters)),
+                           "last_residual_max": float(np.max(t_res)),
+                           "note": "adi2d_step_tol: global iterations until max|x_k - x_(k-1)| / max|x_k| <= tol; "
+                                   "synchronises after every iteration"},
         "masked_segments": {"value": world * d.cells * steps / (m_ms / 1e3), "unit": METRIC,
                             "ms_per_step": m_ms / steps, "global_iterations_per_step": float(np.mean(m_iters)),
                             "note": "segment mode 1: runs of IN nodes (the 3D solver's segmentation), so the disc "

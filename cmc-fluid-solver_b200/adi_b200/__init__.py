@@ -317,6 +317,12 @@ class AdiSolver2D:
         rc = self.lib.adi2d_step(self.h, dt, num_global, num_local, C.byref(it))
         return rc, it.value
 
+    def step_tol(self, dt, max_global, num_local, tol):
+        """UpdateBoundaries + tolerance-mode step; returns (status, iterations, residual)."""
+        it, r = C.c_int(0), C.c_double(0)
+        rc = self.lib.adi2d_step_tol(self.h, dt, max_global, num_local, tol, C.byref(it), C.byref(r))
+        return rc, it.value, r.value
+
     def fields(self, which: int = 0):
         out = [np.zeros(self.shape, self.dtype) for _ in range(3)]
         self._check(self.lib.adi2d_get_state(self.h, which, *[_ptr(a) for a in out]))

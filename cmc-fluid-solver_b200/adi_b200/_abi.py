@@ -34,7 +34,7 @@ EXPORTED = [
     "adi_batch_set_chunk", "adi_batch_get_chunk", "adi_batch_autotune", "adi_batch_set_graphs",
     "adi_batch_launches", "adi_batch_last_error_string", "adi_batch_time_sweeps", "adi_adjoint_run",
     "adi_set_node_values", "adi_set_adjoint_chunk", "adi2d_create", "adi2d_destroy", "adi2d_set_stream", "adi2d_set_grid",
-    "adi2d_set_segments",
+    "adi2d_set_segments", "adi2d_step_tol",
     "adi2d_update_boundaries", "adi2d_time_step", "adi2d_step", "adi2d_get_state", "adi2d_set_state",
     "adi2d_get_layer", "adi2d_last_error", "adi2d_last_error_string",
 ]
@@ -123,6 +123,7 @@ def load() -> C.CDLL:
         "adi2d_set_stream": [vp, vp],
         "adi2d_set_grid": [vp, vp, vp, vp, vp, vp, d],
         "adi2d_set_segments": [vp, i],
+        "adi2d_step_tol": [vp, d, i, i, d, C.POINTER(i), C.POINTER(d)],
         "adi2d_update_boundaries": [vp],
         "adi2d_time_step": [vp, d, i, i, C.POINTER(i)],
         "adi2d_step": [vp, d, i, i, C.POINTER(i)],

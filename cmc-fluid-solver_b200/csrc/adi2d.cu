@@ -117,6 +117,48 @@ __global__ void clear_out_kernel(long long n, const uint8_t *__restrict__ type, 
 
 // Divergence error terms of the 2x2 all-IN blocks, one fixed-order block tree per
 // CTA into partial[blockIdx.x], then the last kernel folds the partials.
+// Tolerance-mode residual: max |x - t| and max |x| over NODE_IN nodes and the three
+// fields, folded per warp with shuffles and across warps with atomicMax on the bit
+// patterns (non-negative values order like their patterns; a NaN wins).
+template <typename R>
+__device__ __forceinline__ R max_nan2(R a, R b)
+{
+    return (b > a || b != b) ? b : a;
+}
+
+template <typename R>
+__global__ void residual2_kernel(long long n, const uint8_t *__restrict__ type, L2<R> x, L2<R> t,
+                                 unsigned long long *out)
+{
+    R dm = R(0), xm = R(0);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        if (type[i] != NODE_IN) continue;
+#pragma unroll
+        for (int v = 0; v < 3; v++) {
+            const R a = x.f[v][i];
+            dm = max_nan2(dm, (R)fabs(a - t.f[v][i]));
+            xm = max_nan2(xm, (R)fabs(a));
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        dm = max_nan2(dm, __shfl_xor_sync(0xffffffffu, dm, o));
+        xm = max_nan2(xm, __shfl_xor_sync(0xffffffffu, xm, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        unsigned long long bd, bx;
+        if (sizeof(R) == 8) {
+            bd = (unsigned long long)__double_as_longlong((double)dm);
+            bx = (unsigned long long)__double_as_longlong((double)xm);
+        } else {
+            bd = (unsigned long long)__float_as_uint((float)dm);
+            bx = (unsigned long long)__float_as_uint((float)xm);
+        }
+        atomicMax(out, bd);
+        atomicMax(out + 1, bx);
+    }
+}
+
 template <typename R>
 __global__ void div2_partial_kernel(int nx, int ny, const uint8_t *__restrict__ type, L2<R> l, R dx, R dy,
                                     double *psum, unsigned long long *pcnt)
@@ -415,7 +457,7 @@ struct adi2d_handle {
     cudaStream_t stream = nullptr, cap_stream = nullptr;
     uint8_t *d_type = nullptr, *d_bct = nullptr;
     std::vector<uint8_t> h_type;
-    void *d_data[3] = {}, *d_L[6][3] = {};   // cur, next, half, temp, next_local, temp_local
+    void *d_data[3] = {}, *d_L[7][3] = {};   // cur, next, half, temp, next_local, temp_local, prev
     Seg *d_segx = nullptr, *d_segy = nullptr;
     int nsegx = 0, nsegy = 0;
     void *d_scratch = nullptr;
@@ -429,6 +471,7 @@ struct adi2d_handle {
     std::string msg;
     cudaGraphExec_t graph = nullptr;
     uint64_t graph_key[2] = {0, 0};
+    unsigned long long *d_res = nullptr;   // tolerance mode: max |x - t|, max |x| bit patterns
     int seg_mode = 0;             // 0: row-spanning (the reference), 1: masked segments
     size_t scratch_bytes = 0;
 };
@@ -436,7 +479,7 @@ struct adi2d_handle {
 namespace {
 
 constexpr int D2_BLOCKS = 64;
-enum { CUR = 0, NXT = 1, HALF = 2, TMP = 3, NLOC = 4, TLOC = 5 };
+enum { CUR = 0, NXT = 1, HALF = 2, TMP = 3, NLOC = 4, TLOC = 5, PREV = 6 };
 
 adi_status f2(adi2d_handle *h, adi_status s, const std::string &m)
 {
@@ -661,6 +704,88 @@ adi_status time_step(adi2d_handle *h, double dt, int num_global, int num_local, 
     return ADI_OK;
 }
 
+// Tolerance mode (no counterpart in the reference, whose 2D loop runs num_global
+// iterations and then continues while the divergence error exceeds 0.1,
+// AdiSolver2D.cpp:290-314): global iterations run until the change of the iterate
+//   r = max |x_k - x_(k-1)| / max |x_k|   over NODE_IN nodes and the three fields
+// (x_k the layer after iteration k, x_0 the state the step starts from) is <= tol,
+// at most max_global of them.  (The nonlinear layer itself is no measure here:
+// SolveDirection hands its temp_local back to temp, AdiSolver2D.cpp:220-225, so
+// after the X direction it equals the result.)  The reference's guard stays: an
+// error above 1.0 is ADI_ERR_DIVERGENCE.  The host reads error and residual after
+// every iteration, so this path runs eagerly.
+template <typename R>
+adi_status time_step_tol(adi2d_handle *h, double dt, int max_global, int num_local, double tol, bool bnd,
+                         int *iters, double *residual)
+{
+    if (h->err_slots < 4) {
+        cudaFree(h->d_err);
+        cudaFreeHost(h->h_err);
+        h->d_err = nullptr;
+        h->h_err = nullptr;
+        h->err_slots = 128;
+        CK2(cudaMalloc((void **)&h->d_err, sizeof(double) * h->err_slots));
+        CK2(cudaMallocHost((void **)&h->h_err, sizeof(double) * h->err_slots));
+        if (h->graph) cudaGraphExecDestroy(h->graph);
+        h->graph = nullptr;
+    }
+    adi_status s;
+    if (bnd && (s = update_boundaries<R>(h)) != ADI_OK) return s;
+    const uint8_t all = T_IN | T_OUT | T_BOUND | T_VALVE;
+    if ((s = copy_types<R>(h, CUR, NXT, all)) != ADI_OK) return s;
+    if ((s = copy_types<R>(h, CUR, HALF, all)) != ADI_OK) return s;
+    if ((s = copy_types<R>(h, CUR, TMP, all)) != ADI_OK) return s;
+    const long long n = (long long)h->nx * h->ny;
+    double err = 0, r = NAN;
+    int it = 0;
+    while (it < max_global) {
+        if ((s = copy_types<R>(h, NXT, PREV, T_IN)) != ADI_OK) return s;
+        if ((s = solve_dir<R>(h, dt, num_local, h->d_segy, h->nsegy, CUR, HALF)) != ADI_OK) return s;
+        if ((s = solve_dir<R>(h, dt, num_local, h->d_segx, h->nsegx, HALF, NXT)) != ADI_OK) return s;
+        if ((s = div2<R>(h, NXT, 0)) != ADI_OK) return s;
+        CK2(cudaMemsetAsync(h->d_res, 0, 2 * sizeof(unsigned long long), h->stream));
+        residual2_kernel<R><<<blocks_for(n), 256, 0, h->stream>>>(n, h->d_type, lay<R>(h, NXT), lay<R>(h, PREV),
+                                                                  h->d_res);
+        CK2(cudaGetLastError());
+        if ((s = it == 0 ? copy_types<R>(h, NXT, TMP, T_IN) : merge_in<R>(h, NXT, TMP)) != ADI_OK) return s;
+        CK2(cudaMemcpyAsync(h->h_err, h->d_err, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK2(cudaMemcpyAsync(h->h_err + 1, h->d_res, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                            h->stream));
+        CK2(cudaStreamSynchronize(h->stream));
+        it++;
+        err = h->h_err[0];
+        unsigned long long bits[2];
+        memcpy(bits, h->h_err + 1, sizeof bits);
+        double dm, xm;
+        if (sizeof(R) == 8) {
+            memcpy(&dm, &bits[0], 8);
+            memcpy(&xm, &bits[1], 8);
+        } else {
+            float a, b;
+            const uint32_t ua = (uint32_t)bits[0], ub = (uint32_t)bits[1];
+            memcpy(&a, &ua, 4);
+            memcpy(&b, &ub, 4);
+            dm = a;
+            xm = b;
+        }
+        r = xm > 0 ? dm / xm : dm;
+        if (err > 0.1 * 10) {
+            h->last_err = err;
+            return f2(h, ADI_ERR_DIVERGENCE, "2D divergence error above 1.0");
+        }
+        if (r <= tol) break;
+    }
+    clear_out_kernel<R><<<blocks_for(n), 256, 0, h->stream>>>(n, h->d_type, lay<R>(h, NXT), (R)h->startT);
+    CK2(cudaGetLastError());
+    if ((s = copy_types<R>(h, NXT, CUR, all)) != ADI_OK) return s;
+    CK2(cudaStreamSynchronize(h->stream));
+    h->last_err = err;
+    h->last_iters = it;
+    if (iters) *iters = it;
+    if (residual) *residual = r;
+    return ADI_OK;
+}
+
 // Masked segments: the 3D solver's segmentation (Grid3D::GenerateListSegments,
 // Grid3D.cpp:47-127) on the 2D grid's columns and rows -- every maximal run of IN
 // nodes, with the non-IN node on each side as its boundary rows; a run reaching the
@@ -727,13 +852,14 @@ void free2(adi2d_handle *h)
     cudaFree(h->d_type);
     cudaFree(h->d_bct);
     for (int v = 0; v < 3; v++) cudaFree(h->d_data[v]);
-    for (int l = 0; l < 6; l++)
+    for (int l = 0; l < 7; l++)
         for (int v = 0; v < 3; v++) cudaFree(h->d_L[l][v]);
     cudaFree(h->d_segx);
     cudaFree(h->d_segy);
     cudaFree(h->d_scratch);
     cudaFree(h->d_psum);
     cudaFree(h->d_pcnt);
+    cudaFree(h->d_res);
     cudaFree(h->d_err);
     cudaFreeHost(h->h_err);
 }
@@ -762,7 +888,7 @@ adi_status adi2d_create(int nx, int ny, double dx, double dy, int precision, con
     cudaError_t e = cudaMalloc((void **)&h->d_type, n);
     if (e == cudaSuccess) e = cudaMalloc((void **)&h->d_bct, n);
     for (int v = 0; v < 3 && e == cudaSuccess; v++) e = cudaMalloc(&h->d_data[v], fb);
-    for (int l = 0; l < 6 && e == cudaSuccess; l++)
+    for (int l = 0; l < 7 && e == cudaSuccess; l++)
         for (int v = 0; v < 3 && e == cudaSuccess; v++) {
             e = cudaMalloc(&h->d_L[l][v], fb);
             if (e == cudaSuccess) e = cudaMemset(h->d_L[l][v], 0, fb);
@@ -770,6 +896,7 @@ adi_status adi2d_create(int nx, int ny, double dx, double dy, int precision, con
     if (e == cudaSuccess) e = cudaMalloc(&h->d_scratch, 5 * fb);
     if (e == cudaSuccess) h->scratch_bytes = 5 * fb;
     if (e == cudaSuccess) e = cudaMalloc((void **)&h->d_psum, sizeof(double) * D2_BLOCKS);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&h->d_res, 2 * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMalloc((void **)&h->d_pcnt, sizeof(unsigned long long) * D2_BLOCKS);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
@@ -902,6 +1029,18 @@ adi_status adi2d_time_step(adi2d_handle *h, double dt, int num_global, int num_l
 adi_status adi2d_step(adi2d_handle *h, double dt, int num_global, int num_local, int *iters_used)
 {
     return step2(h, dt, num_global, num_local, true, iters_used);
+}
+
+adi_status adi2d_step_tol(adi2d_handle *h, double dt, int max_global, int num_local, double tol, int *iters_used,
+                          double *residual)
+{
+    if (!h) return ADI_ERR_BAD_ARG;
+    if (!h->grid_set) return f2(h, ADI_ERR_STATE, "adi2d_set_grid has not been called");
+    if (max_global < 1 || num_local < 1) return f2(h, ADI_ERR_BAD_ARG, "max_global >= 1 and num_local >= 1");
+    if (!(dt > 0) || !std::isfinite(dt)) return f2(h, ADI_ERR_BAD_ARG, "dt must be positive and finite");
+    if (!(tol >= 0)) return f2(h, ADI_ERR_BAD_ARG, "tol must be >= 0");
+    if (h->prec == ADI_FP64) return time_step_tol<double>(h, dt, max_global, num_local, tol, true, iters_used, residual);
+    return time_step_tol<float>(h, dt, max_global, num_local, tol, true, iters_used, residual);
 }
 
 adi_status adi2d_get_state(adi2d_handle *h, int which, void *u, void *v, void *T)

@@ -327,6 +327,18 @@ adi_status adi2d_time_step(adi2d_handle *h, double dt, int num_global, int num_l
 /* adi2d_update_boundaries + adi2d_time_step (FluidSolver2D.cpp:131-132). */
 adi_status adi2d_step(adi2d_handle *h, double dt, int num_global, int num_local, int *iters_used);
 
+/* adi2d_update_boundaries + the step in tolerance mode (no counterpart in the
+ * reference, whose loop runs num_global iterations and then continues while the
+ * divergence error exceeds 0.1): global iterations run until the change of the
+ * iterate
+ *   r = max |x_k - x_(k-1)| / max |x_k|   over NODE_IN nodes and the three fields
+ * (x_k the layer after global iteration k, x_0 the state the step starts from) is
+ * <= tol, at most max_global of them.  The divergence guard stays (error above
+ * 1.0: ADI_ERR_DIVERGENCE).  *iters_used and *residual (either may be NULL) get
+ * the count and the last r.  Synchronises after every iteration. */
+adi_status adi2d_step_tol(adi2d_handle *h, double dt, int max_global, int num_local, double tol, int *iters_used,
+                          double *residual);
+
 /* which 0: cur (the state), 1: next; handle precision, [i][j]. */
 adi_status adi2d_get_state(adi2d_handle *h, int which, void *u, void *v, void *T);
 /* Solver2D::SetLayer (Solver2D.cpp:30-38): the state. */

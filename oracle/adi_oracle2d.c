@@ -184,6 +184,20 @@ int oracle2d_step(void *vh, double dt, int num_global, int num_local)
     return time_step2_f32(s, (float)dt, num_global, num_local);
 }
 
+/* UpdateBoundaries + the tolerance-mode step (time_step2_tol). */
+int oracle2d_step_tol(void *vh, double dt, int max_global, int num_local, double tol, double *res)
+{
+    oracle2d_h *h = vh;
+    if (h->precision == 8) {
+        solver2_f64 *s = h->s;
+        update_bnd2_f64(s);
+        return time_step2_tol_f64(s, dt, max_global, num_local, tol, res);
+    }
+    solver2_f32 *s = h->s;
+    update_bnd2_f32(s);
+    return time_step2_tol_f32(s, (float)dt, max_global, num_local, tol, res);
+}
+
 /* which: 0 cur, 1 next.  Output as double, [i][j]. */
 int oracle2d_get_fields(void *vh, int which, double *u, double *v, double *T_)
 {

@@ -254,6 +254,58 @@ static int FN(time_step2)(FN(solver2) *s, REAL dt, int num_global, int num_local
     return it;
 }
 
+/* Tolerance mode (no counterpart in the reference; restates adi2d_step_tol):
+ * global iterations until r = max|next_k - next_(k-1)| / max|next_k| over NODE_IN
+ * nodes and the three fields (next_0 = the state the step starts from) is <= tol,
+ * at most max_global of them; the reference's guard (error above 1.0) returns -1.
+ * Returns the iterations run; *res gets the last r. */
+static int FN(time_step2_tol)(FN(solver2) *s, REAL dt, int max_global, int num_local, double tol, double *res)
+{
+    FN(copy_all)(s, &s->cur, &s->next);
+    FN(copy_all)(s, &s->cur, &s->half);
+    FN(copy_all)(s, &s->cur, &s->temp);
+    double err = 0, r = NAN;
+    size_t n = (size_t)s->nx * s->ny;
+    int it = 0;
+    REAL *prev = malloc(sizeof(REAL) * 3 * n);
+    while (it < max_global) {
+        for (size_t q = 0; q < n; q++) { prev[q] = s->next.u[q]; prev[n + q] = s->next.v[q]; prev[2 * n + q] = s->next.t[q]; }
+        FN(solve_dir2)(s, dt, num_local, s->segy, s->nsegy, &s->cur, &s->temp, &s->half);
+        FN(solve_dir2)(s, dt, num_local, s->segx, s->nsegx, &s->half, &s->temp, &s->next);
+        err = FN(div_err2)(s, &s->next);
+        REAL dm = 0, xm = 0;
+        for (size_t q = 0; q < n; q++) {
+            if (s->type[q] != NODE_IN_) continue;
+            const REAL *xs[3] = {s->next.u, s->next.v, s->next.t}, *ts[3] = {prev, prev + n, prev + 2 * n};
+            for (int v = 0; v < 3; v++) {
+                REAL a = xs[v][q], d = (REAL)FN(absr)(a - ts[v][q]), ax = (REAL)FN(absr)(a);
+                if (d > dm || d != d) dm = d;
+                if (ax > xm || ax != ax) xm = ax;
+            }
+        }
+        if (it == 0) FN(copy_type)(s, &s->next, &s->temp, NODE_IN_);
+        else FN(merge_in)(s, &s->next, &s->temp);
+        it++;
+        r = xm > 0 ? (double)dm / (double)xm : (double)dm;
+        if (err > 0.1 * 10) { s->last_err = err; *res = r; free(prev); return -1; }
+        if (r <= tol) break;
+    }
+    free(prev);
+    /* ClearOutterCells (Solver2D.cpp:68-80) */
+    for (int i = 0; i < s->nx; i++)
+        for (int j = 0; j < s->ny; j++)
+            if (s->type[IX(s, i, j)] == NODE_OUT_) {
+                s->next.u[IX(s, i, j)] = 0.0;
+                s->next.v[IX(s, i, j)] = 0.0;
+                s->next.t[IX(s, i, j)] = s->startT;
+            }
+    FN(copy_all)(s, &s->next, &s->cur);
+    s->last_err = err;
+    s->last_iters = it;
+    *res = r;
+    return it;
+}
+
 #undef IX
 #undef CAT_
 #undef CAT

@@ -265,6 +265,8 @@ def _load_oracle2d():
         lib.oracle2d_last_err.argtypes = [C.c_void_p]
         lib.oracle2d_segments.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
         lib.oracle2d_set_segments.argtypes = [C.c_void_p, C.c_int]
+        lib.oracle2d_step_tol.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_double,
+                                          C.POINTER(C.c_double)]
         lib.oracle2d_destroy.argtypes = [C.c_void_p]
         _orc2d = lib
     return _orc2d
@@ -313,6 +315,12 @@ class Oracle2D:
 
     def step(self, dt, num_global, num_local) -> int:
         return self.lib.oracle2d_step(self.h, dt, num_global, num_local)
+
+    def step_tol(self, dt, max_global, num_local, tol):
+        """Tolerance-mode step: (iterations or -1, last residual)."""
+        r = C.c_double()
+        it = self.lib.oracle2d_step_tol(self.h, dt, max_global, num_local, tol, C.byref(r))
+        return it, r.value
 
     def fields(self, which=0):
         out = [np.zeros(self.shape) for _ in range(3)]

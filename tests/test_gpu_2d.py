@@ -79,6 +79,25 @@ def test_masked_segments_bit_exact(adi_lib, precision, case):
         assert np.array_equal(a.astype(np.float64), b)
 
 
+@pytest.mark.parametrize("precision", [4, 8])
+@pytest.mark.parametrize("tol", [1e-6, 1e-2, 0.0])
+def test_tolerance_mode_bit_exact(adi_lib, precision, tol):
+    """adi2d_step_tol (up to 4 global iterations until the iterate changes by at
+    most tol): iteration counts, residuals and fields equal to the restatement
+    oracle's tolerance mode, bit for bit."""
+    d = G2.channel_disc(48, 32, radius=5.0, cx=16, cy=16)
+    g = _gpu(adi_lib, d, precision)
+    o = O.Oracle2D(d, precision=precision)
+    for s in range(4):
+        rc, it, r = g.step_tol(1e-3, 4, 1, tol)
+        ito, ro = o.step_tol(1e-3, 4, 1, tol)
+        assert rc == 0 and it == ito and 1 <= it <= 4
+        assert r == ro
+        for which in (0, 1):
+            for a, b in zip(g.fields(which), o.fields(which)):
+                assert np.array_equal(a.astype(np.float64), b), (s, which)
+
+
 def test_layer_io_and_exit_conditions(adi_lib):
     from adi_b200 import _abi
     d = G2.random_domain2d(24, 16, seed=23)

@@ -72,3 +72,27 @@ def test_masked_mode_with_obstacles_runs_and_differs():
     # switching back restores the reference segmentation
     b.set_segment_mode(0)
     assert np.array_equal(a.segments(), b.segments())
+
+
+def test_tolerance_mode_restatement():
+    """Tolerance mode of the 2D restatement: tol = 0 runs max_global iterations and
+    equals the reference-mode step wherever that one stops at num_global (error
+    below 0.1); a huge tol stops after one iteration; the residual falls with the
+    iterations."""
+    d = G2.random_domain2d(26, 18, seed=33, n_discs=2, rmax=2.0)
+    a = O.Oracle2D(d, precision=8)
+    b = O.Oracle2D(d, precision=8)
+    for _ in range(2):
+        it = a.step(1e-3, 3, 1)
+        assert it == 3 and a.last_err() <= 0.1
+        itb, r = b.step_tol(1e-3, 3, 1, 0.0)
+        assert itb == 3 and r > 0
+    for x, y in zip(a.fields(0), b.fields(0)):
+        assert np.array_equal(x, y)
+    c = O.Oracle2D(d, precision=8)
+    assert c.step_tol(1e-3, 4, 1, 1e9)[0] == 1
+    rs = []
+    for m in (1, 2, 3, 4):
+        e = O.Oracle2D(d, precision=8)
+        rs.append(e.step_tol(1e-3, m, 1, 0.0)[1])
+    assert rs[-1] < rs[0]
