@@ -104,21 +104,38 @@ __global__ void __launch_bounds__(256, 2)
     const R mt = merges == 2 ? R(0.25) : R(0.5);
 
     // ---------------- rows: kinds, window values, A^T and xbar ----------------
+    // All first-phase loads go out together: codes, the advecting field and the
+    // destination / temp adjoints of every row inside the line's segment range
+    // (addresses valid there); the row kinds then mask what a row does not use.
     uint8_t cc[K + 4];   // codes of rows p0-2 .. p0+K+1 (OUT outside the segment range)
 #pragma unroll
     for (int q = 0; q < K + 4; q++) {
         const int p = p0 - 2 + q;
         cc[q] = (active && p >= lo && p <= hi) ? d.code[base + (long long)p * sl] : uint8_t(NODE_OUT);
     }
+    R wv[K + 2];     // advecting temp at window rows
+#pragma unroll
+    for (int q = 0; q < K + 2; q++) {
+        const int p = p0 - 1 + q;
+        wv[q] = (active && p >= lo && p <= hi) ? ti.f[DIR][base + (long long)p * sl] : R(0);
+    }
+    R dbr[4][K], tbr[4][K];   // destination and temp adjoints at the owned rows
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        const int p = p0 + i;
+        const bool ok = active && p >= lo && p <= hi;
+        const long long off = base + (long long)p * sl;
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            dbr[v][i] = ok ? dbar.f[v][off] : R(0);
+            tbr[v][i] = ok ? tbar.f[v][off] : R(0);
+        }
+    }
     int kd[K + 2];   // kinds of rows p0-1 .. p0+K
 #pragma unroll
     for (int q = 0; q < K + 2; q++) kd[q] = qkind(code_is_in(cc[q]), code_is_in(cc[q + 1]), code_is_in(cc[q + 2]));
-    R wv[K + 2];     // advecting temp at window rows (IN rows only)
 #pragma unroll
-    for (int q = 0; q < K + 2; q++) {
-        const long long off = base + (long long)(p0 - 1 + q) * sl;
-        wv[q] = kd[q] == Q_IN ? ti.f[DIR][off] : R(0);
-    }
+    for (int q = 0; q < K + 2; q++) wv[q] = kd[q] == Q_IN ? wv[q] : R(0);
     R A[2][K], B[2][K], C[2][K], xb[4][K];
 #pragma unroll
     for (int i = 0; i < K; i++) {
@@ -137,10 +154,11 @@ __global__ void __launch_bounds__(256, 2)
         }
 #pragma unroll
         for (int v = 0; v < 4; v++) {
-            const R db = kd[q] != Q_NONE ? dbar.f[v][off] : R(0);
-            const R to = kd[q] == Q_IN ? tbar.f[v][off] : R(0);
+            const R db = kd[q] != Q_NONE ? dbr[v][i] : R(0);
+            const R to = kd[q] == Q_IN ? tbr[v][i] : R(0);
             xb[v][i] = db + mx * to;
         }
+        (void)off;
     }
 
     // ---------------- chunk elimination of A^T ----------------
@@ -295,7 +313,7 @@ __global__ void __launch_bounds__(256, 2)
         const bool in = kd[q] == Q_IN;
 #pragma unroll
         for (int v = 0; v < 4; v++) {
-            R x = (in ? mt : R(1)) * tbar.f[v][off];   // not yet rewritten: this thread owns the row
+            R x = (in ? mt : R(1)) * tbr[v][i];   // loaded at the start: this thread owns the row
             if (v == DIR) x += wb[i];
             x += i > 0 ? up[v][i - 1] : upp[v];
             x += i < K - 1 ? dn[v][i + 1] : dnn[v];
