@@ -92,6 +92,10 @@ struct adi_handle {
     bool graphs_on = true;
     cudaStream_t cap_stream = nullptr;
     int adjoint_K = 4;   // chunk length of the adjoint sweep; 0: one thread per line
+    // adjoint workspace (checkpoints, tape, adjoint layers), kept between
+    // adi_adjoint_run calls and grown when a call needs more; freed by adi_destroy
+    char *adj_mem = nullptr;
+    size_t adj_cap = 0;
     std::string contract_msg;
     std::string err;
     double diff_error = 0.0;
@@ -221,6 +225,9 @@ cudaError_t fold_profile(adi_handle *h)
 
 void free_all(adi_handle *h)
 {
+    cudaFree(h->adj_mem);
+    h->adj_mem = nullptr;
+    h->adj_cap = 0;
     for (auto &r : h->ev_pending) {
         cudaEventDestroy(r.a);
         cudaEventDestroy(r.b);
@@ -668,12 +675,25 @@ adi_status time_step_tol(adi_handle *h, double dt, int max_global, int num_local
 // ---------------------------------------------------------------------------
 
 // One device allocation carved into 256-byte aligned pieces (thousands of tape
-// fields would otherwise cost a cudaMalloc each).
+// fields would otherwise cost a cudaMalloc each).  The allocation belongs to the
+// handle and is reused by later calls whose workspace fits.
 struct DevArena {
     char *base = nullptr;
     size_t cap = 0, used = 0;
-    ~DevArena() { cudaFree(base); }
-    cudaError_t reserve(size_t bytes) { cap = bytes; return cudaMalloc((void **)&base, bytes); }
+    cudaError_t reserve(adi_handle *h, size_t bytes)
+    {
+        if (h->adj_cap < bytes) {
+            cudaFree(h->adj_mem);
+            h->adj_mem = nullptr;
+            h->adj_cap = 0;
+            const cudaError_t e = cudaMalloc((void **)&h->adj_mem, bytes);
+            if (e != cudaSuccess) return e;
+            h->adj_cap = bytes;
+        }
+        base = h->adj_mem;
+        cap = h->adj_cap;
+        return cudaSuccess;
+    }
     void *get(size_t bytes, cudaError_t &e)
     {
         const size_t b = (bytes + 255) / 256 * 256;
@@ -711,7 +731,7 @@ adi_status adjoint_run(adi_handle *h, double dt, int ng, int nl, int n_steps, in
     const int win = ck < n_steps ? ck : n_steps;
     const size_t fbr = (fb + 255) / 256 * 256;
     DevArena mem;
-    cudaError_t e = mem.reserve(fbr * ((size_t)nck * 4 + 4 * 6 + 2 + (size_t)win * S * 8) + 256 * (DIV_BLOCKS + 16));
+    cudaError_t e = mem.reserve(h, fbr * ((size_t)nck * 4 + 4 * 6 + 2 + (size_t)win * S * 8) + 256 * (DIV_BLOCKS + 16));
     auto layer4 = [&](void **out) {
         for (int v = 0; v < 4; v++) out[v] = mem.get(fb, e);
     };

@@ -265,8 +265,9 @@ adi_status adi_device_pointers(adi_handle *h, void *out8[8]);
  * the sweeps in reverse order, each as a transposed tridiagonal solve over the same
  * segments, recomputing the steps of each window of ckpt_every steps from a
  * stored state.  Device memory: (n_steps/ckpt_every + 12) layers plus the tape of
- * one window, ckpt_every * num_global * num_local * 3 * 8 fields.  The handle ends
- * at the final state. */
+ * one window, ckpt_every * num_global * num_local * 3 * 8 fields, in one
+ * allocation that the handle keeps for later calls (grown when a call needs more,
+ * freed by adi_destroy).  The handle ends at the final state. */
 adi_status adi_adjoint_run(adi_handle *h, double dt, int num_global, int num_local, int n_steps, int ckpt_every,
                            const int box_lo[3], const int box_hi[3], double *J, void *nv_grad, void *state_grad);
 
