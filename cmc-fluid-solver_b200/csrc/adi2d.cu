@@ -415,22 +415,38 @@ __global__ void sweep2_smem_kernel(int nx, int ny, const Seg *__restrict__ segs,
         const R *a = v < 2 ? a_uv : a_t, *b = v < 2 ? b_uv : b_t, *c = v < 2 ? c_uv : c_t;
         R *d = dd + v * n, *cp = cpr + v * n;
         // Thomas (Algorithms.h:21-39) in the reference's operand order
+        // Each row's coefficients are read before the previous row's results are
+        // stored, so the shared-memory loads stay off the dependent chain (the
+        // arithmetic and its order are unchanged).
         R cprev = c[0] / b[0];
         R dprev = d[0] / b[0];
         cp[0] = cprev;
         d[0] = dprev;
+        R an = a[1], bn = b[1], cn = c[1], dn = d[1];   // segments have at least three rows
         for (int p = 1; p < n; p++) {
-            const R ap = a[p], bp = b[p];
-            const R cc = c[p] / (bp - ap * cprev);
-            const R dv = (d[p] - dprev * ap) / (bp - ap * cprev);
+            const R ap = an, bp = bn, cq = cn, dq = dn;
+            if (p + 1 < n) {
+                an = a[p + 1];
+                bn = b[p + 1];
+                cn = c[p + 1];
+                dn = d[p + 1];
+            }
+            const R cc = cq / (bp - ap * cprev);
+            const R dv = (dq - dprev * ap) / (bp - ap * cprev);
             cp[p] = cc;
             d[p] = dv;
             cprev = cc;
             dprev = dv;
         }
         R x = dprev;   // x[n-1] = d'[n-1]
+        R dm = d[n - 2], cm = cp[n - 2];
         for (int p = n - 2; p >= 0; p--) {
-            x = d[p] - cp[p] * x;
+            const R dq = dm, cq = cm;
+            if (p > 0) {
+                dm = d[p - 1];
+                cm = cp[p - 1];
+            }
+            x = dq - cq * x;
             d[p] = x;
         }
     }
