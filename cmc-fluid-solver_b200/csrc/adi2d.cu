@@ -584,11 +584,8 @@ adi_status solve_dir(adi2d_handle *h, double dt, int num_local, const Seg *segs,
     const size_t smem = (size_t)12 * len * sizeof(R);
     for (int it = 0; it < num_local; it++) {
         if (nseg > 0 && smem <= 200 * 1024) {
-            static size_t smem_set = 0;
-            if (smem > 48 * 1024 && smem > smem_set) {
-                CK2(cudaFuncSetAttribute(sweep2_smem_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                smem_set = smem;
-            }
+            static SmemOptIn opt_in;
+            if (smem > 48 * 1024) CK2(ensure_dynamic_smem(opt_in, sweep2_smem_kernel<R>, smem));
             sweep2_smem_kernel<R><<<nseg, 128, smem, h->stream>>>(h->nx, h->ny, segs, h->d_bct, data, lay<R>(h, cur),
                                                                   lay<R>(h, TLOC), lay<R>(h, NLOC), consts<R>(h, dt));
             CK2(cudaGetLastError());

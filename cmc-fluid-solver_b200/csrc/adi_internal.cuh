@@ -3,8 +3,32 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <mutex>
 
 namespace adi {
+
+// Largest dynamic shared-memory size one kernel has been opened to, per device.
+// cudaFuncSetAttribute acts on the current device only, so a process that drives
+// several GPUs must open the kernel on each of them.  The mutex keeps the
+// attribute monotone when two host threads launch the same kernel at once.
+struct SmemOptIn {
+    std::mutex mu;
+    int bytes[64] = {};
+};
+
+template <typename F>
+inline cudaError_t ensure_dynamic_smem(SmemOptIn &rec, F *kern, size_t bytes)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    std::lock_guard<std::mutex> lock(rec.mu);
+    if ((int)bytes <= rec.bytes[dev]) return cudaSuccess;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) rec.bytes[dev] = (int)bytes;
+    return e;
+}
 
 // Node types and BC codes of the reference (Common/Geometry.h:31-41).
 enum : uint8_t { NODE_IN = 0, NODE_OUT = 1, NODE_BOUND = 2, NODE_VALVE = 3 };

@@ -424,12 +424,9 @@ cudaError_t launch_sweep_xypair(int dir, const DomainView<float> &d, const int *
 #define XP(DD, KK)                                                                                              \
     if (dir == DD && K == KK) {                                                                                 \
         auto kern = sweep_xypair_kernel<DD, KK>;                                                                \
-        static int smem_set = 0;                                                                                \
-        if ((int)smem > smem_set) {                                                                             \
-            e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);             \
-            if (e != cudaSuccess) return e;                                                                     \
-            smem_set = (int)smem;                                                                               \
-        }                                                                                                       \
+        static SmemOptIn opt_in;                                                                                \
+        e = ensure_dynamic_smem(opt_in, kern, smem);                                                            \
+        if (e != cudaSuccess) return e;                                                                         \
         int per_sm = 0;                                                                                         \
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);                        \
         if (e != cudaSuccess) return e;                                                                         \

@@ -490,12 +490,9 @@ cudaError_t launch_sweep_xytma(int dir, const DomainView<R> &d, const int *line_
 #define XL(DD, KK, NN, PP)                                                                                       \
     if (dir == DD && K == KK && nlt == NN && P == PP) {                                                          \
         auto kern = sweep_xytma_kernel<R, DD, KK, NN, PP>;                                                       \
-        static int smem_set = 0;                                                                                 \
-        if ((int)smem > smem_set) {                                                                              \
-            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
-            if (e != cudaSuccess) return e;                                                                      \
-            smem_set = (int)smem;                                                                                \
-        }                                                                                                        \
+        static SmemOptIn opt_in;                                                                                 \
+        cudaError_t e = ensure_dynamic_smem(opt_in, kern, smem);                                                 \
+        if (e != cudaSuccess) return e;                                                                          \
         kern<<<blocks, threads, smem, s>>>(maps, d, g, line_lo, next, tout, k, merges, err_flag);                \
         return cudaGetLastError();                                                                               \
     }
