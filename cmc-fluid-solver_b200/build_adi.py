@@ -38,6 +38,7 @@ SOURCES = [
     ("adjoint.cu", []),
     ("adjoint_fast.cu", []),
     ("adi2d.cu", ["--fmad=false"]),
+    ("masks.cu", ["--fmad=false"]),
 ]
 
 

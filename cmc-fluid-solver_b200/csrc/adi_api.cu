@@ -13,6 +13,7 @@
 
 #include <type_traits>
 
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -998,6 +999,193 @@ adi_status adi_set_mask(adi_handle *h, const uint8_t *type, const uint8_t *bc_ve
     h->segs_built = false;
     invalidate_graphs(h);
     h->bv_synced = true;   // the initial state is the node values
+    return ADI_OK;
+}
+
+namespace {
+
+// Device scratch of one mask build, released on every return path.
+struct MaskScratch {
+    std::vector<void *> p;
+    ~MaskScratch()
+    {
+        for (void *q : p) cudaFree(q);
+    }
+    cudaError_t get(void **out, size_t bytes)
+    {
+        *out = nullptr;
+        cudaError_t e = cudaMalloc(out, bytes < 16 ? 16 : bytes);
+        if (e == cudaSuccess) p.push_back(*out);
+        return e;
+    }
+};
+
+// What adi_set_mask derives on the host from a mask, for a mask a device builder
+// wrote into d_code / d_nv (and the initial state into cur).
+adi_status finish_device_mask(adi_handle *h)
+{
+    const long long n = h->n;
+    std::vector<uint8_t> code(n), t(n), bv(n), bt(n);
+    CK(cudaMemcpyAsync(code.data(), h->d_code, n, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    long long nin = 0;
+    for (long long i = 0; i < n; i++) {
+        t[i] = code[i] & CODE_TYPE;
+        bv[i] = (code[i] & CODE_VEL_FREE) ? BC_FREE : BC_NOSLIP;
+        bt[i] = (code[i] & CODE_TEMP_FREE) ? BC_FREE : BC_NOSLIP;
+        nin += t[i] == NODE_IN;
+    }
+    h->contract_msg = check_contract(h, t.data(), bv.data(), bt.data());
+    h->contract_ok = h->contract_msg.empty();
+    h->num_in = nin;
+    h->mask_set = true;
+    h->segs_built = false;
+    invalidate_graphs(h);
+    h->bv_synced = true;   // the initial state is the node values
+    return ADI_OK;
+}
+
+// Status words of a builder: writes outside the grid, loops stopped at their bound.
+adi_status mask_status(adi_handle *h, const int *d_status, const char *what)
+{
+    int st[2] = {0, 0};
+    CK(cudaMemcpyAsync(st, d_status, sizeof st, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (st[1] > 0)
+        return fail(h, ADI_ERR_BAD_ARG,
+                    std::string(what) + ": " + std::to_string(st[1]) +
+                        " scanline walks do not end in the reference's float arithmetic (a near-degenerate triangle)");
+    if (st[0] > 0)
+        return fail(h, ADI_ERR_BAD_ARG,
+                    std::string(what) + ": " + std::to_string(st[0]) + " writes fall outside the node grid");
+    return ADI_OK;
+}
+
+} // namespace
+
+adi_status adi_mask_shape3d(adi_handle *h, const float *verts, int nverts, const int *tris, int ntris, double base_T,
+                            int *fill_passes)
+{
+    if (!h || nverts < 0 || ntris < 0 || (nverts > 0 && !verts) || (ntris > 0 && !tris)) return ADI_ERR_BAD_ARG;
+    for (long long q = 0; q < 3ll * ntris; q++)
+        if (tris[q] < 0 || tris[q] >= nverts)
+            return fail(h, ADI_ERR_BAD_ARG, "triangle " + std::to_string(q / 3) + " names a vertex out of range");
+    const long long n = h->n;
+    MaskScratch sc;
+    uint8_t *types = nullptr;
+    float *dv = nullptr;
+    int *dt = nullptr, *st = nullptr;
+    CK(sc.get((void **)&types, n));
+    CK(sc.get((void **)&dv, sizeof(float) * 3 * (size_t)nverts));
+    CK(sc.get((void **)&dt, sizeof(int) * 3 * (size_t)ntris));
+    CK(sc.get((void **)&st, sizeof(int) * 4));
+    CK(cudaMemsetAsync(st, 0, sizeof(int) * 4, h->stream));
+    if (nverts > 0) CK(cudaMemcpyAsync(dv, verts, sizeof(float) * 3 * (size_t)nverts, cudaMemcpyHostToDevice, h->stream));
+    if (ntris > 0) CK(cudaMemcpyAsync(dt, tris, sizeof(int) * 3 * (size_t)ntris, cudaMemcpyHostToDevice, h->stream));
+    if (!h->mask_set) {
+        // a grid that has had no mask: Grid3D::Init's nodes (v = 0, T = 0, no-slip)
+        CK(cudaMemsetAsync(h->d_code, 0, n, h->stream));
+        for (int v = 0; v < 4; v++) CK(cudaMemsetAsync(h->d_nv[v], 0, n * esize(h), h->stream));
+    }
+    int passes = 0;
+    // every pass but the last turns at least one cell, so n + 1 passes always reach the fixed point
+    CK(launch_mask_shape3d(types, h->nx, h->ny, h->nz, dv, nverts, dt, ntris, st, st + 2,
+                           (int)std::min<long long>(n + 1, INT_MAX), &passes, h->stream));
+    if (fill_passes) *fill_passes = passes;
+    adi_status s = mask_status(h, st, "shape rasterisation");
+    if (s != ADI_OK) return s;
+    const float bt = (float)base_T;   // (FTYPE)baseT
+    if (h->prec == ADI_FP64)
+        CK(launch_mask_shape3d_install<double>(types, h->d_code, layer_of<double>(h->d_nv), layer<double>(h, h->cur), n,
+                                               (double)bt, h->stream));
+    else
+        CK(launch_mask_shape3d_install<float>(types, h->d_code, layer_of<float>(h->d_nv), layer<float>(h, h->cur), n, bt,
+                                              h->stream));
+    return finish_device_mask(h);
+}
+
+adi_status adi_mask_sea(adi_handle *h, const float *depth, int depth_nx, int depth_ny, float zmin, double base_T,
+                        const float in_vel[3], double in_T)
+{
+    if (!h || !depth || !in_vel || depth_nx <= 0 || depth_ny <= 0) return ADI_ERR_BAD_ARG;
+    const long long n = h->n;
+    MaskScratch sc;
+    uint8_t *snap = nullptr;
+    float *dd = nullptr;
+    int *st = nullptr;
+    CK(sc.get((void **)&snap, n));
+    CK(sc.get((void **)&dd, sizeof(float) * (size_t)depth_nx * depth_ny));
+    CK(sc.get((void **)&st, sizeof(int) * 4));
+    CK(cudaMemsetAsync(st, 0, sizeof(int) * 4, h->stream));
+    CK(cudaMemcpyAsync(dd, depth, sizeof(float) * (size_t)depth_nx * depth_ny, cudaMemcpyHostToDevice, h->stream));
+    const float v3[3] = {in_vel[0], in_vel[1], in_vel[2]};
+    if (h->prec == ADI_FP64)
+        CK(launch_mask_sea<double>(h->d_code, snap, layer_of<double>(h->d_nv), layer<double>(h, h->cur), h->nx, h->ny,
+                                   h->nz, dd, depth_nx, depth_ny, zmin, (float)base_T, v3, (float)in_T, st, h->stream));
+    else
+        CK(launch_mask_sea<float>(h->d_code, snap, layer_of<float>(h->d_nv), layer<float>(h, h->cur), h->nx, h->ny,
+                                  h->nz, dd, depth_nx, depth_ny, zmin, (float)base_T, v3, (float)in_T, st, h->stream));
+    adi_status s = mask_status(h, st, "sea mask");
+    if (s != ADI_OK) return s;
+    return finish_device_mask(h);
+}
+
+adi_status adi_mask_extrude2d(adi_handle *h, const uint8_t *type2d, const float *vel2d, const float *T2d,
+                              int active_nz, double depth_var, double base_T)
+{
+    if (!h || !type2d || !vel2d || !T2d) return ADI_ERR_BAD_ARG;
+    if (active_nz < 2 || active_nz > h->nz) return fail(h, ADI_ERR_BAD_ARG, "active_nz must lie in [2, nz]");
+    const long long cols = (long long)h->nx * h->ny;
+    for (long long c = 0; c < cols; c++)
+        if (type2d[c] > NODE_VALVE) return fail(h, ADI_ERR_BAD_ARG, "2D node type out of range");
+    MaskScratch sc;
+    uint8_t *t2 = nullptr;
+    float *v2 = nullptr, *T2 = nullptr;
+    int *st = nullptr;
+    CK(sc.get((void **)&t2, cols));
+    CK(sc.get((void **)&v2, sizeof(float) * 2 * cols));
+    CK(sc.get((void **)&T2, sizeof(float) * cols));
+    CK(sc.get((void **)&st, sizeof(int) * 4));
+    CK(cudaMemsetAsync(st, 0, sizeof(int) * 4, h->stream));
+    CK(cudaMemcpyAsync(t2, type2d, cols, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(v2, vel2d, sizeof(float) * 2 * cols, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(T2, T2d, sizeof(float) * cols, cudaMemcpyHostToDevice, h->stream));
+    if (h->prec == ADI_FP64)
+        CK(launch_mask_extrude2d<double>(h->d_code, layer_of<double>(h->d_nv), layer<double>(h, h->cur), h->nx, h->ny,
+                                         h->nz, t2, v2, T2, active_nz, depth_var, (float)base_T, st, h->stream));
+    else
+        CK(launch_mask_extrude2d<float>(h->d_code, layer_of<float>(h->d_nv), layer<float>(h, h->cur), h->nx, h->ny,
+                                        h->nz, t2, v2, T2, active_nz, depth_var, (float)base_T, st, h->stream));
+    adi_status s = mask_status(h, st, "2D extrusion");
+    if (s != ADI_OK) return s;
+    return finish_device_mask(h);
+}
+
+adi_status adi_get_mask(adi_handle *h, uint8_t *type, uint8_t *bc_vel, uint8_t *bc_temp, double *vx, double *vy,
+                        double *vz, double *T)
+{
+    if (!h || !type || !bc_vel || !bc_temp || !vx || !vy || !vz || !T) return ADI_ERR_BAD_ARG;
+    if (!h->mask_set) return fail(h, ADI_ERR_STATE, "the handle has no mask");
+    const long long n = h->n;
+    std::vector<uint8_t> code(n);
+    CK(cudaMemcpyAsync(code.data(), h->d_code, n, cudaMemcpyDeviceToHost, h->stream));
+    double *dst[4] = {vx, vy, vz, T};
+    std::vector<float> tmp(h->prec == ADI_FP64 ? 0 : n);
+    for (int v = 0; v < 4; v++) {
+        if (h->prec == ADI_FP64) {
+            CK(cudaMemcpyAsync(dst[v], h->d_nv[v], n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        } else {
+            CK(cudaMemcpyAsync(tmp.data(), h->d_nv[v], n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            for (long long i = 0; i < n; i++) dst[v][i] = tmp[i];
+        }
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    for (long long i = 0; i < n; i++) {
+        type[i] = code[i] & CODE_TYPE;
+        bc_vel[i] = (code[i] & CODE_VEL_FREE) ? BC_FREE : BC_NOSLIP;
+        bc_temp[i] = (code[i] & CODE_TEMP_FREE) ? BC_FREE : BC_NOSLIP;
+    }
     return ADI_OK;
 }
 

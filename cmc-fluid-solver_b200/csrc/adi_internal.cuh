@@ -239,6 +239,29 @@ template <typename R>
 cudaError_t launch_objective(const DomainView<R> &d, CLayer<R> x, const int lo[3], const int hi[3], Layer<R> cbar,
                              double *psum, int nblocks, double *out, cudaStream_t s);
 
+// ---- mask builders (masks.cu) ----
+// Shape3D: types (n bytes of scratch) <- NODE_IN, triangles rasterised as
+// NODE_BOUND, outside flood-filled as NODE_OUT.  verts: 3 floats per vertex in
+// grid coordinates; tris: 3 vertex indices per triangle (checked by the caller).
+// status[0]: writes outside the grid, status[1]: loops stopped at their bound;
+// changed: one int of scratch; the flood fill stops after max_passes.
+cudaError_t launch_mask_shape3d(uint8_t *types, int nx, int ny, int nz, const float *verts, int nverts,
+                                const int *tris, int ntris, int *status, int *changed, int max_passes,
+                                int *passes_out, cudaStream_t s);
+template <typename R>
+cudaError_t launch_mask_shape3d_install(const uint8_t *types, uint8_t *code, Layer<R> nv, Layer<R> cur, long long n,
+                                        R baseT, cudaStream_t s);
+// SeaNetCDF from a depth map (snap: n bytes of scratch).
+template <typename R>
+cudaError_t launch_mask_sea(uint8_t *code, uint8_t *snap, Layer<R> nv, Layer<R> cur, int nx, int ny, int nz,
+                            const float *depth, int dnx, int dny, float zmin, float baseT, const float in_vel[3],
+                            float in_T, int *status, cudaStream_t s);
+// Shape2D extrusion of a 2D node grid (t2: types, v2: 2 floats, T2: 1 float per cell).
+template <typename R>
+cudaError_t launch_mask_extrude2d(uint8_t *code, Layer<R> nv, Layer<R> cur, int nx, int ny, int nz,
+                                  const uint8_t *t2, const float *v2, const float *T2, int active_nz, double depth_var,
+                                  float baseT, int *status, cudaStream_t s);
+
 constexpr int DIV_BLOCKS = 592;  // 4 x 148 SMs
 
 } // namespace adi

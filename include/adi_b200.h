@@ -123,6 +123,48 @@ adi_status adi_set_mask(adi_handle *h, const uint8_t *node_type, const uint8_t *
                         const uint8_t *bc_temp, const double *vx, const double *vy,
                         const double *vz, const double *T);
 
+/* ---- mask builders on the GPU ------------------------------------------- *
+ * Each builds the node grid on the device and then behaves as adi_set_mask with
+ * that grid (initial state = node values, contract check, segments to be rebuilt).
+ * The arithmetic is the reference's FTYPE = float arithmetic, so the node grid is
+ * bit-identical to the reference's for the same input.  Inputs the reference
+ * cannot finish (a scanline walk that stops advancing on a near-degenerate
+ * triangle, a write outside the node array) return ADI_ERR_BAD_ARG. */
+
+/* Grid3D::Build (Grid3D.cpp:854-898; Prepare3D_Shape :947-964 and
+ * ComputeSubframeInfo :900-945, the choice of frame and its vertices, are the
+ * caller's): all cells NODE_IN; the triangles rasterised as NODE_BOUND
+ * (RasterPolygon :710-788 and RasterLine on the three edges :790-809); NODE_IN
+ * cells connected to cell (0,0,0) become NODE_OUT (FloodFill :811-852);
+ * NODE_IN/NODE_OUT cells get no-slip, v = 0, T = (float)base_T; NODE_BOUND cells
+ * keep their BCs and values (zero, no-slip on a handle that had no mask, as
+ * Grid3D::Init leaves them).
+ * verts: 3 floats per vertex in grid coordinates ((x - bbox.min) / dx, ...,
+ * Grid3D.cpp:420-428); tris: 3 vertex indices per triangle of the inactive shapes.
+ * *fill_passes (may be NULL): flood-fill passes run. */
+adi_status adi_mask_shape3d(adi_handle *h, const float *verts, int nverts, const int *tris,
+                            int ntris, double base_T, int *fill_passes);
+
+/* Grid3D::Prepare3D_NetCDF (Grid3D.cpp:966-1075) from the depth map the NetCDF
+ * file holds (depth[dj + di * depth_ny], negative under water) and bbox.pMin.z
+ * (zmin): water columns NODE_IN, water next to NODE_OUT and NODE_OUT next to the
+ * resulting walls turned into no-slip walls, NODE_IN cells of the faces y = ny-1
+ * and then x = nx-1 into valves with (in_vel, in_T) below the middle of their
+ * water column and (-in_vel, 2 - in_T) above it. */
+adi_status adi_mask_sea(adi_handle *h, const float *depth, int depth_nx, int depth_ny, float zmin,
+                        double base_T, const float in_vel[3], double in_T);
+
+/* Grid3D::Prepare2D (Grid3D.cpp:608-665): the 2D node grid of FluidSolver2D::Grid2D
+ * (types, velocities (2 floats) and T per (i, j), i-major, of the handle's nx x ny)
+ * extruded over active_nz of the nz levels, with a no-slip/free lid at
+ * active_nz - 2 and a curved bottom of relative height depth_var. */
+adi_status adi_mask_extrude2d(adi_handle *h, const uint8_t *type2d, const float *vel2d,
+                              const float *T2d, int active_nz, double depth_var, double base_T);
+
+/* Reads the node grid back (types, BCs, node values in double). */
+adi_status adi_get_mask(adi_handle *h, uint8_t *type, uint8_t *bc_vel, uint8_t *bc_temp,
+                        double *vx, double *vy, double *vz, double *T);
+
 /* Builds the per-direction segment lists on the GPU from the mask, once.
  * Replaces AdiSolver3D::CreateSegments / Grid3D::GenerateListSegments /
  * GenerateGridBoundaries (AdiSolver3D.cpp:553-562, Grid3D.cpp:47-146).
