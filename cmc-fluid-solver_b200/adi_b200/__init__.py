@@ -56,7 +56,8 @@ class AdiSolver3D:
             self.set_stream(stream)
         self._check(self.lib.adi_set_solver(self.h, solver))
         arrs = domain.arrays()
-        self._check(self.lib.adi_set_mask(self.h, *[_ptr(a) for a in arrs]))
+        if arrs is not None:   # a masks.GridBox leaves the mask to a GPU builder
+            self._check(self.lib.adi_set_mask(self.h, *[_ptr(a) for a in arrs]))
         self.stats = None
 
     # -- plumbing --
@@ -80,6 +81,41 @@ class AdiSolver3D:
             self.close()
         except Exception:
             pass
+
+    # -- mask builders (Grid3D::Prepare on the GPU) --
+    def mask_shape3d(self, verts, tris, base_T: float) -> int:
+        """Grid3D::Build of the triangles (grid-coordinate float32 vertices [nv, 3],
+        vertex indices [nt, 3]); returns the flood-fill passes run."""
+        v = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
+        t = np.ascontiguousarray(tris, np.int32).reshape(-1, 3)
+        passes = C.c_int(0)
+        self._check(self.lib.adi_mask_shape3d(self.h, _ptr(v), len(v), _ptr(t), len(t), base_T, C.byref(passes)))
+        self.stats = None
+        return passes.value
+
+    def mask_sea(self, depth, zmin: float, base_T: float, in_vel=(0.0, 0.0, 0.0), in_T: float = 0.0):
+        """Grid3D::Prepare3D_NetCDF from a depth map depth[di, dj] (negative under water)."""
+        dmap = np.ascontiguousarray(depth, np.float32)
+        vel = np.ascontiguousarray(in_vel, np.float32)
+        self._check(self.lib.adi_mask_sea(self.h, _ptr(dmap), dmap.shape[0], dmap.shape[1], float(np.float32(zmin)),
+                                          base_T, _ptr(vel), in_T))
+        self.stats = None
+
+    def mask_extrude2d(self, type2d, vel2d, T2d, active_nz: int, depth_var: float, base_T: float):
+        """Grid3D::Prepare2D: the 2D node grid [nx, ny] (types, velocities [nx, ny, 2], T)
+        extruded in depth."""
+        t = np.ascontiguousarray(type2d, np.uint8)
+        v = np.ascontiguousarray(vel2d, np.float32)
+        T = np.ascontiguousarray(T2d, np.float32)
+        self._check(self.lib.adi_mask_extrude2d(self.h, _ptr(t), _ptr(v), _ptr(T), active_nz, depth_var, base_T))
+        self.stats = None
+
+    def get_mask(self):
+        """(type, bc_vel, bc_temp, vx, vy, vz, T) of the node grid, each [nx, ny, nz]."""
+        shp = tuple(self.shape)
+        out = [np.zeros(shp, np.uint8) for _ in range(3)] + [np.zeros(shp, np.float64) for _ in range(4)]
+        self._check(self.lib.adi_get_mask(self.h, *[_ptr(a) for a in out]))
+        return out
 
     # -- reference surface --
     def CreateSegments(self):

@@ -37,6 +37,7 @@ EXPORTED = [
     "adi2d_set_segments", "adi2d_step_tol",
     "adi2d_update_boundaries", "adi2d_time_step", "adi2d_step", "adi2d_get_state", "adi2d_set_state",
     "adi2d_get_layer", "adi2d_last_error", "adi2d_last_error_string",
+    "adi_mask_shape3d", "adi_mask_sea", "adi_mask_extrude2d", "adi_get_mask",
 ]
 
 K_NUM = 7
@@ -96,6 +97,10 @@ def load() -> C.CDLL:
         "adi_set_stream": [vp, vp],
         "adi_set_solver": [vp, i],
         "adi_set_mask": [vp] + [vp] * 7,
+        "adi_mask_shape3d": [vp, vp, i, vp, i, d, C.POINTER(i)],
+        "adi_mask_sea": [vp, vp, i, i, C.c_float, d, vp, d],
+        "adi_mask_extrude2d": [vp, vp, vp, vp, i, d, d],
+        "adi_get_mask": [vp] + [vp] * 7,
         "adi_build_segments": [vp, C.POINTER(SegStats)],
         "adi_get_segments": [vp, i, vp, C.c_int64, C.POINTER(C.c_int64)],
         "adi_update_boundaries": [vp],

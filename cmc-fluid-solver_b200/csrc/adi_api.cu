@@ -1021,23 +1021,20 @@ struct MaskScratch {
 };
 
 // What adi_set_mask derives on the host from a mask, for a mask a device builder
-// wrote into d_code / d_nv (and the initial state into cur).
-adi_status finish_device_mask(adi_handle *h)
+// wrote into d_code / d_nv (and the initial state into cur): the contract check
+// (the same rules and the same first failing cell as check_contract) and the
+// NODE_IN count, both computed on the device.
+adi_status finish_device_mask(adi_handle *h, unsigned long long *d_census)
 {
-    const long long n = h->n;
-    std::vector<uint8_t> code(n), t(n), bv(n), bt(n);
-    CK(cudaMemcpyAsync(code.data(), h->d_code, n, cudaMemcpyDeviceToHost, h->stream));
+    CK(launch_mask_census(h->d_code, h->nx, h->ny, h->nz, d_census, h->stream));
+    unsigned long long census[2];
+    CK(cudaMemcpyAsync(census, d_census, sizeof census, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    long long nin = 0;
-    for (long long i = 0; i < n; i++) {
-        t[i] = code[i] & CODE_TYPE;
-        bv[i] = (code[i] & CODE_VEL_FREE) ? BC_FREE : BC_NOSLIP;
-        bt[i] = (code[i] & CODE_TEMP_FREE) ? BC_FREE : BC_NOSLIP;
-        nin += t[i] == NODE_IN;
-    }
-    h->contract_msg = check_contract(h, t.data(), bv.data(), bt.data());
+    static const char *const rules[4] = {"", "NODE_IN cell on the outer frame", "NODE_IN cell next to a NODE_OUT cell",
+                                         "BC_FREE cell shared by two segments of one line"};
+    h->contract_msg = census[0] == ~0ull ? std::string() : std::string(rules[census[0] & 3]);
     h->contract_ok = h->contract_msg.empty();
-    h->num_in = nin;
+    h->num_in = (long long)census[1];
     h->mask_set = true;
     h->segs_built = false;
     invalidate_graphs(h);
@@ -1078,8 +1075,8 @@ adi_status adi_mask_shape3d(adi_handle *h, const float *verts, int nverts, const
     CK(sc.get((void **)&types, n));
     CK(sc.get((void **)&dv, sizeof(float) * 3 * (size_t)nverts));
     CK(sc.get((void **)&dt, sizeof(int) * 3 * (size_t)ntris));
-    CK(sc.get((void **)&st, sizeof(int) * 4));
-    CK(cudaMemsetAsync(st, 0, sizeof(int) * 4, h->stream));
+    CK(sc.get((void **)&st, sizeof(int) * 8));   // [0..1] status, [2] flood flag, [4..7] census
+    CK(cudaMemsetAsync(st, 0, sizeof(int) * 8, h->stream));
     if (nverts > 0) CK(cudaMemcpyAsync(dv, verts, sizeof(float) * 3 * (size_t)nverts, cudaMemcpyHostToDevice, h->stream));
     if (ntris > 0) CK(cudaMemcpyAsync(dt, tris, sizeof(int) * 3 * (size_t)ntris, cudaMemcpyHostToDevice, h->stream));
     if (!h->mask_set) {
@@ -1101,7 +1098,7 @@ adi_status adi_mask_shape3d(adi_handle *h, const float *verts, int nverts, const
     else
         CK(launch_mask_shape3d_install<float>(types, h->d_code, layer_of<float>(h->d_nv), layer<float>(h, h->cur), n, bt,
                                               h->stream));
-    return finish_device_mask(h);
+    return finish_device_mask(h, (unsigned long long *)(st + 4));
 }
 
 adi_status adi_mask_sea(adi_handle *h, const float *depth, int depth_nx, int depth_ny, float zmin, double base_T,
@@ -1115,8 +1112,8 @@ adi_status adi_mask_sea(adi_handle *h, const float *depth, int depth_nx, int dep
     int *st = nullptr;
     CK(sc.get((void **)&snap, n));
     CK(sc.get((void **)&dd, sizeof(float) * (size_t)depth_nx * depth_ny));
-    CK(sc.get((void **)&st, sizeof(int) * 4));
-    CK(cudaMemsetAsync(st, 0, sizeof(int) * 4, h->stream));
+    CK(sc.get((void **)&st, sizeof(int) * 8));   // [0..1] status, [2] flood flag, [4..7] census
+    CK(cudaMemsetAsync(st, 0, sizeof(int) * 8, h->stream));
     CK(cudaMemcpyAsync(dd, depth, sizeof(float) * (size_t)depth_nx * depth_ny, cudaMemcpyHostToDevice, h->stream));
     const float v3[3] = {in_vel[0], in_vel[1], in_vel[2]};
     if (h->prec == ADI_FP64)
@@ -1127,7 +1124,7 @@ adi_status adi_mask_sea(adi_handle *h, const float *depth, int depth_nx, int dep
                                   h->nz, dd, depth_nx, depth_ny, zmin, (float)base_T, v3, (float)in_T, st, h->stream));
     adi_status s = mask_status(h, st, "sea mask");
     if (s != ADI_OK) return s;
-    return finish_device_mask(h);
+    return finish_device_mask(h, (unsigned long long *)(st + 4));
 }
 
 adi_status adi_mask_extrude2d(adi_handle *h, const uint8_t *type2d, const float *vel2d, const float *T2d,
@@ -1145,8 +1142,8 @@ adi_status adi_mask_extrude2d(adi_handle *h, const uint8_t *type2d, const float 
     CK(sc.get((void **)&t2, cols));
     CK(sc.get((void **)&v2, sizeof(float) * 2 * cols));
     CK(sc.get((void **)&T2, sizeof(float) * cols));
-    CK(sc.get((void **)&st, sizeof(int) * 4));
-    CK(cudaMemsetAsync(st, 0, sizeof(int) * 4, h->stream));
+    CK(sc.get((void **)&st, sizeof(int) * 8));   // [0..1] status, [2] flood flag, [4..7] census
+    CK(cudaMemsetAsync(st, 0, sizeof(int) * 8, h->stream));
     CK(cudaMemcpyAsync(t2, type2d, cols, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(v2, vel2d, sizeof(float) * 2 * cols, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(T2, T2d, sizeof(float) * cols, cudaMemcpyHostToDevice, h->stream));
@@ -1158,7 +1155,7 @@ adi_status adi_mask_extrude2d(adi_handle *h, const uint8_t *type2d, const float 
                                         h->nz, t2, v2, T2, active_nz, depth_var, (float)base_T, st, h->stream));
     adi_status s = mask_status(h, st, "2D extrusion");
     if (s != ADI_OK) return s;
-    return finish_device_mask(h);
+    return finish_device_mask(h, (unsigned long long *)(st + 4));
 }
 
 adi_status adi_get_mask(adi_handle *h, uint8_t *type, uint8_t *bc_vel, uint8_t *bc_temp, double *vx, double *vy,

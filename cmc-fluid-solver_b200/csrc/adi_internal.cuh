@@ -262,6 +262,13 @@ cudaError_t launch_mask_extrude2d(uint8_t *code, Layer<R> nv, Layer<R> cur, int 
                                   const uint8_t *t2, const float *v2, const float *T2, int active_nz, double depth_var,
                                   float baseT, int *status, cudaStream_t s);
 
+// Solver contract and NODE_IN count of a node grid on the device: out2[0] = min
+// over cells breaking the contract of (index << 2 | rule), rule 1: NODE_IN on the
+// frame, 2: NODE_IN next to NODE_OUT, 3: BC_FREE cell between two fluid runs
+// (~0 if none); out2[1] = NODE_IN cells.  The caller synchronises before reading.
+cudaError_t launch_mask_census(const uint8_t *code, int nx, int ny, int nz, unsigned long long *out2,
+                               cudaStream_t s);
+
 constexpr int DIV_BLOCKS = 592;  // 4 x 148 SMs
 
 } // namespace adi

@@ -425,7 +425,7 @@ __global__ void sea_face_kernel(uint8_t *code, Layer<R> nv, int nx, int ny, int 
 // Shape2D extrusion (Grid3D::Prepare2D, Grid3D.cpp:608-665), one thread per
 // column: the column is cleared (memset: NODE_IN, no-slip, zeros) and written in
 // the reference's order.  The host checks 2 <= active_nz <= nz; a bottom that
-// would reach past the column is counted in the status word and clipped.
+// would reach outside the column is counted in the status word and clipped.
 // ---------------------------------------------------------------------------
 template <typename R>
 __device__ __forceinline__ void set_full(uint8_t *code, Layer<R> nv, long long c, uint8_t type, int bcv, int bct,
@@ -462,9 +462,9 @@ __global__ void extrude2d_kernel(uint8_t *code, Layer<R> nv, Layer<R> cur, int n
         const double y = __dadd_rn(-1.0, __ddiv_rn(__dmul_rn(2.0, (double)j), (double)ny));
         const double z = __dsub_rn(1.0, __dmul_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), 0.5));
         int bottom = 1 + to_int(__dmul_rn(__dmul_rn(depth_var, z), (double)height));
-        if (bottom > nz - 1) {   // the reference would write into the next columns
+        if (bottom > nz - 1 || bottom < -1) {   // the reference would write into a neighbouring column
             atomicAdd(&status[ST_OUTSIDE], 1);
-            bottom = nz - 1;
+            bottom = bottom < -1 ? -1 : nz - 1;
         }
         code[base] = (uint8_t)(NODE_OUT | (code[base] & ~CODE_TYPE));
         for (int k = 1; k <= bottom; k++)
@@ -494,6 +494,49 @@ __global__ void copy_state_kernel(Layer<R> nv, Layer<R> cur, long long n)
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
 #pragma unroll
         for (int v = 0; v < 4; v++) cur.f[v][c] = nv.f[v][c];
+}
+
+// The solver contract and the NODE_IN count of a node grid, on the device: the
+// same tests as the host's check of an uploaded mask, in the same order, so the
+// first failing cell in linear order (and the rule it fails) is the one the host
+// check reports.  first_bad: min over failing cells of (index << 2 | rule).
+__global__ void mask_census_kernel(const uint8_t *__restrict__ code, int nx, int ny, int nz,
+                                   unsigned long long *first_bad, unsigned long long *num_in)
+{
+    const long long n = (long long)nx * ny * nz;
+    const long long sx = (long long)ny * nz, sy = nz;
+    unsigned long long cnt = 0, bad = ~0ull;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(c / sx), j = (int)((c / sy) % ny), k = (int)(c % nz);
+        const bool frame = i == 0 || j == 0 || k == 0 || i == nx - 1 || j == ny - 1 || k == nz - 1;
+        const uint8_t t = code[c] & CODE_TYPE;
+        auto ty = [&](long long q) { return code[q] & CODE_TYPE; };
+        int rule = 0;
+        if (t == NODE_IN) {
+            cnt++;
+            if (frame) rule = 1;
+            else if (ty(c - sx) == NODE_OUT || ty(c + sx) == NODE_OUT || ty(c - sy) == NODE_OUT ||
+                     ty(c + sy) == NODE_OUT || ty(c - 1) == NODE_OUT || ty(c + 1) == NODE_OUT)
+                rule = 2;
+        } else if (!frame && (code[c] & (CODE_VEL_FREE | CODE_TEMP_FREE))) {
+            if ((ty(c - sx) == NODE_IN && ty(c + sx) == NODE_IN) || (ty(c - sy) == NODE_IN && ty(c + sy) == NODE_IN) ||
+                (ty(c - 1) == NODE_IN && ty(c + 1) == NODE_IN))
+                rule = 3;
+        }
+        if (rule) {
+            const unsigned long long key = ((unsigned long long)c << 2) | (unsigned long long)rule;
+            if (key < bad) bad = key;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+        const unsigned long long b = __shfl_down_sync(0xffffffffu, bad, o);
+        if (b < bad) bad = b;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (cnt) atomicAdd(num_in, cnt);
+        if (bad != ~0ull) atomicMin(first_bad, bad);
+    }
 }
 
 int grid_for(long long n, int threads)
@@ -575,6 +618,17 @@ cudaError_t launch_mask_extrude2d(uint8_t *code, Layer<R> nv, Layer<R> cur, int 
     const long long cols = (long long)nx * ny;
     extrude2d_kernel<R><<<(unsigned)((cols + 127) / 128), 128, 0, s>>>(code, nv, cur, nx, ny, nz, t2, v2, T2, active_nz,
                                                                        depth_var, baseT, status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mask_census(const uint8_t *code, int nx, int ny, int nz, unsigned long long *out2,
+                               cudaStream_t s)
+{
+    const unsigned long long init[2] = {~0ull, 0ull};
+    cudaError_t e = cudaMemcpyAsync(out2, init, sizeof init, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return e;
+    const long long n = (long long)nx * ny * nz;
+    mask_census_kernel<<<grid_for(n, 256), 256, 0, s>>>(code, nx, ny, nz, out2, out2 + 1);
     return cudaGetLastError();
 }
 

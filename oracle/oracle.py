@@ -56,6 +56,18 @@ def _load_ref():
         lib.ref_div_error.restype = C.c_double
         lib.ref_div_error.argtypes = [C.c_void_p]
         lib.ref_destroy.argtypes = [C.c_void_p]
+        vp, i, d = C.c_void_p, C.c_int, C.c_double
+        lib.ref_shape3d_load.restype = vp
+        lib.ref_shape3d_load.argtypes = [C.c_char_p, d, d, d, d, _i32p]
+        lib.ref_shape2d_load.restype = vp
+        lib.ref_shape2d_load.argtypes = [C.c_char_p, d, d, d, d, d, d, _i32p]
+        lib.ref_sea_create.restype = vp
+        lib.ref_sea_create.argtypes = [i, i, i, _f32p, i, i, C.c_float, d, _f32p, d]
+        lib.ref_mask_prepare.argtypes = [vp, d]
+        lib.ref_mask_nodes.argtypes = [vp] + [_u8p] * 3 + [_f32p] * 4
+        lib.ref_shape3d_frame.argtypes = [vp, i, vp, vp, C.POINTER(i)]
+        lib.ref_shape2d_grid.argtypes = [vp, _u8p, _f32p, _f32p]
+        lib.ref_mask_destroy.argtypes = [vp]
         _ref = lib
     return _ref
 
@@ -370,6 +382,76 @@ class Ref2D:
     def close(self):
         if self.h:
             self.lib.ref2d_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class RefMask:
+    """A reference Grid3D built by its own loaders and Prepare (Shape3D from a file,
+    Shape2D from a file, SeaNetCDF from a depth map in memory)."""
+
+    def __init__(self, handle, dims, lib, active_nz=None):
+        if not handle:
+            raise RuntimeError("the reference could not load the grid")
+        self.h, self.dims, self.lib, self.active_nz = handle, tuple(dims), lib, active_nz
+
+    @classmethod
+    def shape3d(cls, path, dx, dy, dz, base_T):
+        lib = _load_ref()
+        dims = np.zeros(4, np.int32)
+        return cls(lib.ref_shape3d_load(path.encode(), dx, dy, dz, base_T, dims), dims[:3], lib)
+
+    @classmethod
+    def shape2d(cls, path, dx, dy, dz, depth, depth_var, base_T):
+        lib = _load_ref()
+        dims = np.zeros(4, np.int32)
+        h = lib.ref_shape2d_load(path.encode(), dx, dy, dz, depth, depth_var, base_T, dims)
+        return cls(h, dims[:3], lib, int(dims[3]))
+
+    @classmethod
+    def sea(cls, dims, depth, zmin, base_T, in_vel, in_T):
+        lib = _load_ref()
+        dmap = np.ascontiguousarray(depth, np.float32)
+        vel = np.ascontiguousarray(in_vel, np.float32)
+        h = lib.ref_sea_create(dims[0], dims[1], dims[2], dmap, dmap.shape[0], dmap.shape[1], zmin, base_T, vel,
+                               in_T)
+        return cls(h, dims, lib)
+
+    def prepare(self, time=0.0):
+        if self.lib.ref_mask_prepare(self.h, time) != 0:
+            raise RuntimeError("Grid3D::Prepare threw")
+
+    def nodes(self):
+        out = [np.zeros(self.dims, np.uint8) for _ in range(3)] + [np.zeros(self.dims, np.float32) for _ in range(4)]
+        self.lib.ref_mask_nodes(self.h, *out)
+        return out
+
+    def frame(self, f):
+        nt = C.c_int(0)
+        nv = self.lib.ref_shape3d_frame(self.h, f, None, None, C.byref(nt))
+        if nv < 0:
+            raise IndexError(f)
+        verts = np.zeros((nv, 3), np.float32)
+        tris = np.zeros((nt.value, 3), np.int32)
+        self.lib.ref_shape3d_frame(self.h, f, verts.ctypes.data, tris.ctypes.data, C.byref(nt))
+        return verts, tris
+
+    def grid2d(self):
+        nx, ny = self.dims[0], self.dims[1]
+        t = np.zeros((nx, ny), np.uint8)
+        v = np.zeros((nx, ny, 2), np.float32)
+        T = np.zeros((nx, ny), np.float32)
+        self.lib.ref_shape2d_grid(self.h, t, v, T)
+        return t, v, T
+
+    def close(self):
+        if self.h:
+            self.lib.ref_mask_destroy(self.h)
             self.h = None
 
     def __del__(self):

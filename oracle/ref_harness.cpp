@@ -85,6 +85,32 @@ struct HarnessGrid : public Grid3D
 	Node *Nodes() { return nodes; }
 };
 
+// A Grid3D built by the reference's own loaders and mask builders (Shape3D,
+// SeaNetCDF, Shape2D), with read access to what they produced.
+struct MaskGrid : public Grid3D
+{
+	// 3D shapes (Grid3D.h:106) or a 2D shape extruded in depth (Grid3D.h:105)
+	MaskGrid(double _dx, double _dy, double _dz, double _baseT, bool netcdf)
+		: Grid3D(_dx, _dy, _dz, _baseT, CPU, netcdf, EVEN_X) { }
+	MaskGrid(double _dx, double _dy, double _dz, double _depth, double _depth_var, double _baseT)
+		: Grid3D(_dx, _dy, _dz, _depth, _depth_var, _baseT, CPU, false, EVEN_X) { }
+	Node *Nodes() { return nodes; }
+	int NumFrames() { return num_frames; }
+	FrameInfo3D *Frames() { return frames; }
+	int ActiveDimz() { return active_dimz; }
+	BBox3D &Box() { return bbox; }
+	// the state LoadNetCDF leaves (Grid3D.cpp:437-486), from a depth map in memory
+	void SetSea(int nx, int ny, int nz, const float *depth, int dnx, int dny, float zmin)
+	{
+		dimx = nx; dimy = ny; dimz = nz;
+		nodes = new Node[(size_t)nx * ny * nz];
+		depthInfo = new DepthInfo3D(dnx, dny);
+		memcpy(depthInfo->depth, depth, sizeof(float) * (size_t)dnx * dny);
+		bbox.pMin.z = zmin;
+		num_frames = 1;
+	}
+};
+
 struct HarnessSolver : public AdiSolver3D
 {
 	TimeLayer3D *Cur() { return cur; }
@@ -311,5 +337,101 @@ void ref_destroy(void *vh)
 	delete h->grid;
 	delete h;
 }
+
+// ---- mask builders ----------------------------------------------------------
+
+// Grid3D(dx, dy, dz, baseT) + LoadFromFile (Load3DShape, Grid3D.cpp:371-435) of a
+// Shape3D text file; dims_out receives dimx, dimy, dimz.
+void *ref_shape3d_load(const char *path, double dx, double dy, double dz, double baseT, int *dims_out)
+{
+	PARAplan::Instance()->init(CPU);
+	MaskGrid *g = new MaskGrid(dx, dy, dz, baseT, false);
+	if (!g->LoadFromFile(const_cast<char *>(path), false)) { delete g; return NULL; }
+	dims_out[0] = g->dimx; dims_out[1] = g->dimy; dims_out[2] = g->dimz;
+	return g;
+}
+
+// Grid3D(dx, dy, dz, depth, depth_var, baseT) + LoadFromFile of a Shape2D file
+// (Grid3D.cpp:497-509); dims_out: dimx, dimy, dimz, active_dimz.
+void *ref_shape2d_load(const char *path, double dx, double dy, double dz, double depth, double depth_var,
+                       double baseT, int *dims_out)
+{
+	PARAplan::Instance()->init(CPU);
+	MaskGrid *g = new MaskGrid(dx, dy, dz, depth, depth_var, baseT);
+	if (!g->LoadFromFile(const_cast<char *>(path), false)) { delete g; return NULL; }
+	dims_out[0] = g->dimx; dims_out[1] = g->dimy; dims_out[2] = g->dimz; dims_out[3] = g->ActiveDimz();
+	return g;
+}
+
+// The state LoadNetCDF leaves, from a depth map in memory, and the inflow of
+// SetBoundParams (Grid3D.cpp:316-320).
+void *ref_sea_create(int nx, int ny, int nz, const float *depth, int dnx, int dny, float zmin, double baseT,
+                     const float *in_vel, double in_T)
+{
+	PARAplan::Instance()->init(CPU);
+	MaskGrid *g = new MaskGrid(1.0, 1.0, 1.0, baseT, true);
+	g->SetSea(nx, ny, nz, depth, dnx, dny, zmin);
+	g->SetBoundParams(Vec3D(in_vel[0], in_vel[1], in_vel[2]), in_T);
+	return g;
+}
+
+// Grid3D::Prepare(time) on the CPU backend.
+int ref_mask_prepare(void *vg, double time)
+{
+	try { ((MaskGrid *)vg)->Prepare(time); }
+	catch (std::exception &) { return -1; }
+	return 0;
+}
+
+// The node array as SoA.
+void ref_mask_nodes(void *vg, unsigned char *type, unsigned char *bc_vel, unsigned char *bc_temp, float *vx,
+                    float *vy, float *vz, float *T)
+{
+	MaskGrid *g = (MaskGrid *)vg;
+	const Node *nd = g->Nodes();
+	size_t n = (size_t)g->dimx * g->dimy * g->dimz;
+	for (size_t i = 0; i < n; i++)
+	{
+		type[i] = (unsigned char)nd[i].type;
+		bc_vel[i] = (unsigned char)nd[i].bc_vel;
+		bc_temp[i] = (unsigned char)nd[i].bc_temp;
+		vx[i] = nd[i].v.x; vy[i] = nd[i].v.y; vz[i] = nd[i].v.z; T[i] = nd[i].T;
+	}
+}
+
+// Vertices (grid coordinates, 3 floats each) and triangles of shape 0 of frame f
+// as Load3DShape left them; returns the vertex count, *ntris the triangle count.
+int ref_shape3d_frame(void *vg, int f, float *verts, int *tris, int *ntris)
+{
+	MaskGrid *g = (MaskGrid *)vg;
+	if (f < 0 || f >= g->NumFrames()) return -1;
+	Shape3D &sh = g->Frames()[f].Shapes[0];
+	if (verts)
+		for (int k = 0; k < sh.NumVertices; k++)
+		{
+			verts[3 * k] = sh.Vertices[k].x; verts[3 * k + 1] = sh.Vertices[k].y; verts[3 * k + 2] = sh.Vertices[k].z;
+		}
+	if (tris)
+		for (int k = 0; k < 3 * sh.NumIndices; k++) tris[k] = sh.Indices[k];
+	*ntris = sh.NumIndices;
+	return sh.NumVertices;
+}
+
+// The 2D helper grid after Prepare (types, velocity and T per (i, j), i-major).
+void ref_shape2d_grid(void *vg, unsigned char *type, float *vel2, float *T)
+{
+	MaskGrid *g = (MaskGrid *)vg;
+	FluidSolver2D::Grid2D *g2 = g->GetGrid2D();
+	for (int i = 0; i < g2->dimx; i++)
+		for (int j = 0; j < g2->dimy; j++)
+		{
+			size_t c = (size_t)i * g2->dimy + j;
+			FluidSolver2D::CondData2D d = g2->GetData(i, j);
+			type[c] = (unsigned char)g2->GetType(i, j);
+			vel2[2 * c] = d.vel.x; vel2[2 * c + 1] = d.vel.y; T[c] = d.T;
+		}
+}
+
+void ref_mask_destroy(void *vg) { delete (MaskGrid *)vg; }
 
 } // extern "C"

@@ -1,0 +1,94 @@
+"""Generates tests/golden/masks.npz: node grids built by the reference's own
+Grid3D loaders and mask builders (oracle/_ref/libref3d.so, compiled from the
+reference's sources by oracle/Makefile) on the synthetic inputs of
+tests/mask_shapes.py, together with the inputs the GPU builders take.
+
+Run from the repository root on a machine with the reference checkout:
+    python tests/golden/make_masks.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+sys.path.insert(0, os.path.join(ROOT, "cmc-fluid-solver_b200"))
+
+import mask_shapes as ms  # noqa: E402
+from adi_b200 import masks  # noqa: E402
+from oracle.oracle import RefMask  # noqa: E402
+
+OUT = os.path.join(ROOT, "tests", "golden", "masks.npz")
+
+# (name, frames, dx, time)
+SHAPE3D = [
+    ("tetra", [ms.tetra() + (None,)], 0.01, 0.0),
+    ("box_frame", [ms.box() + (None,)], 0.02, 0.0),
+    ("box", [ms.box() + (None,)], 0.01, 0.0),
+    ("sphere", [ms.uv_sphere() + (None,)], 0.01, 0.0),
+    ("moving", [ms.tetra() + (None,), (ms.moved(ms.tetra()[0]), ms.tetra()[1], None)], 0.01, 0.005),
+    ("leaky", [ms.box(drop_faces=1) + (None,)], 0.01, 0.0),
+]
+BASE_T = 1.0
+
+
+def nodes_dict(prefix, r):
+    t, bv, bt, vx, vy, vz, T = r.nodes()
+    return {f"{prefix}_type": t, f"{prefix}_bcv": bv, f"{prefix}_bct": bt,
+            f"{prefix}_val": np.stack([vx, vy, vz, T])}
+
+
+def main():
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for name, frames, dx, time in SHAPE3D:
+            path = os.path.join(tmp, name + ".txt")
+            ms.write_shape3d(path, frames)
+            r = RefMask.shape3d(path, dx, dx, dx, BASE_T)
+            sf = masks.load_shape3d(path, dx, dx, dx)
+            assert tuple(int(d) for d in r.dims) == sf.dims
+            verts, tris = sf.subframe(time)
+            r.prepare(time)
+            out.update(nodes_dict("s3_" + name, r))
+            out[f"s3_{name}_verts"] = verts
+            out[f"s3_{name}_tris"] = tris
+            out[f"s3_{name}_dims"] = np.array(sf.dims, np.int32)
+            r.close()
+
+        for name, dvar in (("ch_bump", 0.4), ("ch_flat", 0.0)):
+            path = os.path.join(tmp, "channel2d.txt")
+            ms.write_shape2d(path, ms.channel2d())
+            r = RefMask.shape2d(path, 0.01, 0.01, 0.02, 0.3, dvar, BASE_T)
+            r.prepare(0.0)
+            t2, v2, T2 = r.grid2d()
+            out.update(nodes_dict("e2_" + name, r))
+            out[f"e2_{name}_t2"], out[f"e2_{name}_v2"], out[f"e2_{name}_T2"] = t2, v2, T2
+            out[f"e2_{name}_dims"] = np.array(list(r.dims) + [r.active_nz], np.int32)
+            out[f"e2_{name}_depth_var"] = np.array(dvar)
+            r.close()
+
+    for name, open_far, vel, tin in (("basin", False, (0.0, 0.0, 0.0), 1.0), ("open", True, (0.1, -0.2, 0.05), 1.5)):
+        lats = np.linspace(64.0, 67.0, 64)
+        lons = np.linspace(32.0, 37.0, 50)
+        dep = ms.depth_map(64, 50, open_far=open_far)
+        dims, zmin = masks.sea_geometry(lats, lons, dep, 0.05, 0.1, 2.0)
+        r = RefMask.sea(dims, dep, zmin, BASE_T, vel, tin)
+        r.prepare(0.0)
+        out.update(nodes_dict("sea_" + name, r))
+        out[f"sea_{name}_depth"] = dep
+        out[f"sea_{name}_dims"] = np.array(dims, np.int32)
+        out[f"sea_{name}_zmin"] = np.array(zmin, np.float32)
+        out[f"sea_{name}_vel"] = np.array(vel, np.float32)
+        out[f"sea_{name}_tin"] = np.array(tin)
+        r.close()
+    np.savez_compressed(OUT, **out)
+    print(OUT, os.path.getsize(OUT), "bytes")
+
+
+if __name__ == "__main__":
+    main()
