@@ -105,6 +105,11 @@ CONFIGS = {
     "adjoint64": dict(make=_spheres64_adj, adjoint=True, Re=200.0, Pr=0.72, lam=1.4, dt=5e-4, ng=4, nl=2,
                       n_steps=8, ckpt=4, box=((40, 16, 16), (56, 48, 48)), near_box=((2, 16, 16), (18, 48, 48)),
                       desc="small adjoint for profiling: 64^3 FP32, 10 spheres, 8 steps checkpointed every 4"),
+    "masks262": dict(make=None, masks=True, dx=0.0029,
+                     desc="mask builders: Grid3D::Build of a closed triangle mesh (jittered latitude-longitude "
+                          "sphere, 1656 triangles, radius 0.36) rasterised and flood-filled on a 262x262x264 "
+                          "grid (dx 0.0029, 18.1 M cells), beside Prepare3D_NetCDF of a 256x200 depth map on a "
+                          "251x201x109 grid"),
     "spheres64": dict(make=_spheres64, Re=200.0, Pr=0.72, lam=1.4, dt=5e-4, ng=4, nl=2,
                       desc="small case for profiling: 64^3 FP32, 10 spheres, Re=200, dt=5e-4, "
                            "num_global=4, num_local=2"),
@@ -310,6 +315,32 @@ def run_reference(args):
             "cpu_baseline": {"value": value, "unit": METRIC, "cores": 1, "kind": "reference",
                              "sample": f"{done} steps ({el:.1f} s), the reference 2D solver (single-threaded)"},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }), flush=True)
+        return 0
+    if cfg.get("masks"):
+        from adi_b200 import masks, shapes
+        import oracle as O
+        dx = cfg["dx"]
+        path = os.path.join(tempfile.mkdtemp(), "sphere.txt")
+        shapes.write_shape3d(path, [shapes.uv_sphere(n_lat=24, n_lon=36) + (None,)])
+        n = int(np.prod(masks.load_shape3d(path, dx, dx, dx).dims))
+        r = O.RefMask.shape3d(path, dx, dx, dx, 1.0)
+        with stdout_to_stderr():
+            t0 = time.perf_counter()
+            done = 0
+            while done < args.steps and time.perf_counter() - t0 < args.ref_budget:
+                r.prepare(0.0)
+                done += 1
+            el = time.perf_counter() - t0
+        value = n * done / el
+        print(json.dumps({
+            "impl": "reference", "metric": "cells/s", "value": value, "unit": "cells/s", "n_gpus": world,
+            "steps": done, "warmup": 0, "ms_per_step": 1e3 * el / done, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{args.config}: {cfg['desc']}", "cells": n},
+            "cpu_baseline": {"value": value, "unit": "cells/s", "cores": 1, "kind": "reference",
+                             "sample": f"{done} full Grid3D::Prepare builds ({el:.1f} s), single-threaded as written"},
+            "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }), flush=True)
         return 0
     if cfg.get("batch"):
@@ -998,6 +1029,114 @@ def run_2d(args):
     return 0
 
 
+def run_masks(args):
+    """Mask builders: the whole Grid3D::Build of a triangle mesh per step."""
+    import tempfile
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    import adi_b200
+    from adi_b200 import masks
+    from adi_b200 import shapes as ms
+    cfg = CONFIGS[args.config]
+    dx = cfg["dx"]
+    tmp = tempfile.mkdtemp()
+    path = os.path.join(tmp, "sphere.txt")
+    ms.write_shape3d(path, [ms.uv_sphere(n_lat=24, n_lon=36) + (None,)])
+    sf = masks.load_shape3d(path, dx, dx, dx)
+    verts, tris = sf.subframe(0.0)
+    n = int(np.prod(sf.dims))
+    stream = torch.cuda.current_stream()
+    s = adi_b200.AdiSolver3D(masks.GridBox(*sf.dims, dx, dx, dx), stream=stream.cuda_stream)
+    for _ in range(args.warmup):
+        s.mask_shape3d(verts, tris, 1.0)
+    steps = args.steps
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    clocks = ClockSampler(local)
+    torch.cuda.synchronize()
+    clocks.start()
+    total_ms, passes = 0.0, 0
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        passes = s.mask_shape3d(verts, tris, 1.0)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        total_ms += e0.elapsed_time(e1)
+    clk = clocks.stop()
+    value = world * n * steps / (total_ms / 1e3)
+    # end to end: the build from host geometry plus the node grid read back to the host
+    e2e_steps = max(1, min(steps, 5))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        s.mask_shape3d(verts, tris, 1.0)
+        got = s.get_mask()
+    e2e_s = time.perf_counter() - t0
+    # sea depth map
+    lats, lons = np.linspace(64.0, 67.0, 256), np.linspace(32.0, 37.0, 200)
+    dep = ms.depth_map(256, 200, open_far=True)
+    sdims, zmin = masks.sea_geometry(lats, lons, dep, 0.012, 0.025, 0.5)
+    sea = adi_b200.AdiSolver3D(masks.GridBox(*sdims, 0.012, 0.025, 0.5), stream=stream.cuda_stream)
+    for _ in range(args.warmup):
+        sea.mask_sea(dep, zmin, 1.0, (0.1, -0.2, 0.05), 1.5)
+    torch.cuda.synchronize()
+    se0, se1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    se0.record(stream)
+    for _ in range(steps):
+        sea.mask_sea(dep, zmin, 1.0, (0.1, -0.2, 0.05), 1.5)
+    se1.record(stream)
+    torch.cuda.synchronize()
+    sea_ms = se0.elapsed_time(se1) / steps
+    # algorithmic bytes of a build: the node grid written once (code byte, four node
+    # values, the four fields of the initial state)
+    es = 4
+    alg = n * (1 + 8 * es)
+    achieved = alg / (total_ms / steps / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    line = {
+        "metric": "cells/s", "value": value, "unit": "cells/s", "n_gpus": world, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{args.config}: {cfg['desc']}", "cells": n, "triangles": int(len(tris)),
+                   "flood_fill_passes": passes, "l2": "256 MiB written between builds (L2 flushed)"},
+        "e2e": {"value": n * e2e_steps / e2e_s, "unit": "cells/s", "h2d_bytes_per_step": int(verts.nbytes + tris.nbytes),
+                "d2h_bytes_per_step": int(sum(a.nbytes for a in got)), "steps": e2e_steps,
+                "note": "adi_mask_shape3d from host vertices, then adi_get_mask of the whole node grid "
+                        "(types, BCs, node values as doubles)"},
+        "gpu_launches": None,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if peak else None, "traffic": None, "kernel": "whole build",
+                     "peak_source": peak_kind,
+                     "note": "one step = one host-driven build: rasterisation, flood-fill passes with a host "
+                             "read of the change flag after each, install and contract census; latency-bound"},
+        "sea": {"cells": int(np.prod(sdims)), "ms_per_build": sea_ms,
+                "value": float(np.prod(sdims)) / (sea_ms / 1e3), "unit": "cells/s"},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle as O
+        if not O.have_ref():
+            O.build()
+        r = O.RefMask.shape3d(path, dx, dx, dx, 1.0)
+        with stdout_to_stderr():
+            t0 = time.perf_counter()
+            done = 0
+            while done < 3 and time.perf_counter() - t0 < args.cpu_budget:
+                r.prepare(0.0)
+                done += 1
+            el = time.perf_counter() - t0
+        same = bool(np.array_equal(r.nodes()[0], got[0]))
+        line["cpu_baseline"] = {"value": n * done / el, "unit": "cells/s", "cores": 1, "kind": "reference",
+                                "sample": f"{done} full Grid3D::Prepare builds ({el:.1f} s) of the same mesh and grid "
+                                          f"by the reference (single-threaded as written); node types equal: {same}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    s.close()
+    sea.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -1025,6 +1164,8 @@ def main():
         return run_adjoint(args)
     if CONFIGS[args.config].get("two_d"):
         return run_2d(args)
+    if CONFIGS[args.config].get("masks"):
+        return run_masks(args)
     return run_ours(args)
 
 

@@ -1,7 +1,7 @@
 """Generates tests/golden/masks.npz: node grids built by the reference's own
 Grid3D loaders and mask builders (oracle/_ref/libref3d.so, compiled from the
 reference's sources by oracle/Makefile) on the synthetic inputs of
-tests/mask_shapes.py, together with the inputs the GPU builders take.
+adi_b200/shapes.py, together with the inputs the GPU builders take.
 
 Run from the repository root on a machine with the reference checkout:
     python tests/golden/make_masks.py
@@ -19,7 +19,7 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 sys.path.insert(0, os.path.join(ROOT, "cmc-fluid-solver_b200"))
 
-import mask_shapes as ms  # noqa: E402
+from adi_b200 import shapes as ms  # noqa: E402
 from adi_b200 import masks  # noqa: E402
 from oracle.oracle import RefMask  # noqa: E402
 

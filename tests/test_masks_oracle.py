@@ -14,7 +14,7 @@ import tempfile
 import numpy as np
 import pytest
 
-import mask_shapes as ms
+from adi_b200 import shapes as ms
 import oracle as O
 from adi_b200 import masks
 from golden_util import GOLDEN
