@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstring>
 #include <algorithm>
+#include <initializer_list>
 #include <new>
 #include <string>
 #include <vector>
@@ -97,6 +98,8 @@ struct adi_handle {
     // adi_adjoint_run calls and grown when a call needs more; freed by adi_destroy
     char *adj_mem = nullptr;
     size_t adj_cap = 0;
+    char *mask_mem = nullptr;   // scratch of the mask builders, kept between builds
+    size_t mask_cap = 0;
     std::string contract_msg;
     std::string err;
     double diff_error = 0.0;
@@ -229,6 +232,9 @@ void free_all(adi_handle *h)
     cudaFree(h->adj_mem);
     h->adj_mem = nullptr;
     h->adj_cap = 0;
+    cudaFree(h->mask_mem);
+    h->mask_mem = nullptr;
+    h->mask_cap = 0;
     for (auto &r : h->ev_pending) {
         cudaEventDestroy(r.a);
         cudaEventDestroy(r.b);
@@ -1004,19 +1010,36 @@ adi_status adi_set_mask(adi_handle *h, const uint8_t *type, const uint8_t *bc_ve
 
 namespace {
 
-// Device scratch of one mask build, released on every return path.
+// Device scratch of one mask build: pieces of the handle's mask workspace, which
+// grows to the largest build and is kept (a build allocates nothing after the
+// first one of its size).
 struct MaskScratch {
-    std::vector<void *> p;
-    ~MaskScratch()
+    adi_handle *h;
+    size_t used = 0;
+    static size_t round(size_t b) { return (b + 255) / 256 * 256; }
+    // bytes: the sizes of all pieces the build will take, in order
+    cudaError_t reserve(std::initializer_list<size_t> bytes)
     {
-        for (void *q : p) cudaFree(q);
+        size_t total = 0;
+        for (size_t b : bytes) total += round(b < 16 ? 16 : b);
+        if (h->mask_cap < total) {
+            cudaFree(h->mask_mem);
+            h->mask_mem = nullptr;
+            h->mask_cap = 0;
+            const cudaError_t e = cudaMalloc((void **)&h->mask_mem, total);
+            if (e != cudaSuccess) return e;
+            h->mask_cap = total;
+        }
+        used = 0;
+        return cudaSuccess;
     }
     cudaError_t get(void **out, size_t bytes)
     {
-        *out = nullptr;
-        cudaError_t e = cudaMalloc(out, bytes < 16 ? 16 : bytes);
-        if (e == cudaSuccess) p.push_back(*out);
-        return e;
+        const size_t b = round(bytes < 16 ? 16 : bytes);
+        if (used + b > h->mask_cap) return cudaErrorMemoryAllocation;
+        *out = h->mask_mem + used;
+        used += b;
+        return cudaSuccess;
     }
 };
 
@@ -1068,10 +1091,11 @@ adi_status adi_mask_shape3d(adi_handle *h, const float *verts, int nverts, const
         if (tris[q] < 0 || tris[q] >= nverts)
             return fail(h, ADI_ERR_BAD_ARG, "triangle " + std::to_string(q / 3) + " names a vertex out of range");
     const long long n = h->n;
-    MaskScratch sc;
+    MaskScratch sc{h};
     uint8_t *types = nullptr;
     float *dv = nullptr;
     int *dt = nullptr, *st = nullptr;
+    CK(sc.reserve({(size_t)n, sizeof(float) * 3 * (size_t)nverts, sizeof(int) * 3 * (size_t)ntris, sizeof(int) * 8}));
     CK(sc.get((void **)&types, n));
     CK(sc.get((void **)&dv, sizeof(float) * 3 * (size_t)nverts));
     CK(sc.get((void **)&dt, sizeof(int) * 3 * (size_t)ntris));
@@ -1106,10 +1130,11 @@ adi_status adi_mask_sea(adi_handle *h, const float *depth, int depth_nx, int dep
 {
     if (!h || !depth || !in_vel || depth_nx <= 0 || depth_ny <= 0) return ADI_ERR_BAD_ARG;
     const long long n = h->n;
-    MaskScratch sc;
+    MaskScratch sc{h};
     uint8_t *snap = nullptr;
     float *dd = nullptr;
     int *st = nullptr;
+    CK(sc.reserve({(size_t)n, sizeof(float) * (size_t)depth_nx * depth_ny, sizeof(int) * 8}));
     CK(sc.get((void **)&snap, n));
     CK(sc.get((void **)&dd, sizeof(float) * (size_t)depth_nx * depth_ny));
     CK(sc.get((void **)&st, sizeof(int) * 8));   // [0..1] status, [2] flood flag, [4..7] census
@@ -1135,10 +1160,11 @@ adi_status adi_mask_extrude2d(adi_handle *h, const uint8_t *type2d, const float 
     const long long cols = (long long)h->nx * h->ny;
     for (long long c = 0; c < cols; c++)
         if (type2d[c] > NODE_VALVE) return fail(h, ADI_ERR_BAD_ARG, "2D node type out of range");
-    MaskScratch sc;
+    MaskScratch sc{h};
     uint8_t *t2 = nullptr;
     float *v2 = nullptr, *T2 = nullptr;
     int *st = nullptr;
+    CK(sc.reserve({(size_t)cols, sizeof(float) * 2 * cols, sizeof(float) * cols, sizeof(int) * 8}));
     CK(sc.get((void **)&t2, cols));
     CK(sc.get((void **)&v2, sizeof(float) * 2 * cols));
     CK(sc.get((void **)&T2, sizeof(float) * cols));

@@ -251,7 +251,8 @@ __global__ void fill_types_kernel(uint8_t *type, long long n, uint8_t v)
 
 // One flood-fill scan along direction DIR: each thread walks one line forward and
 // back; a NODE_IN cell reached from a NODE_OUT cell through NODE_IN cells becomes
-// NODE_OUT.  Threads own disjoint lines.
+// NODE_OUT.  Threads own disjoint lines.  The walk reads U cells ahead (independent
+// loads) and then runs the sequential rule over them in registers.
 template <int DIR>
 __global__ void flood_scan_kernel(uint8_t *type, int nx, int ny, int nz, int *changed)
 {
@@ -263,22 +264,34 @@ __global__ void flood_scan_kernel(uint8_t *type, int nx, int ny, int nz, int *ch
     if (DIR == 0) { base = line; stride = (long long)ny * nz; len = nx; }                               // (j, k)
     else if (DIR == 1) { base = (line / nz) * (long long)ny * nz + line % nz; stride = nz; len = ny; }  // (i, k)
     else { base = line * nz; stride = 1; len = nz; }                                                   // (i, j)
+    constexpr int U = 8;
+    uint8_t *row = type + base;
     bool any = false;
     bool reach = false;
-    for (int p = 0; p < len; p++) {
-        uint8_t *c = type + base + p * stride;
-        const uint8_t t = *c;
-        if (t == NODE_OUT) reach = true;
-        else if (t == NODE_IN) { if (reach) { *c = NODE_OUT; any = true; } }
-        else reach = false;
+    for (int p0 = 0; p0 < len; p0 += U) {
+        uint8_t t[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) t[u] = (p0 + u < len) ? row[(long long)(p0 + u) * stride] : (uint8_t)NODE_BOUND;
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (t[u] == NODE_OUT) reach = true;
+            else if (t[u] == NODE_IN) {
+                if (reach) { row[(long long)(p0 + u) * stride] = NODE_OUT; any = true; }
+            } else reach = false;
+        }
     }
     reach = false;
-    for (int p = len - 1; p >= 0; p--) {
-        uint8_t *c = type + base + p * stride;
-        const uint8_t t = *c;
-        if (t == NODE_OUT) reach = true;
-        else if (t == NODE_IN) { if (reach) { *c = NODE_OUT; any = true; } }
-        else reach = false;
+    for (int p1 = len - 1; p1 >= 0; p1 -= U) {
+        uint8_t t[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) t[u] = (p1 - u >= 0) ? row[(long long)(p1 - u) * stride] : (uint8_t)NODE_BOUND;
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (t[u] == NODE_OUT) reach = true;
+            else if (t[u] == NODE_IN) {
+                if (reach) { row[(long long)(p1 - u) * stride] = NODE_OUT; any = true; }
+            } else reach = false;
+        }
     }
     if (any) *changed = 1;
 }
@@ -505,9 +518,18 @@ __global__ void mask_census_kernel(const uint8_t *__restrict__ code, int nx, int
 {
     const long long n = (long long)nx * ny * nz;
     const long long sx = (long long)ny * nz, sy = nz;
+    const bool small = n < (1ll << 32);   // 32-bit index arithmetic suffices
     unsigned long long cnt = 0, bad = ~0ull;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(c / sx), j = (int)((c / sy) % ny), k = (int)(c % nz);
+        int i, j, k;
+        if (small) {
+            const unsigned cu = (unsigned)c, row = cu / (unsigned)nz;
+            k = (int)(cu - row * (unsigned)nz);
+            i = (int)(row / (unsigned)ny);
+            j = (int)(row - (unsigned)i * (unsigned)ny);
+        } else {
+            i = (int)(c / sx); j = (int)((c / sy) % ny); k = (int)(c % nz);
+        }
         const bool frame = i == 0 || j == 0 || k == 0 || i == nx - 1 || j == ny - 1 || k == nz - 1;
         const uint8_t t = code[c] & CODE_TYPE;
         auto ty = [&](long long q) { return code[q] & CODE_TYPE; };
