@@ -345,10 +345,8 @@ adi_status enqueue_global_iteration(adi_handle *h, R dt, int num_local, void *co
         for (int l = 0; l < num_local; l++) {
             const int merges = (dir == 0 && l == num_local - 1) ? 2 : 1;
             const size_t fb = (size_t)h->n * sizeof(R);
-            if (tape) {   // the nonlinear layer this sweep reads
-                for (int v = 0; v < 4; v++)
-                    CK(cudaMemcpyAsync(tape[v], h->d_L[h->ta][v], fb, cudaMemcpyDeviceToDevice, h->stream));
-            }
+            if (tape && q == 0 && l == 0)   // the nonlinear layer the first sweep reads
+                CK(launch_copy_fields(4, h->d_L[h->ta], tape, fb, h->stream));
             CK(timed(h, cls, bytes, [&] {
                 if (h->solver == ADI_SOLVER_FAST)
                     return launch_fast<R>(h, dir, clayer<R>(h, src[q]), clayer<R>(h, h->ta), layer<R>(h, dst[q]),
@@ -357,9 +355,18 @@ adi_status enqueue_global_iteration(adi_handle *h, R dt, int num_local, void *co
                                              clayer<R>(h, h->ta), layer<R>(h, dst[q]), layer<R>(h, h->tb),
                                              (R *)h->d_scratch, k, merges, h->stream);
             }));
-            if (tape) {   // the layer it wrote
-                for (int v = 0; v < 4; v++)
-                    CK(cudaMemcpyAsync(tape[4 + v], h->d_L[dst[q]][v], fb, cudaMemcpyDeviceToDevice, h->stream));
+            if (tape) {
+                // the layer it wrote, and (in the same launch) the nonlinear layer it
+                // wrote, which the next sweep of this iteration reads
+                const bool more = q < 2 || l < num_local - 1;
+                void *src8[8], *dst8[8];
+                for (int v = 0; v < 4; v++) {
+                    src8[v] = h->d_L[dst[q]][v];
+                    dst8[v] = tape[4 + v];
+                    src8[4 + v] = h->d_L[h->tb][v];
+                    dst8[4 + v] = tape[8 + v];
+                }
+                CK(launch_copy_fields(more ? 8 : 4, src8, dst8, fb, h->stream));
                 tape += 8;
             }
             std::swap(h->ta, h->tb);
@@ -756,7 +763,7 @@ adi_status adjoint_run(adi_handle *h, double dt, int ng, int nl, int n_steps, in
                     "adjoint buffers: " + std::string(cudaGetErrorString(e)));
     }
     auto copy4 = [&](void *const *dst, void *const *src) -> adi_status {
-        for (int v = 0; v < 4; v++) CK(cudaMemcpyAsync(dst[v], src[v], fb, cudaMemcpyDeviceToDevice, h->stream));
+        CK(launch_copy_fields(4, src, dst, fb, h->stream));
         return ADI_OK;
     };
     auto zero4 = [&](void *const *dst) -> adi_status {

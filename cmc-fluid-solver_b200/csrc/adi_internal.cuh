@@ -239,6 +239,10 @@ template <typename R>
 cudaError_t launch_objective(const DomainView<R> &d, CLayer<R> x, const int lo[3], const int hi[3], Layer<R> cbar,
                              double *psum, int nblocks, double *out, cudaStream_t s);
 
+// nf (<= 8) arrays of `bytes` each, src[f] -> dst[f], in one launch; every pointer
+// 16-byte aligned (cudaErrorInvalidValue otherwise).
+cudaError_t launch_copy_fields(int nf, const void *const *src, void *const *dst, size_t bytes, cudaStream_t s);
+
 // ---- mask builders (masks.cu) ----
 // Shape3D: types (n bytes of scratch) <- NODE_IN, triangles rasterised as
 // NODE_BOUND, outside flood-filled as NODE_OUT.  verts: 3 floats per vertex in

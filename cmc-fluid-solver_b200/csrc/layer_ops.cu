@@ -405,6 +405,48 @@ cudaError_t launch_residual(const DomainView<R> &d, CLayer<R> x, CLayer<R> t, un
     return cudaGetLastError();
 }
 
+// Up to 8 same-sized arrays copied in one launch (16-byte accesses; the arrays
+// start on 16-byte boundaries, as every layer and workspace piece does).
+struct CopySet {
+    const void *src[8];
+    void *dst[8];
+};
+
+__global__ void __launch_bounds__(256) copy_fields_kernel(CopySet cs, int nf, long long n16, long long tail)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n16; i += stride) {
+        uint4 v[8];
+#pragma unroll
+        for (int f = 0; f < 8; f++)
+            if (f < nf) v[f] = reinterpret_cast<const uint4 *>(cs.src[f])[i];
+#pragma unroll
+        for (int f = 0; f < 8; f++)
+            if (f < nf) reinterpret_cast<uint4 *>(cs.dst[f])[i] = v[f];
+    }
+    if (blockIdx.x == 0 && threadIdx.x < tail)
+        for (int f = 0; f < nf; f++)
+            reinterpret_cast<unsigned char *>(cs.dst[f])[n16 * 16 + threadIdx.x] =
+                reinterpret_cast<const unsigned char *>(cs.src[f])[n16 * 16 + threadIdx.x];
+}
+
+cudaError_t launch_copy_fields(int nf, const void *const *src, void *const *dst, size_t bytes, cudaStream_t s)
+{
+    if (nf < 1 || nf > 8) return cudaErrorInvalidValue;
+    CopySet cs{};
+    for (int f = 0; f < nf; f++) {
+        if (((uintptr_t)src[f] | (uintptr_t)dst[f]) % 16) return cudaErrorInvalidValue;
+        cs.src[f] = src[f];
+        cs.dst[f] = dst[f];
+    }
+    const long long n16 = (long long)(bytes / 16), tail = (long long)(bytes % 16);
+    long long blocks = (n16 + 255) / 256;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (blocks < 1) blocks = 1;
+    copy_fields_kernel<<<(unsigned)blocks, 256, 0, s>>>(cs, nf, n16, tail);
+    return cudaGetLastError();
+}
+
 #define INST(R)                                                                                                  \
     template cudaError_t launch_step_begin_batch<R>(const BatchDomain<R> *, int, long long, int, int, int, int,  \
                                                     bool, cudaStream_t);                                          \
