@@ -11,10 +11,13 @@
 // in shuffles, so the kernel uses neither shared memory nor barriers.
 //
 // Rows, increment form, chunk elimination and boundary handling are those of the
-// generic fast sweep (sweep_fast.cu); see the comments there.  Requirements
+// generic fast sweep (sweep_fast.cu); see the comments there.  The chunk
+// elimination, the cyclic-reduction step and the PCR updates are the shared ones
+// of sweep_common.cuh (packed FP32 in float).  Requirements
 // (checked by the launcher): dimz == P*K, K*sizeof(R) a multiple of 16 bytes,
 // 16-byte aligned field arrays.
 #include "adi_internal.cuh"
+#include "sweep_common.cuh"
 
 #include <climits>
 
@@ -31,19 +34,6 @@ __device__ __forceinline__ int zkind(bool inm, bool in0, bool inp)
     if (inp) return Z_START;
     if (inm) return Z_END;
     return Z_NONE;
-}
-
-template <typename R>
-__device__ __forceinline__ R zrcp(R x)
-{
-    return R(1) / x;
-}
-template <>
-__device__ __forceinline__ float zrcp<float>(float x)
-{
-    float r;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return fmaf(r, fmaf(-x, r, 1.0f), r);   // one Newton-Raphson step for 1/x
 }
 
 template <typename R, int K>
@@ -208,137 +198,40 @@ __global__ void __launch_bounds__(128)
         }
     }
 
-    // ---- chunk elimination (same scheme as sweep_fast.cu) ----
-    R ea[2][K], ec[2][K];
-    R Af[2], Cf[2], Al[2], Cl[2], Df[4], Dl[4];
+    // ---- chunk elimination and reduced system (shared with the X/Y sweeps) ----
+    unsigned freebits = 0;
 #pragma unroll
-    for (int m = 0; m < 2; m++) {
-        const R vis = m == 0 ? kc.vis_v : kc.vis_t;
-        const R bin = m == 0 ? kc.b_v : kc.b_t;
-        R A[K], B[K], C[K];
-#pragma unroll
-        for (int i = 0; i < K; i++) {
-            const int kd = kind[i];
-            const bool fr = m == 0 ? (cc[i] & CODE_VEL_FREE) != 0 : (cc[i] & CODE_TEMP_FREE) != 0;
-            if (kd == Z_IN) { A[i] = -rr[i] - vis; B[i] = bin; C[i] = rr[i] - vis; }
-            else if (kd == Z_NONE) { A[i] = R(0); B[i] = R(1); C[i] = R(0); }
-            else {
-                const bool first = kd != Z_END;
-                B[i] = fr ? R(2) : R(1);
-                A[i] = (!first && fr) ? R(-1) : R(0);
-                C[i] = (first && fr) ? R(-1) : R(0);
-            }
-        }
-        // interior rows 1..K-2 through x_first and x_last
-        {
-            const R r = zrcp<R>(B[1]);
-            ea[m][1] = A[1] * r;
-            ec[m][1] = C[1] * r;
-            if (m == 0) { dv[0][1] *= r; dv[1][1] *= r; dv[2][1] *= r; }
-            else dv[3][1] *= r;
-        }
-#pragma unroll
-        for (int i = 2; i <= K - 2; i++) {
-            const R r = zrcp<R>(B[i] - A[i] * ec[m][i - 1]);
-            if (m == 0) {
-#pragma unroll
-                for (int v = 0; v < 3; v++) dv[v][i] = (dv[v][i] - A[i] * dv[v][i - 1]) * r;
-            } else {
-                dv[3][i] = (dv[3][i] - A[i] * dv[3][i - 1]) * r;
-            }
-            ea[m][i] = -A[i] * ea[m][i - 1] * r;
-            ec[m][i] = C[i] * r;
-        }
-#pragma unroll
-        for (int i = K - 3; i >= 1; i--) {
-            const R ci = ec[m][i];
-            ea[m][i] -= ci * ea[m][i + 1];
-            if (m == 0) {
-#pragma unroll
-                for (int v = 0; v < 3; v++) dv[v][i] -= ci * dv[v][i + 1];
-            } else {
-                dv[3][i] -= ci * dv[3][i + 1];
-            }
-            ec[m][i] = -ci * ec[m][i + 1];
-        }
-        const R rf = zrcp<R>(B[0] - C[0] * ea[m][1]);
-        Af[m] = A[0] * rf;
-        Cf[m] = -C[0] * ec[m][1] * rf;
-        const R rl = zrcp<R>(B[K - 1] - A[K - 1] * ec[m][K - 2]);
-        Al[m] = -A[K - 1] * ea[m][K - 2] * rl;
-        Cl[m] = C[K - 1] * rl;
-        if (m == 0) {
-#pragma unroll
-            for (int v = 0; v < 3; v++) {
-                Df[v] = (dv[v][0] - C[0] * dv[v][1]) * rf;
-                Dl[v] = (dv[v][K - 1] - A[K - 1] * dv[v][K - 2]) * rl;
-            }
-        } else {
-            Df[3] = (dv[3][0] - C[0] * dv[3][1]) * rf;
-            Dl[3] = (dv[3][K - 1] - A[K - 1] * dv[3][K - 2]) * rl;
-        }
+    for (int i = 0; i < K; i++) {
+        if (cc[i] & CODE_VEL_FREE) freebits |= 1u << (2 * i);
+        if (cc[i] & CODE_TEMP_FREE) freebits |= 2u << (2 * i);
     }
+    R ea[2][K], ec[2][K];
+    sweep::Reduced<R> red;
+    sweep::eliminate<R, K>(kind, rr, freebits, kc, dv, ea, ec, red);
+    R (&Al)[2] = red.Al, (&Cl)[2] = red.Cl, (&Dl)[4] = red.Dl;
 
     // ---- reduced system in shuffles ----
     R ea_[2], ec_[2], ed[4];
     {
         // cyclic-reduction step: chunk-last row of the previous lane
-        R pA[2], pC[2], pD[4];
-#pragma unroll
-        for (int m = 0; m < 2; m++) {
-            pA[m] = sh_up(Al[m], 1, P);
-            pC[m] = sh_up(Cl[m], 1, P);
-        }
-#pragma unroll
-        for (int v = 0; v < 4; v++) pD[v] = sh_up(Dl[v], 1, P);
+        R pv[8] = {sh_up(Al[0], 1, P), sh_up(Cl[0], 1, P), sh_up(Al[1], 1, P), sh_up(Cl[1], 1, P),
+                   sh_up(Dl[0], 1, P), sh_up(Dl[1], 1, P), sh_up(Dl[2], 1, P), sh_up(Dl[3], 1, P)};
         if (ch == 0) {
-            pA[0] = pA[1] = pC[0] = pC[1] = R(0);
-            pD[0] = pD[1] = pD[2] = pD[3] = R(0);
-        }
 #pragma unroll
-        for (int m = 0; m < 2; m++) {
-            const R r = zrcp<R>(R(1) - Af[m] * pC[m] - Cf[m] * Al[m]);
-            ea_[m] = -Af[m] * pA[m] * r;
-            ec_[m] = -Cf[m] * Cl[m] * r;
-            if (m == 0) {
-#pragma unroll
-                for (int v = 0; v < 3; v++) ed[v] = (Df[v] - Af[0] * pD[v] - Cf[0] * Dl[v]) * r;
-            } else {
-                ed[3] = (Df[3] - Af[1] * pD[3] - Cf[1] * Dl[3]) * r;
-            }
+            for (int q = 0; q < 8; q++) pv[q] = R(0);
         }
+        sweep::cr_step<R>(red, pv, ea_, ec_, ed);
     }
 #pragma unroll
     for (int s = 1; s < P; s <<= 1) {
-        R mA[2], mC[2], mD[4], pA[2], pC[2], pD[4];
-#pragma unroll
-        for (int m = 0; m < 2; m++) {
-            mA[m] = sh_up(ea_[m], s, P);
-            mC[m] = sh_up(ec_[m], s, P);
-            pA[m] = sh_down(ea_[m], s, P);
-            pC[m] = sh_down(ec_[m], s, P);
-        }
-#pragma unroll
-        for (int v = 0; v < 4; v++) {
-            mD[v] = sh_up(ed[v], s, P);
-            pD[v] = sh_down(ed[v], s, P);
-        }
         // lanes whose partner lies outside the line receive their own row from the
         // shuffle; their coupling to it is exactly zero (first row a = 0, last row
         // c = 0, preserved by every step), so the finite values drop out.
-#pragma unroll
-        for (int m = 0; m < 2; m++) {
-            const R a = ea_[m], c = ec_[m];
-            const R r = zrcp<R>(R(1) - a * mC[m] - c * pA[m]);
-            if (m == 0) {
-#pragma unroll
-                for (int v = 0; v < 3; v++) ed[v] = (ed[v] - a * mD[v] - c * pD[v]) * r;
-            } else {
-                ed[3] = (ed[3] - a * mD[3] - c * pD[3]) * r;
-            }
-            ea_[m] = -a * mA[m] * r;
-            ec_[m] = -c * pC[m] * r;
-        }
+        const R mv[8] = {sh_up(ea_[0], s, P), sh_up(ec_[0], s, P), sh_up(ea_[1], s, P), sh_up(ec_[1], s, P),
+                         sh_up(ed[0], s, P),  sh_up(ed[1], s, P),  sh_up(ed[2], s, P),  sh_up(ed[3], s, P)};
+        const R pv[8] = {sh_down(ea_[0], s, P), sh_down(ec_[0], s, P), sh_down(ea_[1], s, P), sh_down(ec_[1], s, P),
+                         sh_down(ed[0], s, P),  sh_down(ed[1], s, P),  sh_down(ed[2], s, P),  sh_down(ed[3], s, P)};
+        sweep::pcr_update<R>(mv, pv, ea_, ec_, ed);
     }
     R xf[4], xl[4];
 #pragma unroll
