@@ -37,7 +37,7 @@ EXPORTED = [
     "adi2d_set_segments", "adi2d_step_tol",
     "adi2d_update_boundaries", "adi2d_time_step", "adi2d_step", "adi2d_get_state", "adi2d_set_state",
     "adi2d_get_layer", "adi2d_last_error", "adi2d_last_error_string",
-    "adi_mask_shape3d", "adi_mask_sea", "adi_mask_extrude2d", "adi_get_mask",
+    "adi_mask_shape3d", "adi_mask_sea", "adi_mask_extrude2d", "adi_get_mask", "adi_mask_shape2d",
 ]
 
 K_NUM = 7
@@ -101,6 +101,7 @@ def load() -> C.CDLL:
         "adi_mask_sea": [vp, vp, i, i, C.c_float, d, vp, d],
         "adi_mask_extrude2d": [vp, vp, vp, vp, i, d, d],
         "adi_get_mask": [vp] + [vp] * 7,
+        "adi_mask_shape2d": [vp, vp, i, i, i, d, vp, vp, vp, vp, vp],
         "adi_build_segments": [vp, C.POINTER(SegStats)],
         "adi_get_segments": [vp, i, vp, C.c_int64, C.POINTER(C.c_int64)],
         "adi_update_boundaries": [vp],

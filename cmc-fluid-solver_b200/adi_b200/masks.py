@@ -21,6 +21,10 @@ bit-identical to those the reference's ``Grid3D::Build`` receives:
   this build does not link; the caller passes the arrays.
 * ``extrude_dims``   the depth levels of a 2D shape extruded in depth
   (Grid3D::LoadFromFile, Grid3D.cpp:497-509).
+* ``load_shape2d`` / ``Shape2DFrames.subframe`` / ``build_shape2d``   a Shape2D file
+  read as FluidSolver2D::Grid2D reads it (Grid2D.cpp:268-396) and its node grid built
+  on the GPU (``adi_mask_shape2d``, Grid2D::Build); the grid feeds the 2D solver
+  (``adi2d_set_grid``) or the extrusion of a 2D shape in depth (``adi_mask_extrude2d``).
 """
 from __future__ import annotations
 
@@ -166,6 +170,133 @@ def load_shape3d(path: str, dx: float, dy: float, dz: float) -> Shape3DFrames:
     for f in frames:
         f.verts = ((f.verts - pmin) / hf).astype(F)
     return Shape3DFrames(frames, dims, pmin, pmax)
+
+
+@dataclass
+class Shape2D:
+    points: np.ndarray       # float32 [np, 2]
+    vels: np.ndarray         # float32 [np, 2]
+    active: bool             # a moving shape (valve) rather than a wall
+
+
+@dataclass
+class Shape2DFrames:
+    frames: list = field(default_factory=list)      # per frame: list of Shape2D
+    durations: list = field(default_factory=list)
+    dims: tuple = (0, 0)
+
+    def subframe(self, time: float):
+        """(segments [n, 8] float32: p1, p2, v1, v2; node types [n] uint8) that
+        Grid2D::Build rasterises at `time` (Grid2D::Prepare and ComputeSubframe,
+        Grid2D.cpp:411-477), moving shapes first, in the reference's order."""
+        nf = len(self.frames)
+        a = [0.0]
+        for dur in self.durations:
+            a.append(a[-1] + dur)
+        r_time = math.fmod(time, a[nf])
+        frame = 0
+        for i in range(1, nf):
+            if a[i] < r_time:
+                frame = i
+        substep = (r_time - a[frame]) / (a[frame + 1] - a[frame])
+        f0, f1 = self.frames[frame % nf], self.frames[(frame % nf + 1) % nf]
+        ti, ts = F(1.0 - substep), F(substep)
+        shapes = []
+        for s0, s1 in zip(f0, f1):
+            pts = (s0.points * ti + s1.points * ts).astype(F)
+            vel = (s0.vels * ti + s1.vels * ts).astype(F)
+            shapes.append((pts, vel, s0.active))
+        segs, kinds = [], []
+        for want_active, kind in ((True, 3), (False, 2)):   # NODE_VALVE, then NODE_BOUND
+            for pts, vel, active in shapes:
+                if active != want_active:
+                    continue
+                for i in range(len(pts) - 1):
+                    segs.append(np.concatenate([pts[i], pts[i + 1], vel[i], vel[i + 1]]))
+                    kinds.append(kind)
+        segs = np.array(segs, F).reshape(-1, 8)
+        return segs, np.array(kinds, np.uint8)
+
+
+def load_shape2d(path: str, dx: float, dy: float) -> Shape2DFrames:
+    """Grid2D::LoadFromFile (Grid2D.cpp:268-373, no field file) of a Shape2D text
+    file: frames of polylines, each passive (a wall) or moving ("Motion" and a
+    velocity: a valve); the border velocities between frames
+    (ComputeBorderVelocities :375-396), the bounding box with padding, the grid size
+    and the grid coordinates (Grid2D::Init :197-229)."""
+    with open(path, "r") as fh:
+        toks = fh.read().split()
+    pos = 0
+
+    def nxt():
+        nonlocal pos
+        t = toks[pos]
+        pos += 1
+        return t
+
+    def point():
+        return np.array([F(_atof(nxt().replace(",", "."))) for _ in range(2)], F)
+
+    frames, durations = [], []
+    for _ in range(_scan_int(nxt())):
+        durations.append(float(F(float(nxt()))))
+        shapes = []
+        for _ in range(_scan_int(nxt())):
+            npt = _scan_int(nxt())
+            pts = np.array([point() * GRID_SCALE_FACTOR for _ in range(npt)], F).reshape(npt, 2)
+            word = nxt()
+            v = point() if word.startswith("M") else np.zeros(2, F)
+            shapes.append(Shape2D(pts, np.tile((v * GRID_SCALE_FACTOR).astype(F), (npt, 1)), word.startswith("M")))
+        frames.append(shapes)
+    nf = len(frames)
+    for j in range(nf):
+        nj = (j + 1) % nf
+        m = F(1.0 / durations[j])
+        for i, sh in enumerate(frames[j]):
+            nxt_sh = frames[nj][i]
+            if not sh.active:
+                nxt_sh.vels = ((nxt_sh.points - sh.points) * m).astype(F)
+            else:
+                nxt_sh.vels = (nxt_sh.vels + (sh.points - nxt_sh.points) * m).astype(F)
+    pmin = np.full(2, INF, F)
+    pmax = np.full(2, -INF, F)
+    for shapes in frames:
+        for sh in shapes:
+            for pt in sh.points:
+                for c in range(2):
+                    if pt[c] < pmin[c]:
+                        pmin[c] = pt[c]
+                    if pt[c] > pmax[c]:
+                        pmax[c] = pt[c]
+    w = (pmax - pmin).astype(F)
+    pmin = (pmin - w * BBOX_PADDING).astype(F)
+    pmax = (pmax + w * BBOX_PADDING).astype(F)
+    h = (dx, dy)
+    dims = tuple(int(math.ceil(float(F(pmax[c] - pmin[c])) / h[c])) + 1 for c in range(2))
+    hf = np.array([F(dx), F(dy)], F)
+    for shapes in frames:
+        for sh in shapes:
+            sh.points = ((sh.points - pmin) / hf).astype(F)
+    return Shape2DFrames(frames, durations, dims)
+
+
+def build_shape2d(segs, seg_types, nx: int, ny: int, start_T: float, stream=None):
+    """adi_mask_shape2d: the 2D node grid (type, bc, velocity [nx, ny, 2], T) built
+    on the GPU from the segments of Shape2DFrames.subframe."""
+    import ctypes as C
+
+    from . import _abi
+    lib = _abi.load()
+    sg = np.ascontiguousarray(segs, F).reshape(-1, 8)
+    kt = np.ascontiguousarray(seg_types, np.uint8)
+    t = np.zeros((nx, ny), np.uint8)
+    bc = np.zeros((nx, ny), np.uint8)
+    v = np.zeros((nx, ny, 2), F)
+    T = np.zeros((nx, ny), F)
+    handle = stream if (stream is None or isinstance(stream, int)) else getattr(stream, "cuda_stream", stream)
+    _abi.check(lib.adi_mask_shape2d(sg.ctypes.data, kt.ctypes.data, len(sg), nx, ny, start_T, C.c_void_p(handle),
+                                    t.ctypes.data, bc.ctypes.data, v.ctypes.data, T.ctypes.data))
+    return t, bc, v, T
 
 
 def sea_geometry(lats: np.ndarray, lons: np.ndarray, depth: np.ndarray, dx: float, dy: float, dz: float):

@@ -94,19 +94,23 @@ def depth_map(dnx=64, dny=50, seed=3, open_far=False):
     return d.astype(np.float32)
 
 
-def write_shape2d(path: str, shapes, duration=10.0) -> None:
+def write_shape2d(path: str, shapes, duration=10.0, frames=None) -> None:
     """shapes: list of (points [np, 2], velocity or None); a velocity makes the
-    shape a moving wall or valve ("Motion"), None a passive wall."""
-    lines = ["1", _fmt(duration), str(len(shapes))]
-    for pts, vel in shapes:
-        lines.append(str(len(pts)))
-        for p in pts:
-            lines.append(f"{_fmt(p[0])} {_fmt(p[1])}")
-        if vel is None:
-            lines.append("Passive")
-        else:
-            lines.append("Motion")
-            lines.append(f"{_fmt(vel[0])} {_fmt(vel[1])}")
+    shape a moving wall or valve ("Motion"), None a passive wall.  frames: a list
+    of (duration, shapes) for several frames instead (the same shapes, moved)."""
+    frames = frames if frames is not None else [(duration, shapes)]
+    lines = [str(len(frames))]
+    for dur, shp in frames:
+        lines += [_fmt(dur), str(len(shp))]
+        for pts, vel in shp:
+            lines.append(str(len(pts)))
+            for p in pts:
+                lines.append(f"{_fmt(p[0])} {_fmt(p[1])}")
+            if vel is None:
+                lines.append("Passive")
+            else:
+                lines.append("Motion")
+                lines.append(f"{_fmt(vel[0])} {_fmt(vel[1])}")
     with open(path, "w") as fh:
         fh.write("\n".join(lines) + "\n")
 
@@ -121,3 +125,12 @@ def channel2d():
         (np.array([(1000.0, 0.0), (1000.0, 420.0)]), (0.0, 0.0)),
         (np.array([(380.0, 150.0), (470.0, 210.0), (390.0, 280.0), (380.0, 150.0)]), None),
     ]
+
+
+def channel2d_moving():
+    """Two frames of a channel whose obstacle moves down and to the right, with a
+    moving valve segment on the lower wall."""
+    f0 = channel2d()
+    f1 = [(pts if i != 4 else pts + np.array([60.0, -35.0]), vel) for i, (pts, vel) in enumerate(channel2d())]
+    valve = (np.array([(600.0, 0.0), (700.0, 0.0)]), (0.0, 250.0))
+    return [(0.5, f0 + [valve]), (0.7, f1 + [(valve[0] + np.array([20.0, 0.0]), valve[1])])]

@@ -1191,6 +1191,53 @@ adi_status adi_mask_extrude2d(adi_handle *h, const uint8_t *type2d, const float 
     return finish_device_mask(h, (unsigned long long *)(st + 4));
 }
 
+adi_status adi_mask_shape2d(const float *segs, const uint8_t *seg_type, int nseg, int nx, int ny, double start_T,
+                            void *cuda_stream, uint8_t *type2d, uint8_t *bc2d, float *vel2d, float *T2d)
+{
+    if (nseg < 0 || nx < 1 || ny < 1 || (nseg > 0 && (!segs || !seg_type)) || !type2d || !bc2d || !vel2d || !T2d)
+        return ADI_ERR_BAD_ARG;
+    for (int q = 0; q < nseg; q++)
+        if (seg_type[q] != NODE_BOUND && seg_type[q] != NODE_VALVE) return ADI_ERR_BAD_ARG;
+    adi_handle *h = nullptr;   // no handle: CK reports the status only
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    const long long n = (long long)nx * ny;
+    struct Bufs {
+        void *p[8] = {};
+        ~Bufs()
+        {
+            for (void *q : p) cudaFree(q);
+        }
+    } b;
+    CK(cudaMalloc(&b.p[0], sizeof(float) * 8 * (size_t)(nseg > 0 ? nseg : 1)));
+    CK(cudaMalloc(&b.p[1], (size_t)(nseg > 0 ? nseg : 1)));
+    CK(cudaMalloc(&b.p[2], sizeof(unsigned long long) * n));
+    CK(cudaMalloc(&b.p[3], n));
+    CK(cudaMalloc(&b.p[4], sizeof(float) * 2 * n));
+    CK(cudaMalloc(&b.p[5], sizeof(float) * n));
+    CK(cudaMalloc(&b.p[6], n));
+    CK(cudaMalloc(&b.p[7], sizeof(int) * 4));
+    CK(cudaMemsetAsync(b.p[7], 0, sizeof(int) * 4, st));
+    if (nseg > 0) {
+        CK(cudaMemcpyAsync(b.p[0], segs, sizeof(float) * 8 * (size_t)nseg, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(b.p[1], seg_type, nseg, cudaMemcpyHostToDevice, st));
+    }
+    int passes = 0;
+    int *status = (int *)b.p[7];
+    CK(launch_mask_shape2d((const float *)b.p[0], (const uint8_t *)b.p[1], nseg, nx, ny, (float)start_T,
+                           (unsigned long long *)b.p[2], (uint8_t *)b.p[3], (float *)b.p[4], (float *)b.p[5],
+                           (uint8_t *)b.p[6], status, status + 2, (int)std::min<long long>(n + 1, INT_MAX), &passes,
+                           st));
+    int hs[2] = {0, 0};
+    CK(cudaMemcpyAsync(hs, status, sizeof hs, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(type2d, b.p[3], n, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(bc2d, b.p[6], n, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(vel2d, b.p[4], sizeof(float) * 2 * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(T2d, b.p[5], sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (hs[0] > 0 || hs[1] > 0) return ADI_ERR_BAD_ARG;   // a segment leaves the grid or never ends
+    return ADI_OK;
+}
+
 adi_status adi_get_mask(adi_handle *h, uint8_t *type, uint8_t *bc_vel, uint8_t *bc_temp, double *vx, double *vy,
                         double *vz, double *T)
 {

@@ -252,6 +252,12 @@ cudaError_t launch_copy_fields(int nf, const void *const *src, void *const *dst,
 cudaError_t launch_mask_shape3d(uint8_t *types, int nx, int ny, int nz, const float *verts, int nverts,
                                 const int *tris, int ntris, int *status, int *changed, int max_passes,
                                 int *passes_out, cudaStream_t s);
+// Shape2D: a 2D node grid (nx x ny, i-major) from segments (8 floats each: p1, p2,
+// v1, v2 in grid coordinates) in the reference's write order, with their node
+// types (color).  key: nx*ny 64-bit scratch; vel: 2 floats per cell.
+cudaError_t launch_mask_shape2d(const float *segs, const uint8_t *color, int nseg, int nx, int ny, float startT,
+                                unsigned long long *key, uint8_t *type, float *vel, float *T, uint8_t *bc,
+                                int *status, int *changed, int max_passes, int *passes_out, cudaStream_t s);
 template <typename R>
 cudaError_t launch_mask_shape3d_install(const uint8_t *types, uint8_t *code, Layer<R> nv, Layer<R> cur, long long n,
                                         R baseT, cudaStream_t s);

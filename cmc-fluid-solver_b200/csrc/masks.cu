@@ -509,6 +509,80 @@ __global__ void copy_state_kernel(Layer<R> nv, Layer<R> cur, long long n)
         for (int v = 0; v < 4; v++) cur.f[v][c] = nv.f[v][c];
 }
 
+// ---------------------------------------------------------------------------
+// Shape2D (FluidSolver2D::Grid2D::Build, Grid2D.cpp:231-266): a 2D node grid from
+// polylines.  Every cell NODE_IN; the segments of the moving shapes rasterised as
+// NODE_VALVE, then those of the fixed shapes as NODE_BOUND (RasterLine,
+// Grid2D.cpp:109-141, the no-slip form: the cell takes the velocity interpolated
+// along the segment and T = startT); the outside flood-filled from cell (0,0);
+// NODE_IN / NODE_OUT cells get v = 0, T = startT.  Every cell's BC is no-slip.
+//
+// In the reference a later write to a cell replaces an earlier one, in segment
+// order and step order.  Here every segment walks its steps in one thread twice:
+// the first walk claims each cell with the largest (segment, step) sequence
+// number that reaches it (atomicMax), the second writes the data where its own
+// number won, which is the reference's last write.
+// ---------------------------------------------------------------------------
+
+// one segment: p1 (2), p2 (2), v1 (2), v2 (2) in grid coordinates
+struct Seg2D {
+    float p1x, p1y, p2x, p2y, v1x, v1y, v2x, v2y;
+};
+
+template <bool WRITE>
+__global__ void raster2d_kernel(const float *__restrict__ segs, const uint8_t *__restrict__ color, int nseg, int nx,
+                                int ny, unsigned long long *key, uint8_t *type, float *vel, int *status)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nseg) return;
+    const Seg2D sg = reinterpret_cast<const Seg2D *>(segs)[q];
+    const float ox = fsub(sg.p2x, sg.p1x), oy = fsub(sg.p2y, sg.p1y);
+    const int steps = to_int(smax(fabsf(ox), fabsf(oy))) + 1;
+    if (steps > MAX_WALK) {
+        if (!WRITE) atomicAdd(&status[ST_BOUNDED], 1);
+        return;
+    }
+    const float fs = __int2float_rn(steps);
+    const float dpx = fdiv(ox, fs), dpy = fdiv(oy, fs);
+    const float dvx = fdiv(fsub(sg.v2x, sg.v1x), fs), dvy = fdiv(fsub(sg.v2y, sg.v1y), fs);
+    float px = sg.p1x, py = sg.p1y, vx = sg.v1x, vy = sg.v1y;
+    for (int i = 0; i <= steps; i++) {
+        const int x = to_int(px), y = to_int(py);
+        if (x < 0 || x >= nx || y < 0 || y >= ny) {
+            if (!WRITE) atomicAdd(&status[ST_OUTSIDE], 1);
+        } else {
+            const long long c = (long long)x * ny + y;
+            const unsigned long long seq = ((unsigned long long)(q + 1) << 32) | (unsigned)i;
+            if (!WRITE) atomicMax(&key[c], seq);
+            else if (key[c] == seq) {
+                type[c] = color[q];
+                vel[2 * c] = vx;
+                vel[2 * c + 1] = vy;
+            }
+        }
+        px = fadd(px, dpx);
+        py = fadd(py, dpy);
+        vx = fadd(vx, dvx);
+        vy = fadd(vy, dvy);
+    }
+}
+
+// The end of Grid2D::Build (Grid2D.cpp:256-265): NODE_IN / NODE_OUT cells get v = 0;
+// every cell T = startT and a no-slip BC.
+__global__ void shape2d_finish_kernel(const uint8_t *__restrict__ type, float *vel, float *T, uint8_t *bc, long long n,
+                                      float startT)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const uint8_t t = type[c];
+        if (t == NODE_IN || t == NODE_OUT) {
+            vel[2 * c] = 0.0f;
+            vel[2 * c + 1] = 0.0f;
+        }
+        T[c] = startT;
+        bc[c] = BC_NOSLIP;
+    }
+}
+
 // The solver contract and the NODE_IN count of a node grid, on the device: the
 // same tests as the host's check of an uploaded mask, in the same order, so the
 // first failing cell in linear order (and the rule it fails) is the one the host
@@ -569,6 +643,54 @@ int grid_for(long long n, int threads)
 
 } // namespace
 
+// Flood fill from cell (0,0,0), which becomes NODE_OUT whatever it was, through
+// NODE_IN cells (6 neighbours; 4 when nz = 1): passes of X, Y and Z line scans
+// until one changes nothing, at most max_passes.
+static cudaError_t flood_fill(uint8_t *types, int nx, int ny, int nz, int *changed, int max_passes, int *passes_out,
+                              cudaStream_t s)
+{
+    fill_types_kernel<<<1, 1, 0, s>>>(types, 1, NODE_OUT);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    int passes = 0;
+    const long long lz = (long long)nx * ny, ly = (long long)nx * nz, lx = (long long)ny * nz;
+    while (passes < max_passes) {
+        if ((e = cudaMemsetAsync(changed, 0, sizeof(int), s)) != cudaSuccess) return e;
+        if (nz > 1) flood_scan_kernel<2><<<(unsigned)((lz + 127) / 128), 128, 0, s>>>(types, nx, ny, nz, changed);
+        flood_scan_kernel<1><<<(unsigned)((ly + 127) / 128), 128, 0, s>>>(types, nx, ny, nz, changed);
+        flood_scan_kernel<0><<<(unsigned)((lx + 127) / 128), 128, 0, s>>>(types, nx, ny, nz, changed);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        int h = 0;
+        if ((e = cudaMemcpyAsync(&h, changed, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+        passes++;
+        if (!h) break;
+    }
+    *passes_out = passes;
+    return cudaSuccess;
+}
+
+cudaError_t launch_mask_shape2d(const float *segs, const uint8_t *color, int nseg, int nx, int ny, float startT,
+                                unsigned long long *key, uint8_t *type, float *vel, float *T, uint8_t *bc,
+                                int *status, int *changed, int max_passes, int *passes_out, cudaStream_t s)
+{
+    const long long n = (long long)nx * ny;
+    fill_types_kernel<<<grid_for(n, 256), 256, 0, s>>>(type, n, NODE_IN);
+    cudaError_t e = cudaMemsetAsync(key, 0, sizeof(unsigned long long) * n, s);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(vel, 0, sizeof(float) * 2 * n, s)) != cudaSuccess) return e;
+    if (nseg > 0) {
+        const unsigned blocks = (unsigned)((nseg + 127) / 128);
+        raster2d_kernel<false><<<blocks, 128, 0, s>>>(segs, color, nseg, nx, ny, key, type, vel, status);
+        raster2d_kernel<true><<<blocks, 128, 0, s>>>(segs, color, nseg, nx, ny, key, type, vel, status);
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    // FloodFill(NODE_OUT) from (0,0) (Grid2D.cpp:156-195), 4 neighbours
+    if ((e = flood_fill(type, nx, ny, 1, changed, max_passes, passes_out, s)) != cudaSuccess) return e;
+    shape2d_finish_kernel<<<grid_for(n, 256), 256, 0, s>>>(type, vel, T, bc, n, startT);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_mask_shape3d(uint8_t *types, int nx, int ny, int nz, const float *verts, int nverts,
                                 const int *tris, int ntris, int *status, int *changed, int max_passes,
                                 int *passes_out, cudaStream_t s)
@@ -583,26 +705,8 @@ cudaError_t launch_mask_shape3d(uint8_t *types, int nx, int ny, int nz, const fl
         raster_triangles_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(g, verts, tris, ntris, nverts);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
-    // FloodFill from (0,0,0) (Grid3D.cpp:875-878): the start cell is NODE_OUT
-    // whatever it was.
-    fill_types_kernel<<<1, 1, 0, s>>>(types, 1, NODE_OUT);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    int passes = 0;
-    const long long lz = (long long)nx * ny, ly = (long long)nx * nz, lx = (long long)ny * nz;
-    while (passes < max_passes) {
-        if ((e = cudaMemsetAsync(changed, 0, sizeof(int), s)) != cudaSuccess) return e;
-        flood_scan_kernel<2><<<(unsigned)((lz + 127) / 128), 128, 0, s>>>(types, nx, ny, nz, changed);
-        flood_scan_kernel<1><<<(unsigned)((ly + 127) / 128), 128, 0, s>>>(types, nx, ny, nz, changed);
-        flood_scan_kernel<0><<<(unsigned)((lx + 127) / 128), 128, 0, s>>>(types, nx, ny, nz, changed);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        int h = 0;
-        if ((e = cudaMemcpyAsync(&h, changed, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
-        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
-        passes++;
-        if (!h) break;
-    }
-    *passes_out = passes;
-    return cudaSuccess;
+    // FloodFill from (0,0,0) (Grid3D.cpp:875-878)
+    return flood_fill(types, nx, ny, nz, changed, max_passes, passes_out, s);
 }
 
 template <typename R>

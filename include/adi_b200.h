@@ -161,6 +161,22 @@ adi_status adi_mask_sea(adi_handle *h, const float *depth, int depth_nx, int dep
 adi_status adi_mask_extrude2d(adi_handle *h, const uint8_t *type2d, const float *vel2d,
                               const float *T2d, int active_nz, double depth_var, double base_T);
 
+/* FluidSolver2D::Grid2D::Build (Grid2D.cpp:231-266) on the GPU, for the no-slip
+ * grids of the 2D solver and of 2D shapes extruded in depth (Grid3D's 2D grid):
+ * every cell NODE_IN, the segments rasterised (RasterLine, Grid2D.cpp:109-141:
+ * the cell takes the velocity interpolated along the segment, later segments and
+ * steps overwriting earlier ones), the outside flood-filled from cell (0,0)
+ * (FloodFill, :156-195), NODE_IN/NODE_OUT cells v = 0; T = (float)start_T and a
+ * no-slip BC everywhere.  segs: 8 floats per segment (p1, p2, v1, v2, grid
+ * coordinates) in the reference's order -- the segments of the moving shapes,
+ * then those of the fixed ones (Grid2D.cpp:237-252); seg_type: NODE_VALVE or
+ * NODE_BOUND per segment.  The grid (nx x ny, i-major) comes back in host arrays:
+ * node type, BC, velocity (2 floats) and T per cell.  Runs on cuda_stream (NULL:
+ * the default stream) of the current device.  A segment that leaves the grid
+ * (the reference writes outside its node array) returns ADI_ERR_BAD_ARG. */
+adi_status adi_mask_shape2d(const float *segs, const uint8_t *seg_type, int nseg, int nx, int ny, double start_T,
+                            void *cuda_stream, uint8_t *type2d, uint8_t *bc2d, float *vel2d, float *T2d);
+
 /* Reads the node grid back (types, BCs, node values in double). */
 adi_status adi_get_mask(adi_handle *h, uint8_t *type, uint8_t *bc_vel, uint8_t *bc_temp,
                         double *vx, double *vy, double *vz, double *T);

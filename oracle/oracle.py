@@ -66,7 +66,7 @@ def _load_ref():
         lib.ref_mask_prepare.argtypes = [vp, d]
         lib.ref_mask_nodes.argtypes = [vp] + [_u8p] * 3 + [_f32p] * 4
         lib.ref_shape3d_frame.argtypes = [vp, i, vp, vp, C.POINTER(i)]
-        lib.ref_shape2d_grid.argtypes = [vp, _u8p, _f32p, _f32p]
+        lib.ref_shape2d_grid.argtypes = [vp, _u8p, _u8p, _f32p, _f32p]
         lib.ref_mask_destroy.argtypes = [vp]
         _ref = lib
     return _ref
@@ -444,9 +444,11 @@ class RefMask:
     def grid2d(self):
         nx, ny = self.dims[0], self.dims[1]
         t = np.zeros((nx, ny), np.uint8)
+        bc = np.zeros((nx, ny), np.uint8)
         v = np.zeros((nx, ny, 2), np.float32)
         T = np.zeros((nx, ny), np.float32)
-        self.lib.ref_shape2d_grid(self.h, t, v, T)
+        self.lib.ref_shape2d_grid(self.h, t, bc, v, T)
+        self.last_bc2d = bc
         return t, v, T
 
     def close(self):

@@ -417,8 +417,8 @@ int ref_shape3d_frame(void *vg, int f, float *verts, int *tris, int *ntris)
 	return sh.NumVertices;
 }
 
-// The 2D helper grid after Prepare (types, velocity and T per (i, j), i-major).
-void ref_shape2d_grid(void *vg, unsigned char *type, float *vel2, float *T)
+// The 2D helper grid after Prepare (types, BC, velocity and T per (i, j), i-major).
+void ref_shape2d_grid(void *vg, unsigned char *type, unsigned char *bc, float *vel2, float *T)
 {
 	MaskGrid *g = (MaskGrid *)vg;
 	FluidSolver2D::Grid2D *g2 = g->GetGrid2D();
@@ -428,6 +428,7 @@ void ref_shape2d_grid(void *vg, unsigned char *type, float *vel2, float *T)
 			size_t c = (size_t)i * g2->dimy + j;
 			FluidSolver2D::CondData2D d = g2->GetData(i, j);
 			type[c] = (unsigned char)g2->GetType(i, j);
+			bc[c] = (unsigned char)d.type;
 			vel2[2 * c] = d.vel.x; vel2[2 * c + 1] = d.vel.y; T[c] = d.T;
 		}
 }

@@ -72,6 +72,24 @@ def main():
             out[f"e2_{name}_depth_var"] = np.array(dvar)
             r.close()
 
+    with tempfile.TemporaryDirectory() as tmp:
+        # Shape2D node grids (Grid2D::Build) of the 2D grid of Grid3D's Shape2D path
+        for name, frames, time, d in (("channel", [(10.0, ms.channel2d())], 0.0, 0.01),
+                                      ("moving", ms.channel2d_moving(), 0.8, 0.008)):
+            path = os.path.join(tmp, name + ".txt")
+            ms.write_shape2d(path, None, frames=frames)
+            r = RefMask.shape2d(path, d, d, 0.02, 0.3, 0.4, BASE_T)
+            r.prepare(time)
+            t2, v2, T2 = r.grid2d()
+            sf = masks.load_shape2d(path, d, d)
+            assert sf.dims == (int(r.dims[0]), int(r.dims[1]))
+            segs, kinds = sf.subframe(time)
+            out[f"s2_{name}_segs"], out[f"s2_{name}_kinds"] = segs, kinds
+            out[f"s2_{name}_dims"] = np.array(sf.dims, np.int32)
+            out[f"s2_{name}_type"], out[f"s2_{name}_bc"] = t2, r.last_bc2d
+            out[f"s2_{name}_vel"], out[f"s2_{name}_T"] = v2, T2
+            r.close()
+
     for name, open_far, vel, tin in (("basin", False, (0.0, 0.0, 0.0), 1.0), ("open", True, (0.1, -0.2, 0.05), 1.5)):
         lats = np.linspace(64.0, 67.0, 64)
         lons = np.linspace(32.0, 37.0, 50)

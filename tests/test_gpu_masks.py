@@ -167,3 +167,31 @@ def test_contract_check_of_built_mask_matches_upload(adi_lib):
         assert s.step(1e-3, 1, 1) == _abi.ADI_ERR_BAD_ARG
         msgs.append(s.lib.adi_last_error_string(s.h))
     assert msgs[0] == msgs[1] and b"outer frame" in msgs[0]
+
+
+S2 = sorted({k[3:-5] for k in Z.files if k.startswith("s2_") and k.endswith("_type")})
+
+
+@pytest.mark.parametrize("name", S2)
+def test_shape2d_matches_reference(adi_lib, name):
+    """adi_mask_shape2d == the reference's Grid2D::Build (node type, BC, velocity, T)."""
+    p = "s2_" + name
+    nx, ny = (int(v) for v in Z[p + "_dims"])
+    t, bc, v, T = masks.build_shape2d(Z[p + "_segs"], Z[p + "_kinds"], nx, ny, 1.0)
+    np.testing.assert_array_equal(t, Z[p + "_type"])
+    np.testing.assert_array_equal(bc, Z[p + "_bc"])
+    np.testing.assert_array_equal(v.view(np.uint32), Z[p + "_vel"].view(np.uint32))
+    np.testing.assert_array_equal(T.view(np.uint32), Z[p + "_T"].view(np.uint32))
+
+
+def test_shape2d_then_extrusion_matches_reference(adi_lib):
+    """A Shape2D file to a 3D node grid entirely on the GPU: the 2D grid built by
+    adi_mask_shape2d, extruded by adi_mask_extrude2d, equals the reference's
+    Grid3D::Prepare of the same file."""
+    p2, p3 = "s2_channel", "e2_ch_bump"
+    nx, ny = (int(v) for v in Z[p2 + "_dims"])
+    t, bc, v, T = masks.build_shape2d(Z[p2 + "_segs"], Z[p2 + "_kinds"], nx, ny, 1.0)
+    _, _, nz, active = (int(x) for x in Z[p3 + "_dims"])
+    s = _solver(adi_lib, (nx, ny, nz))
+    s.mask_extrude2d(t, v, T, active, float(Z[p3 + "_depth_var"]), 1.0)
+    _compare(s.get_mask(), p3)

@@ -102,3 +102,26 @@ def test_fixtures_are_what_the_reference_builds():
     got = r.nodes()
     np.testing.assert_array_equal(got[0], Z["sea_open_type"])
     np.testing.assert_array_equal(np.stack(got[3:]), Z["sea_open_val"])
+
+
+def test_shape2d_subframe_matches_fixture(tmp_path):
+    """load_shape2d + subframe give the segments recorded with the fixtures (the grid
+    they build is compared with the reference's on the GPU)."""
+    for name, frames, time, d in (("channel", [(10.0, ms.channel2d())], 0.0, 0.01),
+                                  ("moving", ms.channel2d_moving(), 0.8, 0.008)):
+        path = str(tmp_path / (name + ".txt"))
+        ms.write_shape2d(path, None, frames=frames)
+        sf = masks.load_shape2d(path, d, d)
+        segs, kinds = sf.subframe(time)
+        assert sf.dims == tuple(Z[f"s2_{name}_dims"])
+        np.testing.assert_array_equal(segs.view(np.uint32), Z[f"s2_{name}_segs"].view(np.uint32))
+        np.testing.assert_array_equal(kinds, Z[f"s2_{name}_kinds"])
+
+
+@need_ref
+@pytest.mark.parametrize("d", [0.01, 0.008, 0.013])
+def test_shape2d_grid_size_matches_reference(tmp_path, d):
+    path = str(tmp_path / "moving.txt")
+    ms.write_shape2d(path, None, frames=ms.channel2d_moving())
+    r = O.RefMask.shape2d(path, d, d, 0.02, 0.3, 0.4, 1.0)
+    assert masks.load_shape2d(path, d, d).dims == (int(r.dims[0]), int(r.dims[1]))
