@@ -684,8 +684,10 @@ adi_status time_step_tol(adi_handle *h, double dt, int max_global, int num_local
 // ---------------------------------------------------------------------------
 // Adjoint: dJ/d(node values) and dJ/d(initial state) of n_steps adi_step calls,
 // J the kinetic energy in a box at the end.  Checkpoints the state every
-// ckpt_every steps; each window is recomputed with a tape (per sweep: the
-// nonlinear layer read and the layer written) and run backward.
+// ckpt_every steps; each window is run backward from a tape (per sweep: the
+// nonlinear layer read and the layer written), which the forward pass records
+// for the last window and a recomputation from the window's checkpoint for the
+// others.
 // ---------------------------------------------------------------------------
 
 // One device allocation carved into 256-byte aligned pieces (thousands of tape
@@ -772,9 +774,30 @@ adi_status adjoint_run(adi_handle *h, double dt, int ng, int nl, int n_steps, in
     };
     adi_status st;
     const R dtr = (R)dt;
-    // ---- forward, keeping checkpoints ----
+    // one step with its tape (the recomputation of a window does the same)
+    auto taped_step = [&](int t, int t0) -> adi_status {
+        h->bv_synced = true;
+        CK(timed(h, ADI_K_STEP_BEGIN, (int64_t)h->n * (1 + 8 * (int64_t)sizeof(R)), [&] {
+            return launch_step_begin<R>(view<R>(h), layer<R>(h, h->cur), layer<R>(h, h->nxt), layer<R>(h, h->ta),
+                                        layer<R>(h, h->tb), true, h->stream);
+        }));
+        void *const *tp = &tape[(size_t)(t - t0) * S * 8];
+        for (int it = 0; it < ng; it++) {
+            const adi_status s2 = enqueue_global_iteration<R>(h, dtr, nl, tp + (size_t)it * nl * 3 * 8);
+            if (s2 != ADI_OK) return s2;
+        }
+        std::swap(h->cur, h->nxt);
+        h->bv_synced = false;
+        return ADI_OK;
+    };
+    // ---- forward, keeping checkpoints; the last window records its tape directly ----
+    const int last_t0 = (nck - 1) * ck;
     for (int t = 0; t < n_steps; t++) {
         if (t % ck == 0 && (st = copy4(&ckpt[(size_t)(t / ck) * 4], h->d_L[h->cur])) != ADI_OK) return st;
+        if (t >= last_t0) {
+            if ((st = taped_step(t, last_t0)) != ADI_OK) return st;
+            continue;
+        }
         h->bv_synced = true;
         if (h->graphs_on && !h->prof_on) st = step_graph<R>(h, dtr, ng, nl, 0, true);
         else st = enqueue_step<R>(h, dtr, ng, nl, 0, true);
@@ -790,20 +813,10 @@ adi_status adjoint_run(adi_handle *h, double dt, int ng, int nl, int n_steps, in
     // ---- backward, one checkpoint window at a time ----
     for (int w = nck - 1; w >= 0; w--) {
         const int t0 = w * ck, t1 = t0 + ck < n_steps ? t0 + ck : n_steps;
-        if ((st = copy4(h->d_L[h->cur], &ckpt[(size_t)w * 4])) != ADI_OK) return st;
-        for (int t = t0; t < t1; t++) {
-            h->bv_synced = true;
-            CK(timed(h, ADI_K_STEP_BEGIN, (int64_t)h->n * (1 + 8 * (int64_t)sizeof(R)), [&] {
-                return launch_step_begin<R>(view<R>(h), layer<R>(h, h->cur), layer<R>(h, h->nxt), layer<R>(h, h->ta),
-                                            layer<R>(h, h->tb), true, h->stream);
-            }));
-            void *const *tp = &tape[(size_t)(t - t0) * S * 8];
-            for (int it = 0; it < ng; it++) {
-                st = enqueue_global_iteration<R>(h, dtr, nl, tp + (size_t)it * nl * 3 * 8);
-                if (st != ADI_OK) return st;
-            }
-            std::swap(h->cur, h->nxt);
-            h->bv_synced = false;
+        if (w < nck - 1) {   // the last window's tape is the forward pass's
+            if ((st = copy4(h->d_L[h->cur], &ckpt[(size_t)w * 4])) != ADI_OK) return st;
+            for (int t = t0; t < t1; t++)
+                if ((st = taped_step(t, t0)) != ADI_OK) return st;
         }
         for (int t = t1 - 1; t >= t0; t--) {
             void *const *tp = &tape[(size_t)(t - t0) * S * 8];
