@@ -1104,7 +1104,8 @@ def run_masks(args):
                 "d2h_bytes_per_step": int(sum(a.nbytes for a in got)), "steps": e2e_steps,
                 "note": "adi_mask_shape3d from host vertices, then adi_get_mask of the whole node grid "
                         "(types, BCs, node values as doubles)"},
-        "gpu_launches": None,
+        # per build: fill, rasterise, start cell, 3 scans per flood-fill pass, install, census
+        "gpu_launches": steps * (5 + 3 * passes),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if peak else None, "traffic": None, "kernel": "whole build",
                      "peak_source": peak_kind,
