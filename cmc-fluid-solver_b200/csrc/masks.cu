@@ -249,48 +249,62 @@ __global__ void fill_types_kernel(uint8_t *type, long long n, uint8_t v)
         type[c] = v;
 }
 
-// One flood-fill scan along direction DIR: each thread walks one line forward and
-// back; a NODE_IN cell reached from a NODE_OUT cell through NODE_IN cells becomes
-// NODE_OUT.  Threads own disjoint lines.  The walk reads U cells ahead (independent
-// loads) and then runs the sequential rule over them in registers.
+// One flood-fill scan along direction DIR.  Each line is cut into chunks of
+// `chunk` cells; one thread walks one chunk forward and another walks it backward
+// (threads of neighbouring lines are neighbours, so X and Y scans coalesce).  A
+// NODE_IN cell reached from a NODE_OUT cell through NODE_IN cells becomes NODE_OUT;
+// a walk starts reached when the cell just before its chunk (in its direction) is
+// NODE_OUT.  Cells only ever turn from NODE_IN to NODE_OUT, so walks that meet
+// agree, and the passes repeat until one changes nothing: the fixed point is the
+// connected component of the reference's breadth-first search.  Each walk reads
+// U cells ahead (independent loads) before applying the sequential rule to them.
 template <int DIR>
-__global__ void flood_scan_kernel(uint8_t *type, int nx, int ny, int nz, int *changed)
+__global__ void flood_scan_kernel(uint8_t *type, int nx, int ny, int nz, int chunk, int *changed)
 {
     const long long nlines = DIR == 0 ? (long long)ny * nz : (DIR == 1 ? (long long)nx * nz : (long long)nx * ny);
-    const long long line = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (line >= nlines) return;
+    const int len = DIR == 0 ? nx : (DIR == 1 ? ny : nz);
+    const int nch = (len + chunk - 1) / chunk;
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= nlines * nch * 2) return;
+    const long long line = idx % nlines;
+    const long long rest = idx / nlines;
+    const int ch = (int)(rest % nch);
+    const bool bwd = rest >= nch;
     long long base, stride;
-    int len;
-    if (DIR == 0) { base = line; stride = (long long)ny * nz; len = nx; }                               // (j, k)
-    else if (DIR == 1) { base = (line / nz) * (long long)ny * nz + line % nz; stride = nz; len = ny; }  // (i, k)
-    else { base = line * nz; stride = 1; len = nz; }                                                   // (i, j)
+    if (DIR == 0) { base = line; stride = (long long)ny * nz; }                               // (j, k)
+    else if (DIR == 1) { base = (line / nz) * (long long)ny * nz + line % nz; stride = nz; }  // (i, k)
+    else { base = line * nz; stride = 1; }                                                   // (i, j)
+    const int p_lo = ch * chunk, p_hi = min(len, p_lo + chunk) - 1;
     constexpr int U = 8;
     uint8_t *row = type + base;
     bool any = false;
-    bool reach = false;
-    for (int p0 = 0; p0 < len; p0 += U) {
-        uint8_t t[U];
+    if (!bwd) {
+        bool reach = p_lo > 0 && row[(long long)(p_lo - 1) * stride] == NODE_OUT;
+        for (int p0 = p_lo; p0 <= p_hi; p0 += U) {
+            uint8_t t[U];
 #pragma unroll
-        for (int u = 0; u < U; u++) t[u] = (p0 + u < len) ? row[(long long)(p0 + u) * stride] : (uint8_t)NODE_BOUND;
+            for (int u = 0; u < U; u++) t[u] = (p0 + u <= p_hi) ? row[(long long)(p0 + u) * stride] : (uint8_t)NODE_BOUND;
 #pragma unroll
-        for (int u = 0; u < U; u++) {
-            if (t[u] == NODE_OUT) reach = true;
-            else if (t[u] == NODE_IN) {
-                if (reach) { row[(long long)(p0 + u) * stride] = NODE_OUT; any = true; }
-            } else reach = false;
+            for (int u = 0; u < U; u++) {
+                if (t[u] == NODE_OUT) reach = true;
+                else if (t[u] == NODE_IN) {
+                    if (reach) { row[(long long)(p0 + u) * stride] = NODE_OUT; any = true; }
+                } else reach = false;
+            }
         }
-    }
-    reach = false;
-    for (int p1 = len - 1; p1 >= 0; p1 -= U) {
-        uint8_t t[U];
+    } else {
+        bool reach = p_hi < len - 1 && row[(long long)(p_hi + 1) * stride] == NODE_OUT;
+        for (int p1 = p_hi; p1 >= p_lo; p1 -= U) {
+            uint8_t t[U];
 #pragma unroll
-        for (int u = 0; u < U; u++) t[u] = (p1 - u >= 0) ? row[(long long)(p1 - u) * stride] : (uint8_t)NODE_BOUND;
+            for (int u = 0; u < U; u++) t[u] = (p1 - u >= p_lo) ? row[(long long)(p1 - u) * stride] : (uint8_t)NODE_BOUND;
 #pragma unroll
-        for (int u = 0; u < U; u++) {
-            if (t[u] == NODE_OUT) reach = true;
-            else if (t[u] == NODE_IN) {
-                if (reach) { row[(long long)(p1 - u) * stride] = NODE_OUT; any = true; }
-            } else reach = false;
+            for (int u = 0; u < U; u++) {
+                if (t[u] == NODE_OUT) reach = true;
+                else if (t[u] == NODE_IN) {
+                    if (reach) { row[(long long)(p1 - u) * stride] = NODE_OUT; any = true; }
+                } else reach = false;
+            }
         }
     }
     if (any) *changed = 1;
@@ -653,12 +667,16 @@ static cudaError_t flood_fill(uint8_t *types, int nx, int ny, int nz, int *chang
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     int passes = 0;
-    const long long lz = (long long)nx * ny, ly = (long long)nx * nz, lx = (long long)ny * nz;
+    constexpr int CHUNK = 1 << 20;   // whole lines: one forward and one backward walk per line
+    auto threads = [&](long long lines, int len) { return lines * ((len + CHUNK - 1) / CHUNK) * 2; };
+    const long long tz = threads((long long)nx * ny, nz), ty = threads((long long)nx * nz, ny),
+                    tx = threads((long long)ny * nz, nx);
     while (passes < max_passes) {
         if ((e = cudaMemsetAsync(changed, 0, sizeof(int), s)) != cudaSuccess) return e;
-        if (nz > 1) flood_scan_kernel<2><<<(unsigned)((lz + 127) / 128), 128, 0, s>>>(types, nx, ny, nz, changed);
-        flood_scan_kernel<1><<<(unsigned)((ly + 127) / 128), 128, 0, s>>>(types, nx, ny, nz, changed);
-        flood_scan_kernel<0><<<(unsigned)((lx + 127) / 128), 128, 0, s>>>(types, nx, ny, nz, changed);
+        if (nz > 1)
+            flood_scan_kernel<2><<<(unsigned)((tz + 127) / 128), 128, 0, s>>>(types, nx, ny, nz, CHUNK, changed);
+        flood_scan_kernel<1><<<(unsigned)((ty + 127) / 128), 128, 0, s>>>(types, nx, ny, nz, CHUNK, changed);
+        flood_scan_kernel<0><<<(unsigned)((tx + 127) / 128), 128, 0, s>>>(types, nx, ny, nz, CHUNK, changed);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         int h = 0;
         if ((e = cudaMemcpyAsync(&h, changed, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
