@@ -98,7 +98,7 @@ struct adi_handle {
     // adi_adjoint_run calls and grown when a call needs more; freed by adi_destroy
     char *adj_mem = nullptr;
     size_t adj_cap = 0;
-    char *mask_mem = nullptr;   // scratch of the mask builders, kept between builds
+    char *mask_mem = nullptr;   // scratch of the mask builders and adi_get_layer, kept between calls
     size_t mask_cap = 0;
     std::string contract_msg;
     std::string err;
@@ -1030,10 +1030,11 @@ adi_status adi_set_mask(adi_handle *h, const uint8_t *type, const uint8_t *bc_ve
 
 namespace {
 
-// Device scratch of one mask build: pieces of the handle's mask workspace, which
-// grows to the largest build and is kept (a build allocates nothing after the
-// first one of its size).
-struct MaskScratch {
+// Device scratch of one mask build or sampled layer read: pieces of the handle's
+// workspace for these, which grows to the largest request and is kept (a call
+// allocates nothing after the first one of its size).  Every user synchronises
+// the stream before returning, so the next call may reuse the pieces.
+struct HandleScratch {
     adi_handle *h;
     size_t used = 0;
     static size_t round(size_t b) { return (b + 255) / 256 * 256; }
@@ -1111,7 +1112,7 @@ adi_status adi_mask_shape3d(adi_handle *h, const float *verts, int nverts, const
         if (tris[q] < 0 || tris[q] >= nverts)
             return fail(h, ADI_ERR_BAD_ARG, "triangle " + std::to_string(q / 3) + " names a vertex out of range");
     const long long n = h->n;
-    MaskScratch sc{h};
+    HandleScratch sc{h};
     uint8_t *types = nullptr;
     float *dv = nullptr;
     int *dt = nullptr, *st = nullptr;
@@ -1150,7 +1151,7 @@ adi_status adi_mask_sea(adi_handle *h, const float *depth, int depth_nx, int dep
 {
     if (!h || !depth || !in_vel || depth_nx <= 0 || depth_ny <= 0) return ADI_ERR_BAD_ARG;
     const long long n = h->n;
-    MaskScratch sc{h};
+    HandleScratch sc{h};
     uint8_t *snap = nullptr;
     float *dd = nullptr;
     int *st = nullptr;
@@ -1180,7 +1181,7 @@ adi_status adi_mask_extrude2d(adi_handle *h, const uint8_t *type2d, const float 
     const long long cols = (long long)h->nx * h->ny;
     for (long long c = 0; c < cols; c++)
         if (type2d[c] > NODE_VALVE) return fail(h, ADI_ERR_BAD_ARG, "2D node type out of range");
-    MaskScratch sc{h};
+    HandleScratch sc{h};
     uint8_t *t2 = nullptr;
     float *v2 = nullptr, *T2 = nullptr;
     int *st = nullptr;
@@ -1531,35 +1532,23 @@ adi_status adi_get_layer(adi_handle *h, int outdimx, int outdimy, int outdimz, v
     const int l = h->nxt;
     if (h->prec == ADI_FP64) CK(launch_fill_missing<double>(view<double>(h), layer<double>(h, l), h->stream));
     else CK(launch_fill_missing<float>(view<float>(h), layer<float>(h, l), h->stream));
-    const size_t es = esize(h), fb = (size_t)h->n * es;
-    std::vector<unsigned char> host(4 * fb);
-    for (int f = 0; f < 4; f++)
-        CK(cudaMemcpyAsync(host.data() + f * fb, h->d_L[l][f], fb, cudaMemcpyDeviceToHost, h->stream));
+    // point sampling on the device; only the sampled grid crosses to the host
+    const long long m = (long long)outdimx * outdimy * outdimz;
+    const size_t vb = (size_t)m * 3 * esize(h), tbytes = (size_t)m * sizeof(double);
+    HandleScratch sc{h};
+    void *dv = nullptr, *dt = nullptr;
+    CK(sc.reserve({vb, tbytes}));
+    CK(sc.get(&dv, vb));
+    CK(sc.get(&dt, tbytes));
+    if (h->prec == ADI_FP64)
+        CK(launch_sample_layer<double>(clayer<double>(h, l), h->nx, h->ny, h->nz, outdimx, outdimy, outdimz,
+                                       (double *)dv, (double *)dt, h->stream));
+    else
+        CK(launch_sample_layer<float>(clayer<float>(h, l), h->nx, h->ny, h->nz, outdimx, outdimy, outdimz, (float *)dv,
+                                      (double *)dt, h->stream));
+    CK(cudaMemcpyAsync(vout, dv, vb, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(Tout, dt, tbytes, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    // FilterToArrays point sampling (TimeLayer3D.h:869-881)
-    for (int i = 0; i < outdimx; i++)
-        for (int j = 0; j < outdimy; j++)
-            for (int k = 0; k < outdimz; k++) {
-                const long long x = (long long)i * h->nx / outdimx, y = (long long)j * h->ny / outdimy,
-                                z = (long long)k * h->nz / outdimz;
-                const long long src = (x * h->ny + y) * h->nz + z;
-                const long long ind = ((long long)i * outdimy + j) * outdimz + k;
-                if (es == 8) {
-                    const double *H = (const double *)host.data();
-                    double *V = (double *)vout;
-                    V[3 * ind + 0] = H[src];
-                    V[3 * ind + 1] = H[h->n + src];
-                    V[3 * ind + 2] = H[2 * h->n + src];
-                    Tout[ind] = H[3 * h->n + src];
-                } else {
-                    const float *H = (const float *)host.data();
-                    float *V = (float *)vout;
-                    V[3 * ind + 0] = H[src];
-                    V[3 * ind + 1] = H[h->n + src];
-                    V[3 * ind + 2] = H[2 * h->n + src];
-                    Tout[ind] = H[3 * h->n + src];
-                }
-            }
     return ADI_OK;
 }
 

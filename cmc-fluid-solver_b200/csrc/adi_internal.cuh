@@ -157,6 +157,10 @@ cudaError_t launch_div_error(const DomainView<R> &d, CLayer<R> l, R dx, R dy, R 
                              unsigned long long *out_cnt, cudaStream_t s);
 template <typename R>
 cudaError_t launch_fill_missing(const DomainView<R> &d, Layer<R> l, cudaStream_t s);
+// FilterToArrays point sampling onto ox x oy x oz (vout: 3 values per cell, Tout: doubles).
+template <typename R>
+cudaError_t launch_sample_layer(CLayer<R> l, int nx, int ny, int nz, int ox, int oy, int oz, R *vout, double *Tout,
+                                cudaStream_t s);
 // Batch versions: every domain of the batch in one launch (grid y = domain).
 // The divergence partials take nblocks * ndom slots, the results ndom each.
 template <typename R>

@@ -323,6 +323,34 @@ __global__ void fill_missing_kernel(DomainView<R> d, Layer<R> l)
     }
 }
 
+// FilterToArrays point sampling (TimeLayer3D.h:869-881) of a layer onto an
+// ox x oy x oz grid: output cell (i, j, k) takes node (i*nx/ox, j*ny/oy, k*nz/oz);
+// velocity in the layer's precision (3 values per cell), T as double.
+template <typename R>
+__global__ void sample_layer_kernel(CLayer<R> l, int nx, int ny, int nz, int ox, int oy, int oz, R *vout,
+                                    double *Tout)
+{
+    const long long m = (long long)ox * oy * oz;
+    for (long long idx = gtid(); idx < m; idx += gstride()) {
+        const int i = (int)(idx / ((long long)oy * oz)), j = (int)((idx / oz) % oy), k = (int)(idx % oz);
+        const long long x = (long long)i * nx / ox, y = (long long)j * ny / oy, z = (long long)k * nz / oz;
+        const long long src = (x * ny + y) * nz + z;
+        vout[3 * idx + 0] = l.f[0][src];
+        vout[3 * idx + 1] = l.f[1][src];
+        vout[3 * idx + 2] = l.f[2][src];
+        Tout[idx] = (double)l.f[3][src];
+    }
+}
+
+template <typename R>
+cudaError_t launch_sample_layer(CLayer<R> l, int nx, int ny, int nz, int ox, int oy, int oz, R *vout, double *Tout,
+                                cudaStream_t s)
+{
+    const long long m = (long long)ox * oy * oz;
+    sample_layer_kernel<R><<<grid_for(m, 256), 256, 0, s>>>(l, nx, ny, nz, ox, oy, oz, vout, Tout);
+    return cudaGetLastError();
+}
+
 template <typename R>
 cudaError_t launch_update_boundaries(const DomainView<R> &d, Layer<R> cur, cudaStream_t s)
 {
@@ -462,7 +490,9 @@ cudaError_t launch_copy_fields(int nf, const void *const *src, void *const *dst,
     template cudaError_t launch_div_error<R>(const DomainView<R> &, CLayer<R>, R, R, R, double *,                \
                                              unsigned long long *, int, double *, unsigned long long *,          \
                                              cudaStream_t);                                                        \
-    template cudaError_t launch_fill_missing<R>(const DomainView<R> &, Layer<R>, cudaStream_t);
+    template cudaError_t launch_fill_missing<R>(const DomainView<R> &, Layer<R>, cudaStream_t);               \
+    template cudaError_t launch_sample_layer<R>(CLayer<R>, int, int, int, int, int, int, R *, double *,        \
+                                                cudaStream_t);
 INST(float)
 INST(double)
 #undef INST

@@ -246,7 +246,8 @@ adi_status adi_set_state(adi_handle *h, const void *u, const void *v, const void
  * (MISSING_VALUE), then the layer is point-sampled onto an outdimx x outdimy x
  * outdimz grid (0 = full size) at x = i*dimx/outdimx (integer division), etc.
  * v receives 3 interleaved values per point (Vec3D) in the handle's precision,
- * T one double per point. */
+ * T one double per point.  Both steps run on the GPU; only the sampled grid is
+ * copied to the host. */
 adi_status adi_get_layer(adi_handle *h, int outdimx, int outdimy, int outdimz, void *v, double *T);
 
 /* Mean absolute finite-volume divergence of cur over IN cells
