@@ -321,10 +321,11 @@ def run_reference(args):
         from adi_b200 import masks, shapes
         import oracle as O
         dx = cfg["dx"]
-        path = os.path.join(tempfile.mkdtemp(), "sphere.txt")
-        shapes.write_shape3d(path, [shapes.uv_sphere(n_lat=24, n_lon=36) + (None,)])
-        n = int(np.prod(masks.load_shape3d(path, dx, dx, dx).dims))
-        r = O.RefMask.shape3d(path, dx, dx, dx, 1.0)
+        with tempfile.TemporaryDirectory() as tmp:
+            path = os.path.join(tmp, "sphere.txt")
+            shapes.write_shape3d(path, [shapes.uv_sphere(n_lat=24, n_lon=36) + (None,)])
+            n = int(np.prod(masks.load_shape3d(path, dx, dx, dx).dims))
+            r = O.RefMask.shape3d(path, dx, dx, dx, 1.0)
         with stdout_to_stderr():
             t0 = time.perf_counter()
             done = 0
@@ -1040,8 +1041,8 @@ def run_masks(args):
     from adi_b200 import shapes as ms
     cfg = CONFIGS[args.config]
     dx = cfg["dx"]
-    tmp = tempfile.mkdtemp()
-    path = os.path.join(tmp, "sphere.txt")
+    tmpdir = tempfile.TemporaryDirectory()   # removed when the run ends
+    path = os.path.join(tmpdir.name, "sphere.txt")
     ms.write_shape3d(path, [ms.uv_sphere(n_lat=24, n_lon=36) + (None,)])
     sf = masks.load_shape3d(path, dx, dx, dx)
     verts, tris = sf.subframe(0.0)
