@@ -104,6 +104,39 @@ def main():
         out[f"sea_{name}_vel"] = np.array(vel, np.float32)
         out[f"sea_{name}_tin"] = np.array(tin)
         r.close()
+    # the reference's own pipeline from a Shape3D file: its Grid3D::Prepare node grid
+    # stepped by its CPU solver (the GPU test builds the grid with adi_mask_shape3d
+    # from the same vertices and steps it with the exact solver)
+    from adi_b200.geometry import Domain
+    from oracle.oracle import RefSolver
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "sphere.txt")
+        ms.write_shape3d(path, [ms.uv_sphere() + (None,)])
+        dx = 0.025
+        r = RefMask.shape3d(path, dx, dx, dx, BASE_T)
+        r.prepare(0.0)
+        t, bv, bt, vx, vy, vz, T = r.nodes()
+        # the reference leaves the BCs of Shape3D walls unset (whatever the heap held);
+        # they are given the no-slip value that fresh memory holds and the GPU builder
+        # gives a handle without a mask
+        wall = t == 2
+        bv[wall] = 0
+        bt[wall] = 0
+        assert not bv.any() and not bt.any()
+        sf = masks.load_shape3d(path, dx, dx, dx)
+        verts, tris = sf.subframe(0.0)
+        d = Domain(*sf.dims, dx, dx, dx, t, bv, bt, *[a.astype(np.float64) for a in (vx, vy, vz, T)])
+        ref = RefSolver(d, Re=200.0)
+        status, errs = [], []
+        for _ in range(3):
+            status.append(ref.step(2e-4, 4, 2, True))
+            errs.append(ref.div_error())
+        u, v, w, TT = ref.fields(0)
+        ref.close()
+        r.close()
+        out.update({"run_s25_verts": verts, "run_s25_tris": tris, "run_s25_dims": np.array(sf.dims, np.int32),
+                    "run_s25_fields": np.stack([u, v, w, TT]), "run_s25_status": np.array(status, np.int32),
+                    "run_s25_div": np.array(errs), "run_s25_h": np.array([dx, dx, dx])})
     np.savez_compressed(OUT, **out)
     print(OUT, os.path.getsize(OUT), "bytes")
 

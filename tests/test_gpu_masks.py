@@ -195,3 +195,24 @@ def test_shape2d_then_extrusion_matches_reference(adi_lib):
     s = _solver(adi_lib, (nx, ny, nz))
     s.mask_extrude2d(t, v, T, active, float(Z[p3 + "_depth_var"]), 1.0)
     _compare(s.get_mask(), p3)
+
+
+def test_shape3d_file_to_steps_matches_reference_pipeline(adi_lib):
+    """The reference's own pipeline from a Shape3D file -- Grid3D::Prepare then its
+    CPU solver, 3 steps -- against the GPU's: adi_mask_shape3d from the same
+    vertices, then the exact solver.  Fields equal bit for bit on every cell the
+    reference defines (not NODE_OUT; its layers leave those unset)."""
+    from adi_b200 import _abi
+    nx, ny, nz = (int(v) for v in Z["run_s25_dims"])
+    h = float(Z["run_s25_h"][0])
+    box = masks.GridBox(nx, ny, nz, h, h, h)
+    s = adi_lib.AdiSolver3D(box, Re=200.0, solver=_abi.ADI_SOLVER_EXACT)
+    s.mask_shape3d(Z["run_s25_verts"], Z["run_s25_tris"], 1.0)
+    t = s.get_mask()[0]
+    s.CreateSegments()
+    for q in range(3):
+        assert s.step(2e-4, 4, 2, True) == int(Z["run_s25_status"][q])
+        assert abs(s.div_error() - float(Z["run_s25_div"][q])) <= 1e-12 + 1e-9 * abs(float(Z["run_s25_div"][q]))
+    m = t != 1
+    for f, want in zip(s.fields(0), Z["run_s25_fields"]):
+        np.testing.assert_array_equal(f[m].view(np.uint32), want[m].view(np.uint32))
