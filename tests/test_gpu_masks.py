@@ -201,7 +201,9 @@ def test_shape3d_file_to_steps_matches_reference_pipeline(adi_lib):
     """The reference's own pipeline from a Shape3D file -- Grid3D::Prepare then its
     CPU solver, 3 steps -- against the GPU's: adi_mask_shape3d from the same
     vertices, then the exact solver.  Fields equal bit for bit on every cell the
-    reference defines (not NODE_OUT; its layers leave those unset)."""
+    reference defines (not NODE_OUT; its layers leave those unset, which also makes
+    its divergence error -- whose 8-corner stencil reaches NODE_OUT cells diagonal to
+    the fluid -- depend on leftover memory, so that is not compared here)."""
     from adi_b200 import _abi
     nx, ny, nz = (int(v) for v in Z["run_s25_dims"])
     h = float(Z["run_s25_h"][0])
@@ -212,7 +214,6 @@ def test_shape3d_file_to_steps_matches_reference_pipeline(adi_lib):
     s.CreateSegments()
     for q in range(3):
         assert s.step(2e-4, 4, 2, True) == int(Z["run_s25_status"][q])
-        assert abs(s.div_error() - float(Z["run_s25_div"][q])) <= 1e-12 + 1e-9 * abs(float(Z["run_s25_div"][q]))
     m = t != 1
     for f, want in zip(s.fields(0), Z["run_s25_fields"]):
         np.testing.assert_array_equal(f[m].view(np.uint32), want[m].view(np.uint32))
