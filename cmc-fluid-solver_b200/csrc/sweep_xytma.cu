@@ -297,25 +297,65 @@ __global__ void __launch_bounds__(NLT * P, xy_ctas_per_sm((int)sizeof(R), K, NLT
     // nonlinear buffers start each step as copies of cur, and sweeps write only IN
     // nodes), and rows without a matrix row already hold the destination's value;
     // so the whole tile can be stored.
+    if constexpr (sizeof(R) == 4) {
+        // packed FP32: fields (U, T) and (V, W) two at a time, as the elimination left them
+        const float2 xf03 = p2(xf[0], xf[3]), xf12 = p2(xf[1], xf[2]);
+        const float2 xl03 = p2(xl[0], xl[3]), xl12 = p2(xl[1], xl[2]);
 #pragma unroll
-    for (int i = 0; i < K; i++) {
-        const int kd = kind[i];
-        const int tr = i * P + ch;
-        if (kd != R_IN) thm[tr * NLT + li] = wT[tr * WIDE];
-        if (kd == R_NONE) continue;
-#pragma unroll
-        for (int v = 0; v < 4; v++) {
-            const int m = v < 3 ? 0 : 1;
-            R x = i == 0 ? xf[v] : (i == K - 1 ? xl[v] : dv[v][i] - ea[m][i] * xf[v] - ec[m][i] * xl[v]);
-            R *const cslot = tcur + v * fs + tr * NLT + li;
-            if (kd == R_IN) {
-                x += *cslot;
-                const R tv = v == DIR ? wT[tr * WIDE] : tin_of(v)[tr * NLT];
-                R mm = (tv + x) * R(0.5);
-                if (merges == 2) mm = (mm + x) * R(0.5);
-                (v == DIR ? thm : ttin + (v < DIR ? v : v - 1) * fs)[tr * NLT + li] = mm;
+        for (int i = 0; i < K; i++) {
+            const int kd = kind[i];
+            const int tr = i * P + ch;
+            if (kd != R_IN) thm[tr * NLT + li] = wT[tr * WIDE];
+            if (kd == R_NONE) continue;
+            float2 x03, x12;
+            if (i == 0) { x03 = xf03; x12 = xf12; }
+            else if (i == K - 1) { x03 = xl03; x12 = xl12; }
+            else {
+                const float2 nea = p2(-ea[0][i], -ea[1][i]), nec = p2(-ec[0][i], -ec[1][i]);
+                x03 = fma2(nec, xl03, fma2(nea, xf03, p2(dv[0][i], dv[3][i])));
+                x12 = fma2(bc2(nec.x), xl12, fma2(bc2(nea.x), xf12, p2(dv[1][i], dv[2][i])));
             }
-            *cslot = x;
+            R *const c0 = tcur + tr * NLT + li;
+            if (kd == R_IN) {
+                x03 = add2(x03, p2(c0[0], c0[3 * fs]));
+                x12 = add2(x12, p2(c0[fs], c0[2 * fs]));
+                auto tv = [&](int v) -> R { return v == DIR ? wT[tr * WIDE] : tin_of(v)[tr * NLT]; };
+                float2 m03 = mul2(add2(p2(tv(0), tv(3)), x03), bc2(0.5f));
+                float2 m12 = mul2(add2(p2(tv(1), tv(2)), x12), bc2(0.5f));
+                if (merges == 2) {
+                    m03 = mul2(add2(m03, x03), bc2(0.5f));
+                    m12 = mul2(add2(m12, x12), bc2(0.5f));
+                }
+                const float mm[4] = {m03.x, m12.x, m12.y, m03.y};
+#pragma unroll
+                for (int v = 0; v < 4; v++) (v == DIR ? thm : ttin + (v < DIR ? v : v - 1) * fs)[tr * NLT + li] = mm[v];
+            }
+            c0[0] = x03.x;
+            c0[fs] = x12.x;
+            c0[2 * fs] = x12.y;
+            c0[3 * fs] = x03.y;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < K; i++) {
+            const int kd = kind[i];
+            const int tr = i * P + ch;
+            if (kd != R_IN) thm[tr * NLT + li] = wT[tr * WIDE];
+            if (kd == R_NONE) continue;
+#pragma unroll
+            for (int v = 0; v < 4; v++) {
+                const int m = v < 3 ? 0 : 1;
+                R x = i == 0 ? xf[v] : (i == K - 1 ? xl[v] : dv[v][i] - ea[m][i] * xf[v] - ec[m][i] * xl[v]);
+                R *const cslot = tcur + v * fs + tr * NLT + li;
+                if (kd == R_IN) {
+                    x += *cslot;
+                    const R tv = v == DIR ? wT[tr * WIDE] : tin_of(v)[tr * NLT];
+                    R mm = (tv + x) * R(0.5);
+                    if (merges == 2) mm = (mm + x) * R(0.5);
+                    (v == DIR ? thm : ttin + (v < DIR ? v : v - 1) * fs)[tr * NLT + li] = mm;
+                }
+                *cslot = x;
+            }
         }
     }
     tma::cp_async_wait_all();
