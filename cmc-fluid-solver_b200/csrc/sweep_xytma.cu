@@ -185,14 +185,32 @@ __global__ void __launch_bounds__(NLT * P, xy_ctas_per_sm((int)sizeof(R), K, NLT
             // IN rows are never the first or last node of a line
             const R r = tw[1][DIR] * kc.inv_two_h;
             rr[i] = r;
+            R fa, fb;
+            if constexpr (sizeof(R) == 4) {
+                // packed FP32: (U, T) and (V, W) two at a time
+                const float2 lap03 = fma2(bc2(-2.0f), p2(cw[1][0], cw[1][3]), add2(p2(cw[0][0], cw[0][3]),
+                                                                                 p2(cw[2][0], cw[2][3])));
+                const float2 lap12 = fma2(bc2(-2.0f), p2(cw[1][1], cw[1][2]), add2(p2(cw[0][1], cw[0][2]),
+                                                                                 p2(cw[2][1], cw[2][2])));
+                const float2 dif03 = fma2(bc2(-1.0f), p2(cw[0][0], cw[0][3]), p2(cw[2][0], cw[2][3]));
+                const float2 dif12 = fma2(bc2(-1.0f), p2(cw[0][1], cw[0][2]), p2(cw[2][1], cw[2][2]));
+                const float2 d03 = fma2(p2(kc.vis_v, kc.vis_t), lap03, mul2(bc2(-r), dif03));
+                const float2 d12 = fma2(bc2(kc.vis_v), lap12, mul2(bc2(-r), dif12));
+                dv[0][i] = d03.x; dv[3][i] = d03.y; dv[1][i] = d12.x; dv[2][i] = d12.y;
+                const float2 fab = mul2(fma2(bc2(-1.0f), p2(tw[0][0], tw[0][1]), p2(tw[2][0], tw[2][1])),
+                                        bc2(kc.inv_two_h));
+                fa = fab.x;
+                fb = fab.y;
+            } else {
 #pragma unroll
-            for (int v = 0; v < 4; v++) {
-                const R vis = v < 3 ? kc.vis_v : kc.vis_t;
-                dv[v][i] = vis * (cw[0][v] - R(2) * cw[1][v] + cw[2][v]) - r * (cw[2][v] - cw[0][v]);
+                for (int v = 0; v < 4; v++) {
+                    const R vis = v < 3 ? kc.vis_v : kc.vis_t;
+                    dv[v][i] = vis * (cw[0][v] - R(2) * cw[1][v] + cw[2][v]) - r * (cw[2][v] - cw[0][v]);
+                }
+                fa = (tw[2][0] - tw[0][0]) * kc.inv_two_h;
+                fb = (tw[2][1] - tw[0][1]) * kc.inv_two_h;
             }
             dv[DIR][i] -= kc.v_T * ((tw[2][3] - tw[0][3]) * kc.inv_two_h);
-            const R fa = (tw[2][0] - tw[0][0]) * kc.inv_two_h;
-            const R fb = (tw[2][1] - tw[0][1]) * kc.inv_two_h;
             const R fc = (tw[2][2] - tw[0][2]) * kc.inv_two_h;
             const int tr = i * P + ch;
             const R g1 = (thp[tr * NLT + li] - thm[tr * NLT + li]) * (DIR == 0 ? kc.inv_two_dy : kc.inv_two_dx);
