@@ -43,8 +43,11 @@
 // multiply-add, partitioned elimination); the exact sweep is the bit-faithful one.
 //
 // Reciprocals: float uses the hardware approximation (rcp.approx) refined by one
-// Newton-Raphson step r' = r + r (1 - x r); double uses IEEE division.
+// Newton-Raphson step r' = r + r (1 - x r); double uses IEEE division.  The chunk
+// elimination, the cyclic-reduction step and the PCR updates are the shared ones
+// of sweep_common.cuh (packed FP32 in float); the float write-back here is packed too.
 #include "adi_internal.cuh"
+#include "sweep_common.cuh"
 
 #include <climits>
 
@@ -65,19 +68,6 @@ __device__ __forceinline__ int kind_of(uint8_t cm, uint8_t c0, uint8_t cp)
 }
 
 template <typename R>
-__device__ __forceinline__ R rcp(R x)
-{
-    return R(1) / x;
-}
-template <>
-__device__ __forceinline__ float rcp<float>(float x)
-{
-    float r;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return fmaf(r, fmaf(-x, r, 1.0f), r);   // one Newton-Raphson step for 1/x
-}
-
-template <typename R>
 struct Vec4;
 template <>
 struct Vec4<float> {
@@ -87,25 +77,6 @@ template <>
 struct Vec4<double> {
     using T = double2;  // 16 bytes
 };
-
-// Matrix entries of one row of matrix m (velocity or temperature) from the row's
-// kind, advection term r and the matrix's BC code at the node.
-template <typename R>
-__device__ __forceinline__ void row_abc(int kd, R r, bool free_bc, R vis, R b_in, R &a, R &b, R &c)
-{
-    if (kd == K_IN) {
-        a = -r - vis;
-        b = b_in;
-        c = r - vis;
-    } else if (kd == K_NONE) {
-        a = R(0); b = R(1); c = R(0);
-    } else {
-        const bool first = kd != K_END;   // START, or SHARED (Dirichlet by contract)
-        b = free_bc ? R(2) : R(1);
-        a = (!first && free_bc) ? R(-1) : R(0);
-        c = (first && free_bc) ? R(-1) : R(0);
-    }
-}
 
 // Shared-memory slot of value q (0..7) of chunk c of CTA line li in one buffer;
 // conflict-free for the thread mapping of each direction.
@@ -276,83 +247,14 @@ __device__ __forceinline__ void sweep_fast_block(unsigned char *smem_raw, int bu
         }
     }
 
-    // ---------------- 2. chunk elimination ----------------
+    // ---------------- 2. chunk elimination (shared with the X/Y/Z sweeps) ----------------
     // ea[m][i], ec[m][i] (interior rows 1..K-2) end as a'', c''; dv as d''.
     R ea[2][K], ec[2][K];
-    R Af[2], Cf[2], Al[2], Cl[2], Df[4], Dl[4];
-#pragma unroll
-    for (int m = 0; m < 2; m++) {
-        const R vis = m == 0 ? kc.vis_v : kc.vis_t;
-        const R bin = m == 0 ? kc.b_v : kc.b_t;
-        R a0, b0, c0, a1, b1, c1;
-        row_abc<R>(kind[0], rr[0], (freebits >> m) & 1u, vis, bin, a0, b0, c0);
-        row_abc<R>(kind[K - 1], rr[K - 1], (freebits >> (2 * (K - 1) + m)) & 1u, vis, bin, a1, b1, c1);
-        if (K >= 3) {
-#pragma unroll
-            for (int i = 1; i <= K - 2; i++) {
-                R a, b, c;
-                row_abc<R>(kind[i], rr[i], (freebits >> (2 * i + m)) & 1u, vis, bin, a, b, c);
-                if (i == 1) {
-                    const R r = rcp<R>(b);
-                    ea[m][1] = a * r;
-                    ec[m][1] = c * r;
-                    if (m == 0) { dv[0][1] *= r; dv[1][1] *= r; dv[2][1] *= r; }
-                    else dv[3][1] *= r;
-                } else {
-                    const R r = rcp<R>(b - a * ec[m][i - 1]);
-                    if (m == 0) {
-#pragma unroll
-                        for (int v = 0; v < 3; v++) dv[v][i] = (dv[v][i] - a * dv[v][i - 1]) * r;
-                    } else {
-                        dv[3][i] = (dv[3][i] - a * dv[3][i - 1]) * r;
-                    }
-                    ea[m][i] = -a * ea[m][i - 1] * r;
-                    ec[m][i] = c * r;
-                }
-            }
-#pragma unroll
-            for (int i = K - 3; i >= 1; i--) {
-                const R ci = ec[m][i];
-                ea[m][i] -= ci * ea[m][i + 1];
-                if (m == 0) {
-#pragma unroll
-                    for (int v = 0; v < 3; v++) dv[v][i] -= ci * dv[v][i + 1];
-                } else {
-                    dv[3][i] -= ci * dv[3][i + 1];
-                }
-                ec[m][i] = -ci * ec[m][i + 1];
-            }
-            const R rf = rcp<R>(b0 - c0 * ea[m][1]);
-            Af[m] = a0 * rf;
-            Cf[m] = -c0 * ec[m][1] * rf;
-            const R rl = rcp<R>(b1 - a1 * ec[m][K - 2]);
-            Al[m] = -a1 * ea[m][K - 2] * rl;
-            Cl[m] = c1 * rl;
-            if (m == 0) {
-#pragma unroll
-                for (int v = 0; v < 3; v++) {
-                    Df[v] = (dv[v][0] - c0 * dv[v][1]) * rf;
-                    Dl[v] = (dv[v][K - 1] - a1 * dv[v][K - 2]) * rl;
-                }
-            } else {
-                Df[3] = (dv[3][0] - c0 * dv[3][1]) * rf;
-                Dl[3] = (dv[3][K - 1] - a1 * dv[3][K - 2]) * rl;
-            }
-        } else {
-            const R rf = rcp<R>(b0), rl = rcp<R>(b1);
-            Af[m] = a0 * rf;
-            Cf[m] = c0 * rf;
-            Al[m] = a1 * rl;
-            Cl[m] = c1 * rl;
-            if (m == 0) {
-#pragma unroll
-                for (int v = 0; v < 3; v++) { Df[v] = dv[v][0] * rf; Dl[v] = dv[v][K - 1] * rl; }
-            } else {
-                Df[3] = dv[3][0] * rf;
-                Dl[3] = dv[3][K - 1] * rl;
-            }
-        }
-    }
+    sweep::Reduced<R> red;
+    sweep::eliminate<R, K>(kind, rr, freebits, kc, dv, ea, ec, red);
+    const R(&Al)[2] = red.Al;
+    const R(&Cl)[2] = red.Cl;
+    const R(&Dl)[4] = red.Dl;
 
     // ---------------- 3. reduced system of the line ----------------
     // (a) one cyclic-reduction step: remove x_last of chunks ch-1 and ch from the
@@ -366,33 +268,17 @@ __device__ __forceinline__ void sweep_fast_block(unsigned char *smem_raw, int bu
     __syncthreads();
     R ea_[2], ec_[2], ed[4];  // the chunk-first row after the reduction, normalised
     {
-        R pA[2] = {R(0), R(0)}, pC[2] = {R(0), R(0)}, pD[4] = {R(0), R(0), R(0), R(0)};
+        R pv[8] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};
         if (ch > 0) {
-            pA[0] = buf0[slot_of(li, ch - 1, 0)];
-            pC[0] = buf0[slot_of(li, ch - 1, 1)];
-            pA[1] = buf0[slot_of(li, ch - 1, 2)];
-            pC[1] = buf0[slot_of(li, ch - 1, 3)];
 #pragma unroll
-            for (int v = 0; v < 4; v++) pD[v] = buf0[slot_of(li, ch - 1, 4 + v)];
+            for (int q = 0; q < 8; q++) pv[q] = buf0[slot_of(li, ch - 1, q)];
         }
-#pragma unroll
-        for (int m = 0; m < 2; m++) {
-            // row f: Af x_l(ch-1) + x_f + Cf x_l(ch) = Df, with
-            // x_l(ch-1) = pD - pA x_f(ch-1) - pC x_f and x_l(ch) = Dl - Al x_f - Cl x_f(ch+1)
-            const R r = rcp<R>(R(1) - Af[m] * pC[m] - Cf[m] * Al[m]);
-            ea_[m] = -Af[m] * pA[m] * r;
-            ec_[m] = -Cf[m] * Cl[m] * r;
-            if (m == 0) {
-#pragma unroll
-                for (int v = 0; v < 3; v++) ed[v] = (Df[v] - Af[0] * pD[v] - Cf[0] * Dl[v]) * r;
-            } else {
-                ed[3] = (Df[3] - Af[1] * pD[3] - Cf[1] * Dl[3]) * r;
-            }
-        }
+        sweep::cr_step<R>(red, pv, ea_, ec_, ed);
     }
     // (b) parallel cyclic reduction over the P chunk-first unknowns.  Step n
     //     writes buffer (n odd ? buf1 : buf0); the barrier of step n+1 (or of
     //     stage (c)) orders step n's reads before the buffer is written again.
+    //     A partner outside the line contributes zeros.
     int nstep = 0;
     for (int s = 1; s < P; s <<= 1, nstep++) {
         R *bw = (nstep & 1) ? buf0 : buf1;
@@ -403,39 +289,17 @@ __device__ __forceinline__ void sweep_fast_block(unsigned char *smem_raw, int bu
 #pragma unroll
         for (int v = 0; v < 4; v++) bw[slot_of(li, ch, 4 + v)] = ed[v];
         __syncthreads();
-        R mA[2] = {R(0), R(0)}, mC[2] = {R(0), R(0)}, mD[4] = {R(0), R(0), R(0), R(0)};
-        R pA[2] = {R(0), R(0)}, pC[2] = {R(0), R(0)}, pD[4] = {R(0), R(0), R(0), R(0)};
+        R mv[8] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};
+        R pv[8] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};
         if (ch - s >= 0) {
 #pragma unroll
-            for (int m = 0; m < 2; m++) {
-                mA[m] = bw[slot_of(li, ch - s, 2 * m)];
-                mC[m] = bw[slot_of(li, ch - s, 2 * m + 1)];
-            }
-#pragma unroll
-            for (int v = 0; v < 4; v++) mD[v] = bw[slot_of(li, ch - s, 4 + v)];
+            for (int q = 0; q < 8; q++) mv[q] = bw[slot_of(li, ch - s, q)];
         }
         if (ch + s < P) {
 #pragma unroll
-            for (int m = 0; m < 2; m++) {
-                pA[m] = bw[slot_of(li, ch + s, 2 * m)];
-                pC[m] = bw[slot_of(li, ch + s, 2 * m + 1)];
-            }
-#pragma unroll
-            for (int v = 0; v < 4; v++) pD[v] = bw[slot_of(li, ch + s, 4 + v)];
+            for (int q = 0; q < 8; q++) pv[q] = bw[slot_of(li, ch + s, q)];
         }
-#pragma unroll
-        for (int m = 0; m < 2; m++) {
-            const R a = ea_[m], c = ec_[m];
-            const R r = rcp<R>(R(1) - a * mC[m] - c * pA[m]);
-            if (m == 0) {
-#pragma unroll
-                for (int v = 0; v < 3; v++) ed[v] = (ed[v] - a * mD[v] - c * pD[v]) * r;
-            } else {
-                ed[3] = (ed[3] - a * mD[3] - c * pD[3]) * r;
-            }
-            ea_[m] = -a * mA[m] * r;
-            ec_[m] = -c * pC[m] * r;
-        }
+        sweep::pcr_update<R>(mv, pv, ea_, ec_, ed);
     }
     // (c) x_first of this chunk is ed; x_last from its own row and x_first(ch+1)
     R *bx = (nstep & 1) ? buf0 : buf1;
@@ -470,6 +334,14 @@ __device__ __forceinline__ void sweep_fast_block(unsigned char *smem_raw, int bu
         } else if (i == K - 1) {
 #pragma unroll
             for (int v = 0; v < 4; v++) x[v] = xl[v];
+        } else if constexpr (sizeof(R) == 4) {
+            // packed FP32: (U, T) and (V, W) two at a time
+            using namespace sweep;
+            const float2 nea = p2(-ea[0][i], -ea[1][i]), nec = p2(-ec[0][i], -ec[1][i]);
+            const float2 x03 = fma2(nec, p2(xl[0], xl[3]), fma2(nea, p2(xf[0], xf[3]), p2(dv[0][i], dv[3][i])));
+            const float2 x12 =
+                fma2(bc2(nec.x), p2(xl[1], xl[2]), fma2(bc2(nea.x), p2(xf[1], xf[2]), p2(dv[1][i], dv[2][i])));
+            x[0] = x03.x; x[3] = x03.y; x[1] = x12.x; x[2] = x12.y;
         } else {
 #pragma unroll
             for (int v = 0; v < 3; v++) x[v] = dv[v][i] - ea[0][i] * xf[v] - ec[0][i] * xl[v];
@@ -477,13 +349,27 @@ __device__ __forceinline__ void sweep_fast_block(unsigned char *smem_raw, int bu
         }
         const long long off = base + (long long)(p0 + i) * sl;
         if (kd == K_IN) {
+            if constexpr (sizeof(R) == 4) {
+                using namespace sweep;
+                const float2 x03 = add2(p2(cu[0][i + 1], cu[3][i + 1]), p2(x[0], x[3]));
+                const float2 x12 = add2(p2(cu[1][i + 1], cu[2][i + 1]), p2(x[1], x[2]));
+                float2 m03 = mul2(add2(p2(tv[0][i + 1], tv[3][i + 1]), x03), bc2(0.5f));
+                float2 m12 = mul2(add2(p2(tv[1][i + 1], tv[2][i + 1]), x12), bc2(0.5f));
+                if (merges == 2) {
+                    m03 = mul2(add2(m03, x03), bc2(0.5f));
+                    m12 = mul2(add2(m12, x12), bc2(0.5f));
+                }
+                next.f[0][off] = x03.x; next.f[3][off] = x03.y; next.f[1][off] = x12.x; next.f[2][off] = x12.y;
+                tout.f[0][off] = m03.x; tout.f[3][off] = m03.y; tout.f[1][off] = m12.x; tout.f[2][off] = m12.y;
+            } else {
 #pragma unroll
-            for (int v = 0; v < 4; v++) {
-                const R xv = cu[v][i + 1] + x[v];
-                next.f[v][off] = xv;
-                R m = (tv[v][i + 1] + xv) * R(0.5);
-                if (merges == 2) m = (m + xv) * R(0.5);
-                tout.f[v][off] = m;
+                for (int v = 0; v < 4; v++) {
+                    const R xv = cu[v][i + 1] + x[v];
+                    next.f[v][off] = xv;
+                    R m = (tv[v][i + 1] + xv) * R(0.5);
+                    if (merges == 2) m = (m + xv) * R(0.5);
+                    tout.f[v][off] = m;
+                }
             }
         } else {
 #pragma unroll
