@@ -10,8 +10,10 @@
 //   SeaNetCDF (Grid3D::Prepare3D_NetCDF, Grid3D.cpp:966-1075): water columns
 //            from a depth map, the water next to land or air turned into
 //            no-slip walls, and the two far faces into inflow/outflow valves.
-//   Shape2D  (Grid3D::Prepare2D, Grid3D.cpp:608-665): a 2D node grid extruded
-//            in depth with a curved bottom.
+//   Shape2D  (FluidSolver2D::Grid2D::Build, Grid2D.cpp:231-266): a 2D node grid
+//            from polylines (moving ones as valves, fixed ones as walls) and a
+//            flood fill; and Grid3D::Prepare2D (Grid3D.cpp:608-665): a 2D node
+//            grid extruded in depth with a curved bottom.
 //
 // The arithmetic is the reference's FTYPE = float arithmetic step for step:
 // every operation is an explicitly rounded intrinsic (no contraction into FMA,
@@ -24,7 +26,9 @@
 // Parallel structure.  Rasterisation runs one warp per triangle: the scanline
 // walk (a running float sum, hence sequential) is computed by all lanes alike and
 // the cells of each scanline span are split over the lanes; every write stores
-// the same value (NODE_BOUND), so concurrent writers agree.  The flood fill is a
+// the same value (NODE_BOUND), so concurrent writers agree.  2D polylines write
+// data that differ per cell, so there the last write in the reference's order is
+// found first (a claim pass) and then carried out.  The flood fill is a
 // fixed-point iteration of line scans along X, Y and Z, each of which turns a
 // NODE_IN run into NODE_OUT when one of its ends touches a NODE_OUT cell; the fixed
 // point is the connected component the reference's breadth-first search finds.
