@@ -1,5 +1,8 @@
 // Device building blocks shared by the fast sweep kernels (sweep_fast.cu,
-// sweep_zwarp.cu, sweep_xytma.cu).
+// sweep_zwarp.cu, sweep_xytma.cu, sweep_xypair.cu) and the chunked adjoint sweep
+// (adjoint_fast.cu).  In float the chunk elimination, the cyclic-reduction step and
+// the PCR updates run in packed FP32 (sm_100 two-lane FMA/MUL), the velocity and
+// temperature matrices (and the field pairs U,T / V,W) side by side.
 //
 // A chunk is K consecutive rows of one line system.  Row kinds follow the
 // segment structure of Grid3D::GenerateListSegments (Grid3D.cpp:47-127): an IN
