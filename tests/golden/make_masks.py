@@ -137,6 +137,25 @@ def main():
         out.update({"run_s25_verts": verts, "run_s25_tris": tris, "run_s25_dims": np.array(sf.dims, np.int32),
                     "run_s25_fields": np.stack([u, v, w, TT]), "run_s25_status": np.array(status, np.int32),
                     "run_s25_div": np.array(errs), "run_s25_h": np.array([dx, dx, dx])})
+    # the reference's 2D pipeline from a Shape2D file: its Grid2D::Build node grid
+    # stepped by its own 2D solver (float, as shipped)
+    from adi_b200.geometry2d import Domain2D
+    from oracle.oracle import Ref2D
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "moving.txt")
+        ms.write_shape2d(path, None, frames=ms.channel2d_moving())
+        d2 = 0.008
+        r = RefMask.shape2d(path, d2, d2, 0.02, 0.3, 0.4, BASE_T)
+        r.prepare(0.8)
+        t2, v2, T2 = r.grid2d()
+        dom = Domain2D(int(r.dims[0]), int(r.dims[1]), d2, d2, t2, r.last_bc2d, v2[..., 0].astype(np.float64),
+                       v2[..., 1].astype(np.float64), T2.astype(np.float64), startT=BASE_T)
+        ref2 = Ref2D(dom, Re=100.0)
+        for _ in range(3):
+            ref2.step(1e-3, 2, 1)
+        out["run2d_fields"] = np.stack(ref2.fields(0))
+        ref2.close()
+        r.close()
     np.savez_compressed(OUT, **out)
     print(OUT, os.path.getsize(OUT), "bytes")
 
