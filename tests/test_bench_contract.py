@@ -1,6 +1,6 @@
 """The reference arm of bench.py on the CPU: one JSON line with the keys the
 benchmark contract needs (metric, value, unit, impl, cpu_baseline, e2e), for a
-3D and the 2D workload.  The arm times the reference's own CPU solver built from
+3D, the 2D and the mask-builder workload.  The arm times the reference's own CPU solver built from
 its sources (oracle/_ref); without that build the test is skipped."""
 import json
 import os
@@ -38,3 +38,15 @@ def test_reference_arm_json(config, lib):
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
     assert d["e2e"]["value"] == d["value"]
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+
+
+def test_reference_arm_json_masks():
+    """The mask-builder workload's reference arm: the reference's own Grid3D::Prepare,
+    timed in cells per second."""
+    if not os.path.exists(REF3D):
+        pytest.skip("the reference build (oracle/_ref) is not present")
+    d = _reference_line("masks262")
+    assert d["impl"] == "reference" and d["metric"] == "cells/s" and d["unit"] == "cells/s"
+    assert d["value"] > 0 and d["steps"] >= 1 and d["config"]["cells"] == 262 * 262 * 264
+    assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["value"] == d["value"]
+    assert d["e2e"]["value"] == d["value"]
