@@ -18,7 +18,7 @@ bit-identical to those the reference's ``Grid3D::Build`` receives:
 * ``sea_geometry``   the grid size and bbox.pMin.z that Grid3D::LoadNetCDF derives
   from the latitudes, longitudes and depths of a bathymetry file
   (Grid3D.cpp:437-486).  Reading the NetCDF-4 file itself needs libnetcdf, which
-  this build does not link; the caller passes the arrays.
+  libadi_b200 does not link; the caller passes the arrays.
 * ``extrude_dims``   the depth levels of a 2D shape extruded in depth
   (Grid3D::LoadFromFile, Grid3D.cpp:497-509).
 * ``load_shape2d`` / ``Shape2DFrames.subframe`` / ``build_shape2d``   a Shape2D file
