@@ -38,7 +38,6 @@
 #include "adi_internal.cuh"
 
 #include <climits>
-#include <mutex>
 
 namespace adi {
 
@@ -302,9 +301,28 @@ __global__ void __launch_bounds__(128)
         return (uint8_t)(ntype[off] | (nbcv[off] == BC_FREE ? CODE_VEL_FREE : 0) |
                          (nbct[off] == BC_FREE ? CODE_TEMP_FREE : 0));
     };
+    // Caller-owned masks are not checked on the host the way adi_set_mask checks
+    // them, so a line that breaks the solver contract where it would make a read
+    // leave the arrays -- a NODE_IN cell at either end of the line, or any NODE_IN
+    // cell in a line on the outer frame (its off-line stencil crosses the face) --
+    // is skipped whole: its nodes are neither read as rows nor written.
+    bool usable = valid;
+    if (valid) {
+        int c1, c2, n1, n2;   // the line's two fixed coordinates and their extents
+        if (DIR == 0) { c1 = line / g.nz; c2 = line % g.nz; n1 = g.ny; n2 = g.nz; }
+        else if (DIR == 1) { c1 = line / g.nz; c2 = line % g.nz; n1 = g.nx; n2 = g.nz; }
+        else { c1 = line / g.ny; c2 = line % g.ny; n1 = g.nx; n2 = g.ny; }
+        const bool on_frame = c1 == 0 || c1 == n1 - 1 || c2 == 0 || c2 == n2 - 1;
+        const bool end_in = ntype[base] == NODE_IN || ntype[base + (long long)(g.len - 1) * sl] == NODE_IN;
+        if (end_in) usable = false;
+        if (on_frame) {
+            for (int q = 1; q + 1 < g.len && usable; q++)
+                if (ntype[base + (long long)q * sl] == NODE_IN) usable = false;
+        }
+    }
     // segment range of the line, by the rule of Grid3D::GenerateListSegments
     int lo = INT_MAX, hi = -1;
-    if (valid) {
+    if (usable) {
         int state = 0, start = 0;
         for (int q = 0; q + 1 < g.len; q++) {
             const bool in = ntype[base + (long long)(q + 1) * sl] == NODE_IN;
@@ -322,7 +340,7 @@ __global__ void __launch_bounds__(128)
     const unsigned full = 0xffffffffu;
     const int wlo = __reduce_min_sync(full, lo);
     const int whi = __reduce_max_sync(full, hi);
-    if (!valid || hi < 0) return;
+    if (!usable || hi < 0) return;
 
     const long long sx = (long long)g.ny * g.nz, sy = g.nz;
     const long long so1 = DIR == 0 ? sy : sx;
@@ -436,24 +454,18 @@ __global__ void __launch_bounds__(128)
 
 namespace {
 
-// Device address of g_static_scratch per device, looked up once per device.
-std::mutex g_static_mu;
-void *g_static_ptr[64] = {};
-
+// Device address of g_static_scratch in the current device's context.  Host code
+// cannot pass the symbol itself (its host-side name is a stand-in, not a device
+// address), so every call looks the address up with the device current; the
+// lookup is a host-side table read once the module is loaded, and looking it up
+// each time keeps it right after a device reset or in another driver context.
+// The first lookup on a device loads the module.
 cudaError_t static_scratch(void **out)
 {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lk(g_static_mu);
-    if (!g_static_ptr[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_static_scratch);
-        if (e != cudaSuccess) return e;
-        g_static_ptr[dev] = p;
-    }
-    *out = g_static_ptr[dev];
+    *out = p;
     return cudaSuccess;
 }
 
@@ -501,7 +513,9 @@ adi_status static_sweep(const adi_static_sweep_args *a, void *scratch)
         else if (a->dir == 1) SL(1);
         else SL(2);
 #undef SL
-        if (cudaGetLastError() != cudaSuccess) return ADI_ERR_CUDA;
+        // peek, not get: a launch error stays pending for the caller's own
+        // cudaGetLastError (this entry point has no handle to carry a message)
+        if (cudaPeekAtLastError() != cudaSuccess) return ADI_ERR_CUDA;
     }
     return ADI_OK;
 }
@@ -520,6 +534,8 @@ extern "C" adi_status adi_sweep_exact_static(const adi_static_sweep_args *a)
     for (int v = 0; v < 4; v++)
         if (!a->node_value[v] || !a->cur[v] || !a->temp_in[v] || !a->next[v] || !a->temp_out[v])
             return ADI_ERR_BAD_ARG;
+    // an error left pending by earlier work is the caller's: report it, keep it
+    if (cudaPeekAtLastError() != cudaSuccess) return ADI_ERR_CUDA;
     void *scratch = nullptr;
     if (static_scratch(&scratch) != cudaSuccess) return ADI_ERR_CUDA;
     if (a->precision == ADI_FP64) return static_sweep<double>(a, scratch);

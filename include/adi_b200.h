@@ -477,14 +477,26 @@ const char *adi_batch_last_error_string(const adi_batch *b);
  *     same thread, so nothing needs clearing.  Calls whose work overlaps on the GPU
  *     (different streams, or different host threads on one device) race on the
  *     array: serialise them, e.g. issue them on one stream.
- *   - the first call on a device looks up the array's device address
- *     (cudaGetSymbolAddress) with that device current; make that first call
- *     before any stream capture.
+ *   - every call looks up the array's device address (cudaGetSymbolAddress)
+ *     with the caller's device current, so it stays right after a device reset
+ *     or in a non-primary driver context; the first call on a device also loads
+ *     the library's module there, so make that first call before any stream
+ *     capture.
  * All pointers are device pointers in the precision's element type, except the
  * three uint8 node arrays (Grid3D Node SoA).  temp_in and temp_out must not
  * alias each other or cur; next must not alias cur or temp_in.  merges is 1, or 2
  * for the sweep that also carries the per-iteration extra merge.  Asynchronous
- * on `stream`. */
+ * on `stream`.
+ * The node arrays should meet adi_set_mask's solver contract (no NODE_IN cell on
+ * the outer frame or next to NODE_OUT, no BC_FREE cell between two fluid runs of
+ * a line); they are not checked on the host.  Lines whose rows would read outside
+ * the arrays -- a NODE_IN cell at either end of the line, or any NODE_IN cell in a
+ * line on the outer frame -- are skipped by the kernel (left unwritten); other
+ * violations give the reference's arithmetic on the given mask.
+ * Errors: ADI_ERR_BAD_ARG, ADI_ERR_CAPACITY, or ADI_ERR_CUDA when a CUDA error is
+ * pending before the call or a launch fails.  There is no handle and so no
+ * message string; the CUDA error is left pending for the caller's
+ * cudaGetLastError. */
 typedef struct adi_static_sweep_args {
     int dir;                  /* ADI_X, ADI_Y or ADI_Z */
     int dimx, dimy, dimz;
