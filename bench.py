@@ -16,7 +16,15 @@ e2e    : the same K steps through the C ABI with host buffers: each step uploads
          the state from pinned host memory (adi_set_state), steps, and reads the
          result back (adi_get_state).
 roofline: the sweep kernels (the dominant class), algorithmic bytes per launch /
-         their CUDA-event time, against the measured HBM copy bandwidth.
+         their CUDA-event time, against the measured HBM copy bandwidth.  The
+         per-kernel times come from a second pass over the same steps with the
+         library's per-launch CUDA events on (direct launches, an event pair
+         around each); those events sit between launches, so the per-class sum
+         runs a few percent above the graph-replayed ms_per_step and the
+         achieved GB/s are a lower bound.
+accuracy: max relative field error of 10 FP32 steps (the timed path) against 10
+         steps of the FP64 CPU oracle (the C restatement of the reference's step,
+         oracle/), computed after the timed region on rank 0.
 cpu_baseline: the reference's own CPU solver (oracle/_ref/libref3d.so, compiled
          from its sources) on the same workload on this host's cores (rank 0, N=1).
 
@@ -114,6 +122,32 @@ CONFIGS = {
                       desc="small case for profiling: 64^3 FP32, 10 spheres, Re=200, dt=5e-4, "
                            "num_global=4, num_local=2"),
 }
+
+
+# What both arms print under "config": the workload and how the L2 is treated
+# between timed steps, identical in the GPU line and the reference line so that the
+# two name the same workload; the details of one arm's run go under "run".
+L2_POLICY = {
+    "single": "GPU arm: L2 flushed between timed steps (256 MiB memset, excluded from the time); "
+              "reference arm: the host CPU",
+    "batch": "GPU arm: L2 flushed between timed steps (256 MiB memset, excluded from the time), working set "
+             "far above L2; reference arm: the host CPU",
+    "adjoint": "GPU arm: working set (tape of 8 steps) far above L2; reference arm: the host CPU",
+    "2d": "GPU arm: the whole 2D state (under 3 MB) stays in L2, one graph launch per step; reference arm: the "
+          "host CPU",
+    "masks": "GPU arm: 256 MiB written between builds (L2 flushed); reference arm: the host CPU",
+}
+
+
+def workload_kind(cfg) -> str:
+    for k in ("batch", "adjoint", "masks"):
+        if cfg.get(k):
+            return k
+    return "2d" if cfg.get("two_d") else "single"
+
+
+def workload_config(args, cfg, cells) -> dict:
+    return {"workload": f"{args.config}: {cfg['desc']}", "cells": int(cells), "l2": L2_POLICY[workload_kind(cfg)]}
 
 
 def measured_peaks():
@@ -311,7 +345,7 @@ def run_reference(args):
             "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
             "steps": done, "warmup": args.warmup, "ms_per_step": 1e3 * el / done, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{args.config}: {cfg['desc']}", "cells": d.cells},
+            "config": workload_config(args, cfg, d.cells),
             "cpu_baseline": {"value": value, "unit": METRIC, "cores": 1, "kind": "reference",
                              "sample": f"{done} steps ({el:.1f} s), the reference 2D solver (single-threaded)"},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -338,7 +372,7 @@ def run_reference(args):
             "impl": "reference", "metric": "cells/s", "value": value, "unit": "cells/s", "n_gpus": world,
             "steps": done, "warmup": 0, "ms_per_step": 1e3 * el / done, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{args.config}: {cfg['desc']}", "cells": n},
+            "config": workload_config(args, cfg, n),
             "cpu_baseline": {"value": value, "unit": "cells/s", "cores": 1, "kind": "reference",
                              "sample": f"{done} full Grid3D::Prepare builds ({el:.1f} s), single-threaded as written"},
             "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -354,7 +388,7 @@ def run_reference(args):
             "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
             "steps": 1, "warmup": 0, "ms_per_step": 1e3 * el, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{args.config}: {cfg['desc']}", "cells": sum(d.cells for d in domains)},
+            "config": workload_config(args, cfg, sum(d.cells for d in domains)),
             "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }), flush=True)
@@ -370,7 +404,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
         "steps": done, "warmup": args.warmup, "ms_per_step": 1e3 * el / done, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{args.config}: {cfg['desc']}", "cells": d.cells},
+        "config": workload_config(args, cfg, d.cells),
         "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "reference",
                          "sample": f"{done} full steps of {args.config} ({el:.1f} s), OpenMP {cores} threads"},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -495,12 +529,11 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{args.config}: {cfg['desc']}", "cells": d.cells,
-                   "segments_xyz": stats["num_segments"], "segment_nodes_xyz": stats["num_nodes"],
-                   "solver": args.solver, "fast_shapes": shapes if args.solver == "fast" else None,
-                   "parallelism": f"replicas x{world}" if world > 1 else "single domain",
-                   "l2": "flushed between steps (256 MiB memset, excluded from the time)",
-                   "algorithmic_bytes_per_step": step_bytes},
+        "config": workload_config(args, cfg, d.cells),
+        "run": {"segments_xyz": stats["num_segments"], "segment_nodes_xyz": stats["num_nodes"],
+                "solver": args.solver, "fast_shapes": shapes if args.solver == "fast" else None,
+                "parallelism": f"replicas x{world}" if world > 1 else "single domain",
+                "algorithmic_bytes_per_step": step_bytes},
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes,
                 "steps": e2e_steps},
         "gpu_launches": launches,
@@ -742,11 +775,10 @@ def run_batch(args):
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{args.config}: {cfg['desc']}", "cells": all_cells, "domains": len(domains),
-                   "domains_this_rank": len(mine), "chunk_K_xyz": batch.chunks(),
-                   "parallelism": (f"domains LPT-sharded over {world} ranks (loads "
-                                   f"{[int(x) for x in part_loads(costs, parts)]})" if world > 1 else "one batch"),
-                   "l2": "flushed between steps (256 MiB memset, excluded from the time); working set far above L2"},
+        "config": workload_config(args, cfg, all_cells),
+        "run": {"domains": len(domains), "domains_this_rank": len(mine), "chunk_K_xyz": batch.chunks(),
+                "parallelism": (f"domains LPT-sharded over {world} ranks (loads "
+                                f"{[int(x) for x in part_loads(costs, parts)]})" if world > 1 else "one batch")},
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 16 * my_cells,
                 "d2h_bytes_per_step": 16 * my_cells, "steps": e2e_steps},
         "gpu_launches": launches,
@@ -875,9 +907,8 @@ def run_adjoint(args):
         "metric": METRIC, "value": d.cells * ns / (adj_ms / 1e3), "unit": METRIC, "n_gpus": 1, "steps": ns,
         "warmup": args.warmup, "ms_per_step": adj_ms / ns, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{args.config}: {cfg['desc']}", "cells": d.cells, "checkpoint_every": ck,
-                   "l2": "working set (tape of 8 steps, 12 GB) far above L2",
-                   "workspace": "allocated by the warm-up adjoint call and kept by the handle"},
+        "config": workload_config(args, cfg, d.cells),
+        "run": {"checkpoint_every": ck, "workspace": "allocated by the warm-up adjoint call and kept by the handle"},
         "adjoint_over_forward": adj_ms / fwd_ms, "forward_ms": fwd_ms, "adjoint_ms": adj_ms,
         "J": J, "grad_theta_far_box_max_abs": float(np.max(np.abs(g_far))),
         "grad_check": {"box": cfg["near_box"], "J": Jn, "max_rel_err_vs_fp64_central_fd": rel, "fd_h": 1e-3,
@@ -986,10 +1017,8 @@ def run_2d(args):
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": steps, "warmup": args.warmup,
         "ms_per_step": total_ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{args.config}: {cfg['desc']}", "cells": d.cells,
-                   "global_iterations_per_step": mean_iters,
-                   "l2": "the whole 2D state (under 3 MB) stays in L2; each step is one graph launch and one "
-                         "read of the iteration errors"},
+        "config": workload_config(args, cfg, d.cells),
+        "run": {"global_iterations_per_step": mean_iters},
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 3 * 8 * d.cells,
                 "d2h_bytes_per_step": 3 * 8 * d.cells, "steps": e2e_steps},
         "gpu_launches": None,
@@ -1099,8 +1128,8 @@ def run_masks(args):
         "metric": "cells/s", "value": value, "unit": "cells/s", "n_gpus": world, "steps": steps,
         "warmup": args.warmup, "ms_per_step": total_ms / steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{args.config}: {cfg['desc']}", "cells": n, "triangles": int(len(tris)),
-                   "flood_fill_passes": passes, "l2": "256 MiB written between builds (L2 flushed)"},
+        "config": workload_config(args, cfg, n),
+        "run": {"triangles": int(len(tris)), "flood_fill_passes": passes},
         "e2e": {"value": n * e2e_steps / e2e_s, "unit": "cells/s", "h2d_bytes_per_step": int(verts.nbytes + tris.nbytes),
                 "d2h_bytes_per_step": int(sum(a.nbytes for a in got)), "steps": e2e_steps,
                 "note": "adi_mask_shape3d from host vertices, then adi_get_mask of the whole node grid "

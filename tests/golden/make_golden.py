@@ -2,7 +2,7 @@
 solver (oracle/_ref/libref3d.so, compiled from the reference sources by
 oracle/Makefile).  Run on a machine that has the reference checkout:
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle REF=<reference checkout>/src && python tests/golden/make_golden.py
 
 Each case stores the synthetic inputs (node arrays), the reference's segment lists
 for X, Y, Z, and its fields after selected steps of the driver loop
