@@ -550,8 +550,8 @@ def run_ours(args):
                                stream.cuda_stream, shp)
         line["accuracy"] = {"max_rel_err_vs_fp64": err, "steps": acc_steps, "bound": 1e-5,
                             "within_bound": max(err.values()) <= 1e-5,
-                            "reference": "the FP64 fast path from the same state (equal to the FP64 CPU oracle to "
-                                         "1e-11 in the tests)"}
+                            "reference": "the FP64 CPU oracle (C restatement of the reference's step) from the "
+                                         "same state"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
         with stdout_to_stderr():
@@ -568,34 +568,46 @@ def run_ours(args):
     return 0
 
 
-def accuracy_vs_fp64(d, Re, Pr, lam, dt, ng, nl, steps, solver_kind, stream, shapes=None):
-    """Max relative field error over the IN cells, per field (u, v, w, T), of `steps`
-    FP32 steps against FP64 steps of the same domain from the same state:
-    max|x32 - x64| / max|x64|.  The FP64 side is the fast FP64 path, which equals the
-    FP64 CPU oracle to 1e-11 of each field's scale in tests/test_gpu_fast.py; the CPU
-    oracle itself would take minutes at these sizes."""
-    import adi_b200
-    sides = []
-    for prec in (adi_b200.ADI_FP32, adi_b200.ADI_FP64):
-        s = adi_b200.AdiSolver3D(d, Re=Re, Pr=Pr, lam=lam, precision=prec,
-                                 solver=solver_kind if prec == adi_b200.ADI_FP32 else adi_b200.ADI_SOLVER_FAST,
-                                 stream=stream)
-        s.CreateSegments()
-        if shapes and prec == adi_b200.ADI_FP32:
-            for dr, (K, NL) in enumerate(shapes):
-                s.set_fast_shape(dr, K, NL)
-        for _ in range(steps):
-            rc = s.step(dt, ng, nl, False)
-            if rc != 0:
-                raise RuntimeError(f"adi_step failed with status {rc}")
-        sides.append([f.astype(np.float64) for f in s.fields(0)])
-        s.close()
+def _oracle64_fields(d, Re, Pr, lam, dt, ng, nl, steps):
+    """The FP64 CPU oracle (the C restatement of the reference's step, oracle/) after
+    `steps` driver steps from the domain's initial state.  Used only as the checker."""
+    import oracle as O
+    o = O.OracleSolver(d, precision=8, params=O.fluid_params_normalized(Re, Pr, lam))
+    for _ in range(steps):
+        if o.step(dt, ng, nl, False) != 0:
+            raise RuntimeError("the FP64 oracle diverged")
+    out = o.fields(0)
+    o.close()
+    return out
+
+
+def _max_rel(x32, x64, d):
     m = d.type == G.NODE_IN
     out = {}
-    for name, a, b in zip("uvwT", sides[0], sides[1]):
+    for name, a, b in zip("uvwT", x32, x64):
         scale = float(np.max(np.abs(b[m])))
-        out[name] = float(np.max(np.abs(a[m] - b[m]))) / (scale if scale > 0 else 1.0)
+        out[name] = float(np.max(np.abs(a[m].astype(np.float64) - b[m]))) / (scale if scale > 0 else 1.0)
     return out
+
+
+def accuracy_vs_fp64(d, Re, Pr, lam, dt, ng, nl, steps, solver_kind, stream, shapes=None):
+    """Max relative field error over the IN cells, per field (u, v, w, T), of `steps`
+    FP32 steps of the timed path against the FP64 CPU oracle from the same state:
+    max|x32 - x64| / max|x64|."""
+    import adi_b200
+    s = adi_b200.AdiSolver3D(d, Re=Re, Pr=Pr, lam=lam, precision=adi_b200.ADI_FP32, solver=solver_kind,
+                             stream=stream)
+    s.CreateSegments()
+    if shapes:
+        for dr, (K, NL) in enumerate(shapes):
+            s.set_fast_shape(dr, K, NL)
+    for _ in range(steps):
+        rc = s.step(dt, ng, nl, False)
+        if rc != 0:
+            raise RuntimeError(f"adi_step failed with status {rc}")
+    x32 = s.fields(0)
+    s.close()
+    return _max_rel(x32, _oracle64_fields(d, Re, Pr, lam, dt, ng, nl, steps), d)
 
 
 def accuracy_batch_member(d, Re, Pr, lam, dt, ng, nl, steps, chunks, stream):
@@ -612,23 +624,10 @@ def accuracy_batch_member(d, Re, Pr, lam, dt, ng, nl, steps, chunks, stream):
         rc = b.step(dt, ng, nl, False)
         if rc != 0:
             raise RuntimeError(f"adi_batch_step failed with status {rc}: {b.last_error()}")
-    x32 = [f.astype(np.float64) for f in m.fields(0)]
+    x32 = m.fields(0)
     b.close()
     m.close()
-    s64 = adi_b200.AdiSolver3D(d, Re=Re, Pr=Pr, lam=lam, precision=adi_b200.ADI_FP64, stream=stream)
-    s64.CreateSegments()
-    for _ in range(steps):
-        rc = s64.step(dt, ng, nl, False)
-        if rc != 0:
-            raise RuntimeError(f"adi_step failed with status {rc}")
-    x64 = s64.fields(0)
-    s64.close()
-    msk = d.type == G.NODE_IN
-    out = {}
-    for name, a, c in zip("uvwT", x32, x64):
-        scale = float(np.max(np.abs(c[msk])))
-        out[name] = float(np.max(np.abs(a[msk] - c[msk]))) / (scale if scale > 0 else 1.0)
-    return out
+    return _max_rel(x32, _oracle64_fields(d, Re, Pr, lam, dt, ng, nl, steps), d)
 
 
 def cpu_reference_batch(domains, cfg, budget_s: float):
@@ -798,8 +797,8 @@ def run_batch(args):
                                     stream.cuda_stream)
         line["accuracy"] = {"max_rel_err_vs_fp64": err, "steps": acc_steps, "bound": 1e-5,
                             "within_bound": max(err.values()) <= 1e-5, "domain": list(d0.shape),
-                            "reference": "one member stepped through the batched path against the FP64 fast path "
-                                         "from the same state (equal to the FP64 CPU oracle to 1e-11 in the tests)"}
+                            "reference": "one member stepped through the batched path against the FP64 CPU oracle "
+                                         "(C restatement of the reference's step) from the same state"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
         with stdout_to_stderr():
