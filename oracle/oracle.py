@@ -55,6 +55,7 @@ def _load_ref():
         lib.ref_set_state.argtypes = [C.c_void_p] + [_f32p] * 4
         lib.ref_div_error.restype = C.c_double
         lib.ref_div_error.argtypes = [C.c_void_p]
+        lib.ref_get_layer.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, _f32p, _f64p]
         lib.ref_destroy.argtypes = [C.c_void_p]
         vp, i, d = C.c_void_p, C.c_int, C.c_double
         lib.ref_shape3d_load.restype = vp
@@ -166,6 +167,17 @@ class RefSolver:
     def div_error(self) -> float:
         return self.lib.ref_div_error(self.h)
 
+    def get_layer(self, outdimx=0, outdimy=0, outdimz=0):
+        """Solver3D::GetLayer (Solver3D.cpp:21-25): velocities [ox, oy, oz, 3] (float)
+        and T [ox, oy, oz] (double); it also sets the OUT cells of next to 99999."""
+        ox, oy, oz = outdimx or self.shape[0], outdimy or self.shape[1], outdimz or self.shape[2]
+        v = np.zeros((ox, oy, oz, 3), np.float32)
+        T = np.zeros((ox, oy, oz), np.float64)
+        rc = self.lib.ref_get_layer(self.h, outdimx, outdimy, outdimz, v, T)
+        if rc != 0:
+            raise RuntimeError(f"ref_get_layer failed ({rc})")
+        return v, T
+
     def close(self):
         if self.h:
             self.lib.ref_destroy(self.h)
@@ -176,6 +188,34 @@ class RefSolver:
             self.close()
         except Exception:
             pass
+
+
+ADAPTER_LIB = os.path.join(HERE, "_ref", "libadapter3d.so")
+
+
+def have_adapter() -> bool:
+    return os.path.exists(ADAPTER_LIB)
+
+
+def adapter_run(d, Re, Pr, lam, dt, num_global, num_local, steps, solver_kind, outdims=(0, 0, 0)):
+    """The reference driver loop through the B200AdiSolver3D host adapter
+    (oracle/adapter_harness.cpp, built against the reference's headers): returns
+    GetLayer's velocities [ox, oy, oz, 3] (float) and T [ox, oy, oz] (double) after
+    `steps` steps."""
+    lib = C.CDLL(ADAPTER_LIB)
+    lib.adapter_run.argtypes = ([C.c_int] * 3 + [C.c_double] * 3 + [_u8p] * 3 + [_f32p] * 4 + [C.c_double] * 4 +
+                                [C.c_int] * 7 + [_f32p, _f64p, C.c_char_p, C.c_int])
+    t, bv, bt, vx, vy, vz, T = d.arrays()
+    f = [np.ascontiguousarray(a, np.float32) for a in (vx, vy, vz, T)]
+    ox, oy, oz = (o or s for o, s in zip(outdims, d.shape))
+    vout = np.zeros((ox, oy, oz, 3), np.float32)
+    Tout = np.zeros((ox, oy, oz), np.float64)
+    err = C.create_string_buffer(512)
+    rc = lib.adapter_run(d.nx, d.ny, d.nz, d.dx, d.dy, d.dz, t, bv, bt, *f, Re, Pr, lam, dt, num_global, num_local,
+                         steps, solver_kind, outdims[0], outdims[1], outdims[2], vout, Tout, err, len(err))
+    if rc != 0:
+        raise RuntimeError(f"adapter_run failed ({rc}): {err.value.decode(errors='replace')}")
+    return vout, Tout
 
 
 class OracleSolver:

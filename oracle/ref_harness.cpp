@@ -323,6 +323,25 @@ int ref_set_state(void *vh, const float *u, const float *v, const float *w, cons
 
 // Mean absolute finite-volume divergence of cur (TimeLayer3D::EvalDivError,
 // TimeLayer3D.h:595-641).
+// Solver3D::GetLayer (Solver3D.cpp:21-25) of the reference solver: v gets 3 floats
+// per output point, T one double.
+int ref_get_layer(void *vh, int outdimx, int outdimy, int outdimz, float *v, double *T)
+{
+	RefHandle *h = (RefHandle *)vh;
+	if (h->solver == NULL) return -2;
+	const size_t m = (size_t)(outdimx ? outdimx : h->grid->dimx) * (outdimy ? outdimy : h->grid->dimy) *
+	                 (outdimz ? outdimz : h->grid->dimz);
+	std::vector<Vec3D> vel(m);
+	h->solver->GetLayer(vel.data(), T, outdimx, outdimy, outdimz);
+	for (size_t i = 0; i < m; i++)
+	{
+		v[3 * i] = vel[i].x;
+		v[3 * i + 1] = vel[i].y;
+		v[3 * i + 2] = vel[i].z;
+	}
+	return 0;
+}
+
 double ref_div_error(void *vh)
 {
 	RefHandle *h = (RefHandle *)vh;
