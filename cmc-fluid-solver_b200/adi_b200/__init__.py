@@ -71,6 +71,10 @@ class AdiSolver3D:
     def set_solver(self, kind: int):
         self._check(self.lib.adi_set_solver(self.h, kind))
 
+    def set_fault_injection(self, what: int):
+        """adi_set_fault_injection: test-only failure modes (ADI_FAULT_*)."""
+        self._check(self.lib.adi_set_fault_injection(self.h, what))
+
     def close(self):
         if self.h:
             self.lib.adi_destroy(self.h)

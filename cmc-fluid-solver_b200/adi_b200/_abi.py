@@ -21,6 +21,7 @@ STATUS_NAMES = {
 globals().update({name: code for code, name in STATUS_NAMES.items()})
 ADI_FP32, ADI_FP64 = 4, 8
 ADI_SOLVER_EXACT, ADI_SOLVER_FAST = 0, 1
+ADI_FAULT_NONE, ADI_FAULT_SKIP_TILE_LOADS = 0, 1
 
 # every entry point include/adi_b200.h declares
 EXPORTED = [
@@ -38,6 +39,7 @@ EXPORTED = [
     "adi2d_update_boundaries", "adi2d_time_step", "adi2d_step", "adi2d_get_state", "adi2d_set_state",
     "adi2d_get_layer", "adi2d_last_error", "adi2d_last_error_string",
     "adi_mask_shape3d", "adi_mask_sea", "adi_mask_extrude2d", "adi_get_mask", "adi_mask_shape2d",
+    "adi_set_fault_injection",
 ]
 
 K_NUM = 7
@@ -96,6 +98,7 @@ def load() -> C.CDLL:
         "adi_destroy": [vp],
         "adi_set_stream": [vp, vp],
         "adi_set_solver": [vp, i],
+        "adi_set_fault_injection": [vp, i],
         "adi_set_mask": [vp] + [vp] * 7,
         "adi_mask_shape3d": [vp, vp, i, vp, i, d, C.POINTER(i)],
         "adi_mask_sea": [vp, vp, i, i, C.c_float, d, vp, d],

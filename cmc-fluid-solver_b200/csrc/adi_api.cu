@@ -67,6 +67,7 @@ struct adi_handle {
 
     bool mask_set = false, segs_built = false, contract_ok = false;
     bool bv_synced = false;   // cur == node values at every BOUND/VALVE node
+    int fault = ADI_FAULT_NONE;   // adi_set_fault_injection
 
     // Step results the host reads back: divergence sum and count, the device error
     // flag, the residual maxima (bit patterns).  Pinned, so the copies can sit in a
@@ -179,6 +180,8 @@ SweepConst<R> sweep_const(const adi_handle *h, int dir, R dt)
     k.inv_two_dy = R(1) / k.two_dy;
     k.inv_two_dz = R(1) / k.two_dz;
     k.nv_in_temp = h->bv_synced ? 1 : 0;
+    k.skip_tile_loads = h->fault == ADI_FAULT_SKIP_TILE_LOADS ? 1 : 0;
+    k.tile_wait_tries = k.skip_tile_loads ? 16 : 1 << 17;
     return k;
 }
 
@@ -976,6 +979,16 @@ adi_status adi_set_solver(adi_handle *h, int kind)
     if (!h) return ADI_ERR_BAD_ARG;
     if (kind != ADI_SOLVER_EXACT && kind != ADI_SOLVER_FAST) return fail(h, ADI_ERR_BAD_ARG, "unknown solver kind");
     h->solver = kind;
+    invalidate_graphs(h);
+    return ADI_OK;
+}
+
+adi_status adi_set_fault_injection(adi_handle *h, int what)
+{
+    if (!h) return ADI_ERR_BAD_ARG;
+    if (what != ADI_FAULT_NONE && what != ADI_FAULT_SKIP_TILE_LOADS)
+        return fail(h, ADI_ERR_BAD_ARG, "unknown fault-injection mode");
+    h->fault = what;
     invalidate_graphs(h);
     return ADI_OK;
 }

@@ -106,6 +106,12 @@ struct SweepConst {
     // Dirichlet boundary rows can then read their value from the temp tile they
     // already hold instead of loading the node-value arrays.
     int nv_in_temp;
+    // Bounded wait of the TMA-fed X/Y sweep for its tiles: polls of about 10 us
+    // each (2^17 normally).  skip_tile_loads (set only by adi_set_fault_injection,
+    // to test failure detection) makes that sweep issue no tile load at all, so its
+    // wait runs out and the step reports ADI_ERR_TIMEOUT with nothing in flight.
+    int tile_wait_tries;
+    int skip_tile_loads;
 };
 
 // Launch shape of the fast sweep: NL lines per CTA, chunks of K rows per thread,

@@ -150,6 +150,7 @@ __global__ void __launch_bounds__(NLT * P, xy_ctas_per_sm((int)sizeof(R), K, NLT
         const int k0 = (tile - outer * kblocks) * NLT;
         constexpr uint32_t bytes =
             (uint32_t)(9 * (size_t)L * NLT * sizeof(R) + (size_t)L * WIDE * sizeof(R) + (size_t)L * 16);
+        if (kc.skip_tile_loads) return;   // fault injection: the tile never arrives
         tma::arrive_expect_tx(bar, bytes);
         // coordinates (innermost first): X {k, j, c, i}, Y {k, c, i, x}
         const int c1 = DIR == 0 ? outer : 0, c3 = DIR == 0 ? 0 : outer;
@@ -196,7 +197,7 @@ __global__ void __launch_bounds__(NLT * P, xy_ctas_per_sm((int)sizeof(R), K, NLT
         // Bounded wait.  A thread whose wait gave up computes on whatever the tile
         // holds; the CTA checks every thread's wait at the release barrier and
         // leaves before writing anything of this tile.
-        const bool tiles_ok = tma::mbar_wait(bar, it & 1, 1 << 17);
+        const bool tiles_ok = tma::mbar_wait(bar, it & 1, kc.tile_wait_tries);
 
         // ---------------- rows from the tile: one pass, 3-row window ----------------
         const int code_col = li + (k0 & 15);          // this line's byte in a code row
@@ -339,7 +340,8 @@ __global__ void __launch_bounds__(NLT * P, xy_ctas_per_sm((int)sizeof(R), K, NLT
         if (__syncthreads_or(!tiles_ok)) {
             if (t == 0) {
                 atomicExch(err_flag, 1);
-                tma::mbar_wait(bar, it & 1, 1 << 10);   // copies still in flight
+                // copies still in flight (none when the loads were never issued)
+                tma::mbar_wait(bar, it & 1, kc.tile_wait_tries < (1 << 10) ? kc.tile_wait_tries : 1 << 10);
             }
             break;
         }

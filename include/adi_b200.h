@@ -110,6 +110,16 @@ adi_status adi_set_solver(adi_handle *h, int kind);
 /* Message for the last non-OK status of this handle (static storage). */
 const char *adi_last_error_string(const adi_handle *h);
 
+/* Fault injection, for testing failure detection (no counterpart in the
+ * reference).  ADI_FAULT_SKIP_TILE_LOADS: the TMA-fed X/Y sweeps (fast solver,
+ * 8- or 16-line tile shapes) issue no tile loads, so their bounded wait for the
+ * tiles gives up after about 160 us; the step's next synchronising call returns
+ * ADI_ERR_TIMEOUT and the sweep writes nothing.  Nothing is left in flight and
+ * the context stays usable: ADI_FAULT_NONE restores normal steps.  Rebuilds the
+ * handle's step graphs. */
+typedef enum adi_fault { ADI_FAULT_NONE = 0, ADI_FAULT_SKIP_TILE_LOADS = 1 } adi_fault;
+adi_status adi_set_fault_injection(adi_handle *h, int what);
+
 /* ---- grid / mask ------------------------------------------------------- */
 
 /* Uploads the Grid3D node array as SoA: node type, bc_vel, bc_temp and the
