@@ -22,6 +22,12 @@ roofline: the sweep kernels (the dominant class), algorithmic bytes per launch /
          around each); those events sit between launches, so the per-class sum
          runs a few percent above the graph-replayed ms_per_step and the
          achieved GB/s are a lower bound.
+batched / adjoint_over_forward / adjoint / ellipsoids384: the default run (spheres128,
+         one GPU) also runs the metric's other workloads with bounded step counts and
+         attaches their results: batched64 as one batch against the same domains
+         stepped one by one, adjoint128's adjoint/forward time with its gradient
+         check against FP64 central differences, and ellipsoids384 (value and sweep
+         roofline); --no-extras leaves them out.
 accuracy: max relative field error of 10 FP32 steps (the timed path) against 10
          steps of the FP64 CPU oracle (the C restatement of the reference's step,
          oracle/), computed after the timed region on rank 0.
@@ -89,7 +95,8 @@ CONFIGS = {
                        desc="plain 3D ADI forward: 128^3 FP32 box, 40 solid spheres (radii U[4,12], "
                             "centres U[0,128)^3, seed 0), inflow u=1 on x=0, Re=200, dt=5e-4, "
                             "num_global=4, num_local=2"),
-    "ellipsoids384": dict(make=_ellipsoids384, Re=500.0, Pr=0.72, lam=1.4, dt=2e-4, ng=4, nl=2,
+    "ellipsoids384": dict(make=_ellipsoids384, Re=500.0, Pr=0.72, lam=1.4, dt=2e-4, ng=4, nl=2, acc_steps=1,
+                          e2e_steps=5,
                           desc="large 3D single domain: 384^3 FP32, 300 solid ellipsoids (semi-axes "
                                "U[3,20], seed 1) plus a thin-walled tube along x, Re=500, dt=2e-4, "
                                "num_global=4, num_local=2"),
@@ -148,6 +155,15 @@ def workload_kind(cfg) -> str:
 
 def workload_config(args, cfg, cells) -> dict:
     return {"workload": f"{args.config}: {cfg['desc']}", "cells": int(cells), "l2": L2_POLICY[workload_kind(cfg)]}
+
+
+def emit(args, line):
+    """Prints a workload's JSON line, or keeps it (args.result) for a caller that
+    attaches it to another line."""
+    if getattr(args, "defer_print", False):
+        args.result = line
+    else:
+        print(json.dumps(line), flush=True)
 
 
 def measured_peaks():
@@ -487,7 +503,7 @@ def run_ours(args):
     cur = s.fields(0)
     for a, b in zip(pinned[:4], cur):
         a[...] = b
-    e2e_steps = max(1, min(args.steps, 20))
+    e2e_steps = max(1, min(args.steps, cfg.get("e2e_steps", 20)))
     barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -544,7 +560,7 @@ def run_ours(args):
         "clocks": clk,
     }
     if rank == 0:
-        acc_steps = 10
+        acc_steps = cfg.get("acc_steps", 10)
         shp = [(K, NL) for K, NL, _ in s.fast_shapes()] if args.solver == "fast" else None
         err = accuracy_vs_fp64(d, cfg["Re"], cfg["Pr"], cfg["lam"], dt, ng, nl, acc_steps, solver_kind,
                                stream.cuda_stream, shp)
@@ -561,7 +577,7 @@ def run_ours(args):
                                 "sample": f"{done} full steps of {args.config} ({el:.1f} s) on the reference "
                                           f"CPU solver, OpenMP {os.environ['OMP_NUM_THREADS']} threads"}
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        emit(args, line)
     s.close()
     if world > 1:
         torch.distributed.destroy_process_group()
@@ -808,7 +824,7 @@ def run_batch(args):
                                 "sample": f"one step of each of the first {done} domains ({el:.1f} s) on the "
                                           f"reference CPU solver, OpenMP {os.environ['OMP_NUM_THREADS']} threads"}
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        emit(args, line)
     batch.close()
     for m in members:
         m.close()
@@ -919,7 +935,7 @@ def run_adjoint(args):
     }
     del step_bytes
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        emit(args, line)
     s.close()
     s64.close()
     return 0
@@ -1178,6 +1194,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of reference CPU time for cpu_baseline")
     ap.add_argument("--ref-budget", type=float, default=120.0, help="seconds cap for --impl reference")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="spheres128 at N = 1: skip the batched64 / adjoint128 / ellipsoids384 objects")
     ap.add_argument("--no-plain-loop", action="store_true",
                     help="batched configs: skip timing the same domains stepped one at a time")
     ap.add_argument("--shapes", default=None,
@@ -1196,7 +1214,64 @@ def main():
         return run_2d(args)
     if CONFIGS[args.config].get("masks"):
         return run_masks(args)
-    return run_ours(args)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.config != "spheres128" or world > 1 or args.no_extras:
+        return run_ours(args)
+    # The headline workload at N = 1 also carries the metric's other parts
+    # (batched vs plain, adjoint/forward, the large single domain), measured in
+    # the same run; the N > 1 runs carry the headline only.
+    args.defer_print = True
+    rc = run_ours(args)
+    line = args.result
+    line.update(run_extras(args))
+    print(json.dumps(line), flush=True)
+    return rc
+
+
+def run_extras(args):
+    """batched64 (one batch vs the same domains stepped one by one), adjoint128
+    (adjoint/forward time and the gradient check) and ellipsoids384, each through
+    its own runner with a bounded number of steps; returns the objects the headline
+    line carries."""
+    import copy
+
+    def sub(config, steps):
+        a = copy.copy(args)
+        a.config, a.steps, a.warmup, a.shapes = config, steps, 3, None
+        a.no_cpu_baseline, a.no_plain_loop, a.defer_print, a.result = True, False, True, None
+        t0 = time.perf_counter()
+        cfg = CONFIGS[config]
+        (run_batch if cfg.get("batch") else run_adjoint if cfg.get("adjoint") else run_ours)(a)
+        return a.result, time.perf_counter() - t0
+
+    out = {}
+    b, wall = sub("batched64", 10)
+    plain = (b.get("plain_per_domain") or {}).get("value")
+    out["batched"] = {
+        "workload": b["config"]["workload"], "cells": b["config"]["cells"], "value": b["value"], "unit": METRIC,
+        "ms_per_step": b["ms_per_step"], "steps": b["steps"], "plain_per_domain_value": plain,
+        "batched_over_plain": b["value"] / plain if plain else None,
+        "roofline": {k: b["roofline"][k] for k in ("kernel", "achieved", "peak", "frac", "unit")},
+        "accuracy_max_rel_err_vs_fp64": max(b["accuracy"]["max_rel_err_vs_fp64"].values()),
+        "e2e": b["e2e"], "gpu_launches": b["gpu_launches"], "clocks": b["clocks"], "wall_s": wall,
+    }
+    a, wall = sub("adjoint128", 40)
+    out["adjoint_over_forward"] = a["adjoint_over_forward"]
+    out["adjoint"] = {
+        "workload": a["config"]["workload"], "forward_ms": a["forward_ms"], "adjoint_ms": a["adjoint_ms"],
+        "adjoint_over_forward": a["adjoint_over_forward"],
+        "grad_check_max_rel_err_vs_fp64_central_fd": a["grad_check"]["max_rel_err_vs_fp64_central_fd"],
+        "grad_check_bound": 1e-4, "clocks": a["clocks"], "wall_s": wall,
+    }
+    e, wall = sub("ellipsoids384", 10)
+    out["ellipsoids384"] = {
+        "workload": e["config"]["workload"], "cells": e["config"]["cells"], "value": e["value"], "unit": METRIC,
+        "ms_per_step": e["ms_per_step"], "steps": e["steps"], "fast_shapes": e["run"]["fast_shapes"],
+        "roofline": {k: e["roofline"][k] for k in ("kernel", "achieved", "peak", "frac", "unit", "per_kernel")},
+        "accuracy": e["accuracy"], "e2e": e["e2e"], "gpu_launches": e["gpu_launches"], "clocks": e["clocks"],
+        "wall_s": wall,
+    }
+    return out
 
 
 if __name__ == "__main__":

@@ -66,10 +66,11 @@ __host__ __device__ constexpr size_t round128(size_t b) { return (b + 127) / 128
 
 // CTAs per SM a launch shape is compiled for (FP32; FP64 tiles fit fewer): the
 // register cap follows from it and the shared-memory budget per CTA must allow it
-// (K = 8 with 8 lines: a 47 KB tile plus 11 KB of reduced-system slots, three).
-__host__ __device__ constexpr int xy_ctas_per_sm(int es, int K, int NLT)
+// (K = 8 with 8 lines: a 47 KB tile plus 11 KB of reduced-system slots, three;
+// lines longer than 32 chunks: one CTA of NLT * P threads).
+__host__ __device__ constexpr int xy_ctas_per_sm(int es, int K, int NLT, int P)
 {
-    return es != 4 ? 1 : (K == 4 ? (NLT == 8 ? 3 : 1) : (K == 8 ? (NLT == 8 ? 3 : 2) : 1));
+    return es != 4 || P > 32 ? 1 : (K == 4 ? (NLT == 8 ? 3 : 1) : (K == 8 ? (NLT == 8 ? 3 : 2) : 1));
 }
 
 
@@ -87,7 +88,7 @@ __host__ __device__ constexpr size_t xy_tile_bytes(int L)
 // memory allows (xy_ctas_per_sm): FP32 K = 8 four of 8 lines or two of 16, K = 4
 // three of 8 lines.
 template <typename R, int DIR, int K, int NLT, int P>
-__global__ void __launch_bounds__(NLT * P, xy_ctas_per_sm((int)sizeof(R), K, NLT))
+__global__ void __launch_bounds__(NLT * P, xy_ctas_per_sm((int)sizeof(R), K, NLT, P))
     sweep_xytma_kernel(const __grid_constant__ XYMaps maps, DomainView<R> d, LineGeom g, Layer<R> next,
                        Layer<R> tout, SweepConst<R> kc, int merges, int ntiles, int *err_flag)
 {
@@ -137,9 +138,18 @@ __global__ void __launch_bounds__(NLT * P, xy_ctas_per_sm((int)sizeof(R), K, NLT
             else { v[2 * u] = a.x; v[2 * u + 1] = a.y; }
         }
     };
-    // the warp-phase role of this thread: chunk wc of line wl
+    // The warp-phase role of this thread: chunk wc of line wl.  A line of P <= 32
+    // chunks sits in P lanes of one warp (32 / P lines per warp); a longer line
+    // (P = 32 W) in W consecutive warps, which meet on a named barrier of their own.
     const int lane = t & 31;
-    const int wl = (t >> 5) * (32 / P) + lane / P, wc = lane % P;
+    constexpr int WPL = P > 32 ? P / 32 : 1;   // warps per line
+    static_assert(P <= 32 || P % 32 == 0, "lines longer than a warp span whole warps");
+    const int wl = P <= 32 ? (t >> 5) * (32 / P) + lane / P : (t >> 5) / WPL;
+    const int wc = P <= 32 ? lane % P : 32 * ((t >> 5) % WPL) + lane;
+    auto line_sync = [&]() {
+        if constexpr (P <= 32) __syncwarp();
+        else asm volatile("bar.sync %0, %1;" ::"r"(1 + wl), "r"(32 * WPL) : "memory");
+    };
 
 
     // Loads of one tile (thread 0).  Every box delivers its full size (zero fill
@@ -360,35 +370,81 @@ __global__ void __launch_bounds__(NLT * P, xy_ctas_per_sm((int)sizeof(R), K, NLT
             }
 #pragma unroll
             for (int v = 0; v < 4; v++) { wr.Df[v] = rv[8 + v]; wr.Dl[v] = rv[12 + v]; }
-            auto up = [&](R x, int dd) { return __shfl_up_sync(0xffffffffu, x, dd, P); };
-            auto dn = [&](R x, int dd) { return __shfl_down_sync(0xffffffffu, x, dd, P); };
             R ea_[2], ec_[2], ed[4];
-            {
-                // cyclic-reduction step with the previous chunk's last row
-                R pv[8] = {up(wr.Al[0], 1), up(wr.Cl[0], 1), up(wr.Al[1], 1), up(wr.Cl[1], 1),
-                           up(wr.Dl[0], 1), up(wr.Dl[1], 1), up(wr.Dl[2], 1), up(wr.Dl[3], 1)};
-                if (wc == 0) {
-#pragma unroll
-                    for (int q = 0; q < 8; q++) pv[q] = R(0);
-                }
-                cr_step<R>(wr, pv, ea_, ec_, ed);
-            }
-#pragma unroll
-            for (int st = 1; st < P; st <<= 1) {
-                const R mv[8] = {up(ea_[0], st), up(ec_[0], st), up(ea_[1], st), up(ec_[1], st),
-                                 up(ed[0], st),  up(ed[1], st),  up(ed[2], st),  up(ed[3], st)};
-                const R pv[8] = {dn(ea_[0], st), dn(ec_[0], st), dn(ea_[1], st), dn(ec_[1], st),
-                                 dn(ed[0], st),  dn(ed[1], st),  dn(ed[2], st),  dn(ed[3], st)};
-                pcr_update<R>(mv, pv, ea_, ec_, ed);
-            }
             R xo[8];
+            (void)line_sync;
+            if constexpr (P <= 32) {
+                auto up = [&](R x, int dd) { return __shfl_up_sync(0xffffffffu, x, dd, P); };
+                auto dn = [&](R x, int dd) { return __shfl_down_sync(0xffffffffu, x, dd, P); };
+                {
+                    // cyclic-reduction step with the previous chunk's last row
+                    R pv[8] = {up(wr.Al[0], 1), up(wr.Cl[0], 1), up(wr.Al[1], 1), up(wr.Cl[1], 1),
+                               up(wr.Dl[0], 1), up(wr.Dl[1], 1), up(wr.Dl[2], 1), up(wr.Dl[3], 1)};
+                    if (wc == 0) {
 #pragma unroll
-            for (int v = 0; v < 4; v++) {
-                R nf = dn(ed[v], 1);
-                if (wc == P - 1) nf = R(0);
-                const int m = v < 3 ? 0 : 1;
-                xo[v] = ed[v];
-                xo[4 + v] = wr.Dl[v] - wr.Al[m] * ed[v] - wr.Cl[m] * nf;   // Cl = 0 on the last chunk
+                        for (int q = 0; q < 8; q++) pv[q] = R(0);
+                    }
+                    cr_step<R>(wr, pv, ea_, ec_, ed);
+                }
+#pragma unroll
+                for (int st = 1; st < P; st <<= 1) {
+                    const R mv[8] = {up(ea_[0], st), up(ec_[0], st), up(ea_[1], st), up(ec_[1], st),
+                                     up(ed[0], st),  up(ed[1], st),  up(ed[2], st),  up(ed[3], st)};
+                    const R pv[8] = {dn(ea_[0], st), dn(ec_[0], st), dn(ea_[1], st), dn(ec_[1], st),
+                                     dn(ed[0], st),  dn(ed[1], st),  dn(ed[2], st),  dn(ed[3], st)};
+                    pcr_update<R>(mv, pv, ea_, ec_, ed);
+                }
+#pragma unroll
+                for (int v = 0; v < 4; v++) {
+                    R nf = dn(ed[v], 1);
+                    if (wc == P - 1) nf = R(0);
+                    const int m = v < 3 ? 0 : 1;
+                    xo[v] = ed[v];
+                    xo[4 + v] = wr.Dl[v] - wr.Al[m] * ed[v] - wr.Cl[m] * nf;   // Cl = 0 on the last chunk
+                }
+            } else {
+                // The line's rows are exchanged through shared memory, the line's
+                // warps meeting on their named barrier: the cyclic-reduction step
+                // reads the previous chunk's RED slot, then RED's two halves serve as
+                // the ping-pong buffers of the PCR steps (each 8 values per slot).
+                const int q = wl * (P + 1) + wc;
+                {
+                    R pv[8] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};
+                    if (wc > 0) {
+                        R pr[16];
+                        uload(RED, q - 1, pr, 16);
+                        pv[0] = pr[4]; pv[1] = pr[6]; pv[2] = pr[5]; pv[3] = pr[7];
+#pragma unroll
+                        for (int v = 0; v < 4; v++) pv[4 + v] = pr[12 + v];
+                    }
+                    cr_step<R>(wr, pv, ea_, ec_, ed);
+                }
+                U16 *const bufA = RED, *const bufB = RED + 8 / UW * NQ;
+                line_sync();   // every RED read of the line is done
+                int n = 0;
+#pragma unroll
+                for (int st = 1; st < P; st <<= 1, n++) {
+                    U16 *const bw = (n & 1) ? bufA : bufB;
+                    const R mine[8] = {ea_[0], ec_[0], ea_[1], ec_[1], ed[0], ed[1], ed[2], ed[3]};
+                    ustore(bw, q, mine, 8);
+                    line_sync();
+                    R mv[8], pv[8];
+                    uload(bw, wc - st >= 0 ? q - st : q, mv, 8);
+                    uload(bw, wc + st < P ? q + st : q, pv, 8);
+                    pcr_update<R>(mv, pv, ea_, ec_, ed);
+                }
+                U16 *const bx = (n & 1) ? bufA : bufB;
+                const R mine[8] = {ed[0], ed[1], ed[2], ed[3], R(0), R(0), R(0), R(0)};
+                ustore(bx, q, mine, 8);
+                line_sync();
+                R nf[8];
+                uload(bx, wc + 1 < P ? q + 1 : q, nf, 8);
+#pragma unroll
+                for (int v = 0; v < 4; v++) {
+                    const int m = v < 3 ? 0 : 1;
+                    xo[v] = ed[v];
+                    xo[4 + v] = wr.Dl[v] - wr.Al[m] * ed[v] - wr.Cl[m] * (wc + 1 < P ? nf[v] : R(0));
+                }
             }
             ustore(XS, wl * (P + 1) + wc, xo, 8);
         }
@@ -551,11 +607,13 @@ bool xytma_supported(int dir, int nx, int ny, int nz, int K, int nlt, int elem_b
     if (K != 4 && K != 8 && K != 16) return false;
     if (L % K != 0) return false;
     const int P = L / K;
-    if (P != 4 && P != 8 && P != 16 && !(P == 32 && K == 4)) return false;   // compiled chunk counts
+    // compiled chunk counts; lines of 64 or 96 chunks (several warps per line) in float, K = 4, 8 lines
+    const bool multi = (P == 64 || P == 96) && K == 4 && nlt == 8 && elem_bytes == 4;
+    if (P != 4 && P != 8 && P != 16 && !(P == 32 && K == 4) && !multi) return false;
     const int threads = nlt * P;
-    if (threads < 32 || threads > 512) return false;
+    if (threads < 32 || threads > 1024) return false;
     // the CTAs per SM the shape is compiled for (228 KB per SM, 1 KB reserved per CTA)
-    const size_t budget = 228 * 1024 / xy_ctas_per_sm(elem_bytes, K, nlt) - 1024;
+    const size_t budget = 228 * 1024 / xy_ctas_per_sm(elem_bytes, K, nlt, P) - 1024;
     return xytma_smem_bytes(L, P, nlt, elem_bytes) <= (budget < 227 * 1024 ? budget : 227 * 1024);
 }
 
@@ -627,6 +685,9 @@ cudaError_t launch_sweep_xytma(int dir, const DomainView<R> &d, const int *line_
     XLP(0, 8, 16) XLP(0, 16, 16) XLP(1, 8, 16) XLP(1, 16, 16)
     XLP(0, 4, 8) XLP(1, 4, 8) XLP(0, 4, 16) XLP(1, 4, 16)
     XL(0, 4, 8, 32) XL(1, 4, 8, 32) XL(0, 4, 16, 32) XL(1, 4, 16, 32)
+    if constexpr (sizeof(R) == 4) {
+        XL(0, 4, 8, 64) XL(1, 4, 8, 64) XL(0, 4, 8, 96) XL(1, 4, 8, 96)
+    }
 #undef XLP
 #undef XL
     return cudaErrorInvalidConfiguration;

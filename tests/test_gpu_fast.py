@@ -167,6 +167,26 @@ def test_xytma_kernel(adi_lib, xK, nl, precision):
     assert max(errs_n) < (1e-11 if precision == "fp64" else 2e-6), errs_n
 
 
+@pytest.mark.parametrize("nx", [256, 384])
+def test_xytma_lines_over_several_warps(adi_lib, nx):
+    """TMA-fed X sweep with X lines of 64 and 96 chunks (K = 4, 8 lines per CTA): a
+    line spans two or three warps, whose reduced system goes through shared memory
+    with a named barrier per line; against the FP64 oracle."""
+    d = G.random_domain(nx, 32, 32, seed=83, shell=True, n_obstacles=12, rmax=5.0)
+    params = (140.0, 0.72, 1.4)
+    s = solver(adi_lib, d, params, shapes=[(4, -8), (4, -8), (4, 0)])
+    assert s.fast_shapes()[0] == (4, -8, nx // 4)
+    orc = O.OracleSolver(d, precision=8, params=fluid_params_tuple(("normalized", params)))
+    m = non_out(d)
+    for _ in range(3):
+        assert s.step(8e-4, 4, 2, True) == 0
+        assert orc.step(8e-4, 4, 2, True) == 0
+    errs = rel_errors(s.fields(0), orc.fields(0), m)
+    assert max(errs) < 2e-6, errs
+    errs_n = rel_errors(s.fields(1), orc.fields(1), m)
+    assert max(errs_n) < 2e-6, errs_n
+
+
 def _slab_domain(nx, ny, nz, seed):
     """Random shell domain plus a wall slab at k = 1..16, so that the first 16-line
     tile of every X and Y plane holds no segment (the persistent kernel skips it)."""

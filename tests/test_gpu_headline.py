@@ -3,10 +3,11 @@
 The benchmark's headline workload is spheres128: a 128^3 float box with 40 solid
 spheres (seed 0), Re 200, dt 5e-4, num_global 4, num_local 2, stepped by
 UpdateBoundaries + TimeStep (AdiSolver3D.cpp:286-391, FluidSolver3D.cpp:241-242).
-Its autotuner picks the TMA-fed X/Y sweep with 8 or 16 lines per CTA (K = 8,
-P = 16 chunks per 128-row line) and the warp-resident Z sweep (K = 4, P = 32);
-every such shape is a separate template instantiation, so the tests pin each one
-and compare it with the oracle on the full-size domain:
+Its autotuner picks among the TMA-fed X/Y sweep's shapes (8 or 16 lines per CTA,
+chunks of K = 4 or 8 rows, so P = 32 or 16 chunks per 128-row line) and the
+warp-resident Z sweep (K = 4, P = 32 or K = 8, P = 16); every such shape is a
+separate template instantiation, so the tests pin each one and compare it with
+the oracle on the full-size domain:
 
 * the exact solver equals the reference's own CPU solver (oracle/_ref) bit for
   bit after two driver steps;
@@ -34,9 +35,10 @@ DT = 5e-4
 # (K, NL) per direction as set_fast_shape takes them: NL = -8 / -16 is the TMA
 # X/Y sweep with 8 / 16 lines per CTA, NL = 0 the warp-resident Z sweep.
 HEADLINE_SHAPES = [
+    [(4, -8), (4, -8), (4, 0)],
+    [(4, -16), (4, -16), (8, 0)],
     [(8, -8), (8, -8), (4, 0)],
     [(8, -16), (8, -16), (4, 0)],
-    [(8, -16), (8, -8), (8, 0)],
 ]
 
 
