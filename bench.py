@@ -187,15 +187,16 @@ def ncu_traffic(config: str, kernel: str):
 
 def sweep_kernel_name(solver: str, shape) -> str:
     """Kernel that runs one direction's sweep: the exact kernel, or the fast variant its shape selects
-    (lines per CTA NL > 0 generic chunked, 0 warp-resident Z lines, -16 / -8 TMA-fed X/Y tiles of 16 / 8
-    lines, -32 persistent double-buffered X/Y tiles with two lines per thread)."""
+    (lines per CTA NL > 0 generic chunked, 0 warp-resident Z lines, -16 / -8 the X/Y tile kernel with TMA-loaded
+    tiles of 16 / 8 lines, -1 the same kernel with tiles copied element-wise (cp.async), -32 persistent
+    double-buffered X/Y tiles with two lines per thread)."""
     if solver == "exact":
         return "sweep_exact_kernel"
     nl = shape[1]
     if nl > 0:
         return "sweep_fast_kernel"
-    return {0: "sweep_zwarp_kernel", -16: "sweep_xytma_kernel", -8: "sweep_xytma_kernel",
-            -32: "sweep_xypair_kernel"}[nl]
+    return {0: "sweep_zwarp_kernel", -16: "sweep_xy_kernel[tma]", -8: "sweep_xy_kernel[tma]",
+            -1: "sweep_xy_kernel[cp.async]", -32: "sweep_xypair_kernel"}[nl]
 
 
 class ClockSampler:

@@ -302,6 +302,7 @@ bool shape_ok(const adi_handle *h, int dir, const FastShape &s)
     if (s.mode == 2 || s.mode == 4)
         return dir < 2 && xytma_supported(dir, h->nx, h->ny, h->nz, s.K, s.mode == 2 ? 16 : 8, (int)esize(h));
     if (s.mode == 3) return dir < 2 && xypair_supported(dir, h->nx, h->ny, h->nz, s.K, (int)esize(h));
+    if (s.mode == 5) return dir < 2 && xycp_supported(dir, h->nx, h->ny, h->nz, s.K, (int)esize(h));
     return s.mode == 0 && fast_shape_supported(dir, s, line_len(h, dir), (int)esize(h));
 }
 
@@ -317,6 +318,8 @@ cudaError_t launch_fast(adi_handle *h, int dir, CLayer<R> cur, CLayer<R> tin, La
     if (s.mode == 2 || s.mode == 4)
         return launch_sweep_xytma<R>(dir, d, h->d_line_lo[dir], cur, tin, next, tout, k, merges, s.K,
                                      s.mode == 2 ? 16 : 8, h->d_err, h->stream);
+    if (s.mode == 5)
+        return launch_sweep_xycp<R>(dir, d, cur, tin, next, tout, k, merges, s.K, h->d_err, h->stream);
     if (s.mode == 3) {
         if constexpr (std::is_same<R, float>::value)
             return launch_sweep_xypair(dir, d, h->d_line_lo[dir], cur, tin, next, tout, k, merges, s.K, h->d_err,
@@ -397,6 +400,10 @@ std::vector<FastShape> shape_candidates(const adi_handle *h, int dir)
             if (shape_ok(h, dir, s)) out.push_back(s);
             FastShape s8{K, 8, len / K, 4};
             if (shape_ok(h, dir, s8)) out.push_back(s8);
+        }
+        for (int K : {4, 5}) {
+            FastShape s{K, 8, (len + K - 1) / K, 5};
+            if (shape_ok(h, dir, s)) out.push_back(s);
         }
     }
     for (int K : {4, 8, 12, 16})
@@ -1365,7 +1372,9 @@ adi_status adi_get_fast_shape(adi_handle *h, int dir, int *K, int *NL, int *P)
     if (!h || dir < 0 || dir > 2) return ADI_ERR_BAD_ARG;
     const FastShape s = h->shape[dir];
     if (K) *K = s.K;
-    if (NL) *NL = s.mode == 1 ? 0 : (s.mode == 2 ? -16 : (s.mode == 3 ? -32 : (s.mode == 4 ? -8 : s.NL)));
+    if (NL)
+        *NL = s.mode == 1 ? 0
+                          : (s.mode == 2 ? -16 : (s.mode == 3 ? -32 : (s.mode == 4 ? -8 : (s.mode == 5 ? -1 : s.NL))));
     if (P) *P = (line_len(h, dir) + s.K - 1) / s.K;
     return ADI_OK;
 }
@@ -1374,10 +1383,10 @@ adi_status adi_set_fast_shape(adi_handle *h, int dir, int K, int NL)
 {
     if (!h || dir < 0 || dir > 2 || K <= 0) return ADI_ERR_BAD_ARG;
     const int len = line_len(h, dir);
-    if (NL < 0 && NL != -8 && NL != -16 && NL != -32)
+    if (NL < 0 && NL != -8 && NL != -16 && NL != -32 && NL != -1)
         return fail(h, ADI_ERR_BAD_ARG, "unsupported fast-sweep shape");
-    const int mode = NL == 0 ? 1 : (NL == -16 ? 2 : (NL == -32 ? 3 : (NL == -8 ? 4 : 0)));
-    FastShape s{K, NL < 0 ? -NL : NL, (len + K - 1) / K, mode};
+    const int mode = NL == 0 ? 1 : (NL == -16 ? 2 : (NL == -32 ? 3 : (NL == -8 ? 4 : (NL == -1 ? 5 : 0))));
+    FastShape s{K, NL == -1 ? 8 : (NL < 0 ? -NL : NL), (len + K - 1) / K, mode};
     if (!shape_ok(h, dir, s)) return fail(h, ADI_ERR_BAD_ARG, "unsupported fast-sweep shape");
     h->shape[dir] = s;
     h->tuned = true;
@@ -1690,6 +1699,16 @@ adi_status batch_build(adi_batch *b)
             bd[q].lo[dir] = h->d_line_lo[dir];
             bd[q].hi[dir] = h->d_line_hi[dir];
             const LineGeom g = line_geom(dir, h->nx, h->ny, h->nz);
+            if (b->K[dir] < 0) {
+                // X/Y tile kernel: items (domain, tile of 8 lines), lines up to 32 |K| rows
+                if (g.len > 32 * -b->K[dir])
+                    return bfail(b, ADI_ERR_CAPACITY, "a domain's lines are too long for the batched tile sweep");
+                const int ntiles = (dir == 0 ? h->ny : h->nx) * ((h->nz + 7) / 8);
+                for (int tl = 0; tl < ntiles; tl++) items[dir].push_back({0, make_int2(q, tl)});
+                bd[q].P[dir] = 32;
+                bd[q].NL[dir] = 8;
+                continue;
+            }
             const int P = (g.len + b->K[dir] - 1) / b->K[dir];
             if (P > 256) return bfail(b, ADI_ERR_CAPACITY, "a domain's lines are too long for the batched sweep");
             const int NL = std::max(1, 256 / P);
@@ -1717,7 +1736,7 @@ adi_status batch_build(adi_batch *b)
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        b->grid[dir] = std::max(1, std::min(b->nitems[dir], sms * (b->K[dir] == 4 ? 2 : 1)));
+        b->grid[dir] = std::max(1, std::min(b->nitems[dir], sms * (b->K[dir] == 4 ? 2 : 1)));   // generic kernel
     }
     if (!b->d_doms) BCK(cudaMalloc(&b->d_doms, b->host_doms.size()));
     b->dt_loaded = NAN;
@@ -1742,6 +1761,19 @@ adi_status batch_load_dt(adi_batch *b, double dt)
     return ADI_OK;
 }
 
+// One batched sweep: the X/Y tile kernel (K < 0: tiles of 8 lines copied
+// element-wise, chunks of |K| rows) or the generic chunked kernel (K > 0).
+template <typename R>
+cudaError_t batch_sweep(adi_batch *b, int dir, int K, int src, int tin, int dst, int tout, int merges)
+{
+    const BatchDomain<R> *doms = (const BatchDomain<R> *)b->d_doms;
+    if (K < 0)
+        return launch_sweep_xy_batch<R>(dir, -K, doms, b->d_items[dir], b->nitems[dir], src, tin, dst, tout, merges,
+                                        b->hs[0]->d_err, b->stream);
+    return launch_sweep_fast_batch<R>(dir, K, doms, b->d_items[dir], b->nitems[dir], b->grid[dir], src, tin, dst, tout,
+                                      merges, b->stream);
+}
+
 template <typename R>
 adi_status batch_enqueue(adi_batch *b, int num_global, int num_local, int compute_error, int &ta, int &tb)
 {
@@ -1758,8 +1790,7 @@ adi_status batch_enqueue(adi_batch *b, int num_global, int num_local, int comput
             const int dir = order[q];
             for (int l = 0; l < num_local; l++) {
                 const int merges = (dir == 0 && l == num_local - 1) ? 2 : 1;
-                BCK(launch_sweep_fast_batch<R>(dir, b->K[dir], doms, b->d_items[dir], b->nitems[dir], b->grid[dir],
-                                               src[q], ta, dst[q], tb, merges, b->stream));
+                BCK(batch_sweep<R>(b, dir, b->K[dir], src[q], ta, dst[q], tb, merges));
                 b->launches += b->nitems[dir] > 0;
                 std::swap(ta, tb);
             }
@@ -1938,7 +1969,7 @@ adi_status adi_batch_set_graphs(adi_batch *b, int on)
 
 adi_status adi_batch_set_chunk(adi_batch *b, int dir, int K)
 {
-    if (!b || dir < 0 || dir > 2 || (K != 4 && K != 8)) return ADI_ERR_BAD_ARG;
+    if (!b || dir < 0 || dir > 2 || (K != 4 && K != 8 && !(dir < 2 && (K == -4 || K == -5)))) return ADI_ERR_BAD_ARG;
     const int old = b->K[dir];
     b->K[dir] = K;
     adi_status s = b->prec == ADI_FP64 ? batch_build<double>(b) : batch_build<float>(b);
@@ -1982,7 +2013,8 @@ adi_status adi_batch_autotune(adi_batch *b, double dt, int reps)
     for (int dir = 0; dir < 3; dir++) {
         float best = 1e30f;
         int bestK = b->K[dir];
-        for (int K : {4, 8}) {
+        for (int K : {4, 8, -4, -5}) {
+            if (K < 0 && dir == 2) continue;
             b->K[dir] = K;
             adi_status s = b->prec == ADI_FP64 ? batch_build<double>(b) : batch_build<float>(b);
             if (s != ADI_OK) continue;
@@ -1992,12 +2024,8 @@ adi_status adi_batch_autotune(adi_batch *b, double dt, int reps)
             for (int r = 0; r < reps + 1; r++) {
                 BCK(cudaEventRecord(e0, b->stream));
                 cudaError_t e = b->prec == ADI_FP64
-                    ? launch_sweep_fast_batch<double>(dir, K, (const BatchDomain<double> *)b->d_doms, b->d_items[dir],
-                                                      b->nitems[dir], b->grid[dir], h0->cur, h0->ta, h0->half, h0->tb,
-                                                      1, b->stream)
-                    : launch_sweep_fast_batch<float>(dir, K, (const BatchDomain<float> *)b->d_doms, b->d_items[dir],
-                                                     b->nitems[dir], b->grid[dir], h0->cur, h0->ta, h0->half, h0->tb,
-                                                     1, b->stream);
+                    ? batch_sweep<double>(b, dir, K, h0->cur, h0->ta, h0->half, h0->tb, 1)
+                    : batch_sweep<float>(b, dir, K, h0->cur, h0->ta, h0->half, h0->tb, 1);
                 BCK(e);
                 BCK(cudaEventRecord(e1, b->stream));
                 BCK(cudaEventSynchronize(e1));
@@ -2028,12 +2056,8 @@ adi_status adi_batch_time_sweeps(adi_batch *b, double dt, int reps, float *ms_ou
         for (int r = 0; r < reps + 1; r++) {
             BCK(cudaEventRecord(e0, b->stream));
             cudaError_t e = b->prec == ADI_FP64
-                ? launch_sweep_fast_batch<double>(dir, b->K[dir], (const BatchDomain<double> *)b->d_doms,
-                                                  b->d_items[dir], b->nitems[dir], b->grid[dir], h0->cur, h0->ta,
-                                                  h0->half, h0->tb, 1, b->stream)
-                : launch_sweep_fast_batch<float>(dir, b->K[dir], (const BatchDomain<float> *)b->d_doms,
-                                                 b->d_items[dir], b->nitems[dir], b->grid[dir], h0->cur, h0->ta,
-                                                 h0->half, h0->tb, 1, b->stream);
+                ? batch_sweep<double>(b, dir, b->K[dir], h0->cur, h0->ta, h0->half, h0->tb, 1)
+                : batch_sweep<float>(b, dir, b->K[dir], h0->cur, h0->ta, h0->half, h0->tb, 1);
             BCK(e);
             BCK(cudaEventRecord(e1, b->stream));
             BCK(cudaEventSynchronize(e1));

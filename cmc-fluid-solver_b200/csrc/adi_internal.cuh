@@ -208,6 +208,17 @@ cudaError_t launch_sweep_xytma(int dir, const DomainView<R> &d, const int *line_
                                Layer<R> next, Layer<R> tout, const SweepConst<R> &k, int merges, int K, int nlt,
                                int *err_flag, cudaStream_t s);
 bool xytma_supported(int dir, int nx, int ny, int nz, int K, int nlt, int elem_bytes);
+// The same X/Y sweep with tiles copied element-wise by the CTA's threads (cp.async):
+// any nz, lines up to 160 rows (K = 4: up to 128, K = 5: up to 160), 8 lines per CTA.
+template <typename R>
+cudaError_t launch_sweep_xycp(int dir, const DomainView<R> &d, CLayer<R> cur, CLayer<R> tin, Layer<R> next,
+                              Layer<R> tout, const SweepConst<R> &k, int merges, int K, int *err_flag, cudaStream_t s);
+bool xycp_supported(int dir, int nx, int ny, int nz, int K, int elem_bytes);
+// ... and for every domain of a batch in one persistent launch (work items
+// (domain, tile of 8 lines); each domain's line length at most 32 K rows).
+template <typename R>
+cudaError_t launch_sweep_xy_batch(int dir, int K, const BatchDomain<R> *doms, const int2 *items, int nitems, int src,
+                                  int tin, int dst, int tout, int merges, int *err_flag, cudaStream_t s);
 cudaError_t launch_sweep_xypair(int dir, const DomainView<float> &d, const int *line_lo, CLayer<float> cur,
                                 CLayer<float> tin, Layer<float> next, Layer<float> tout, const SweepConst<float> &k,
                                 int merges, int K, int *err_flag, cudaStream_t s);

@@ -43,6 +43,7 @@
 #include "sweep_common.cuh"
 
 #include "tma.cuh"
+#include "sweep_xyload.cuh"
 
 #include <mutex>
 #include <type_traits>
@@ -70,7 +71,8 @@ __host__ __device__ constexpr size_t round128(size_t b) { return (b + 127) / 128
 // lines longer than 32 chunks: one CTA of NLT * P threads).
 __host__ __device__ constexpr int xy_ctas_per_sm(int es, int K, int NLT, int P)
 {
-    return es != 4 || P > 32 ? 1 : (K == 4 ? (NLT == 8 ? 3 : 1) : (K == 8 ? (NLT == 8 ? 3 : 2) : 1));
+    return es != 4 || P > 32 ? 1
+                             : (K == 4 ? (NLT == 8 ? 3 : 1) : (K == 8 ? (NLT == 8 ? 3 : 2) : (K == 5 ? 2 : 1)));
 }
 
 
@@ -87,10 +89,9 @@ __host__ __device__ constexpr size_t xy_tile_bytes(int L)
 // immediate.  The register cap lets as many CTAs be resident as their shared
 // memory allows (xy_ctas_per_sm): FP32 K = 8 four of 8 lines or two of 16, K = 4
 // three of 8 lines.
-template <typename R, int DIR, int K, int NLT, int P>
+template <typename R, int DIR, int K, int NLT, int P, typename Loader>
 __global__ void __launch_bounds__(NLT * P, xy_ctas_per_sm((int)sizeof(R), K, NLT, P))
-    sweep_xytma_kernel(const __grid_constant__ XYMaps maps, DomainView<R> d, LineGeom g, Layer<R> next,
-                       Layer<R> tout, SweepConst<R> kc, int merges, int ntiles, int *err_flag)
+    sweep_xy_kernel(const __grid_constant__ Loader ld, int merges, int ntiles, int *err_flag)
 {
     using T = XYTile<R, NLT>;
     constexpr int WIDE = T::WIDE, WOFF = T::WOFF;
@@ -98,7 +99,6 @@ __global__ void __launch_bounds__(NLT * P, xy_ctas_per_sm((int)sizeof(R), K, NLT
     extern __shared__ __align__(128) unsigned char smem[];
     const int t = threadIdx.x;
     const int ch = t / NLT, li = t - ch * NLT;
-    const int kblocks = g.nz / NLT;   // tiles per (outer index): X lines j*nz + k, Y lines i*nz + k
 
     // tile layout ([K][P][width] each; every tile starts on a 128-byte boundary)
     constexpr size_t plane = round128((size_t)L * NLT * sizeof(R));
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(NLT * P, xy_ctas_per_sm((int)sizeof(R), K, NLT
     using U16 = typename std::conditional<sizeof(R) == 4, float4, double2>::type;
     U16 *const RED = reinterpret_cast<U16 *>(smem + 9 * plane + wide_bytes + code_bytes);
     U16 *const XS = RED + 16 / UW * NQ;
-    uint64_t *const bar = reinterpret_cast<uint64_t *>(XS + 8 / UW * NQ);
+    const XYSmem<R> sm{tcur, ttin, twide, thm, thp, tcode, reinterpret_cast<uint64_t *>(XS + 8 / UW * NQ)};
     auto ustore = [&](U16 *buf, int q, const R *v, int n) {
 #pragma unroll
         for (int u = 0; u < n / UW; u++) {
@@ -152,38 +152,9 @@ __global__ void __launch_bounds__(NLT * P, xy_ctas_per_sm((int)sizeof(R), K, NLT
     };
 
 
-    // Loads of one tile (thread 0).  Every box delivers its full size (zero fill
-    // included): cur 4, temp 3, off-line halo 2 planes, the wide advecting tile and
-    // the code tile.
-    auto issue = [&](int tile) {
-        const int outer = tile / kblocks;
-        const int k0 = (tile - outer * kblocks) * NLT;
-        constexpr uint32_t bytes =
-            (uint32_t)(9 * (size_t)L * NLT * sizeof(R) + (size_t)L * WIDE * sizeof(R) + (size_t)L * 16);
-        if (kc.skip_tile_loads) return;   // fault injection: the tile never arrives
-        tma::arrive_expect_tx(bar, bytes);
-        // coordinates (innermost first): X {k, j, c, i}, Y {k, c, i, x}
-        const int c1 = DIR == 0 ? outer : 0, c3 = DIR == 0 ? 0 : outer;
-        for (int v = 0; v < 4; v++) {
-            load_4d(tcur + v * fs, &maps.cur[v], k0, c1, 0, c3, bar);
-            if (v != DIR) load_4d(ttin + (v < DIR ? v : v - 1) * fs, &maps.tin[v], k0, c1, 0, c3, bar);
-        }
-        load_4d(twide, &maps.fwide, k0 - WOFF, c1, 0, c3, bar);
-        if (DIR == 0) {
-            load_4d(thm, &maps.tin[DIR], k0, outer - 1, 0, 0, bar);
-            load_4d(thp, &maps.tin[DIR], k0, outer + 1, 0, 0, bar);
-        } else {
-            load_4d(thm, &maps.tin[DIR], k0, 0, 0, outer - 1, bar);
-            load_4d(thp, &maps.tin[DIR], k0, 0, 0, outer + 1, bar);
-        }
-        load_4d(tcode, &maps.code, k0 & ~15, c1, 0, c3, bar);   // byte tiles start 16-byte aligned
-    };
-    if (t == 0) {
-        tma::mbar_init(bar, 1);
-        tma::fence_barrier_init();
-    }
+    ld.init(sm, t);
     __syncthreads();
-    if (t == 0 && (int)blockIdx.x < ntiles) issue(blockIdx.x);
+    uint64_t codes = (int)blockIdx.x < ntiles ? ld.issue(blockIdx.x, sm, fs, t) : 0;
 
     using namespace sweep;
     const int p0 = ch * K;
@@ -202,15 +173,16 @@ __global__ void __launch_bounds__(NLT * P, xy_ctas_per_sm((int)sizeof(R), K, NLT
 
     int it = 0;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
-        const int outer = tile / kblocks;
-        const int k0 = (tile - outer * kblocks) * NLT;
-        // Bounded wait.  A thread whose wait gave up computes on whatever the tile
-        // holds; the CTA checks every thread's wait at the release barrier and
-        // leaves before writing anything of this tile.
-        const bool tiles_ok = tma::mbar_wait(bar, it & 1, kc.tile_wait_tries);
+        const XYTileGeo geo = ld.geo(tile);
+        const SweepConst<R> &kc = ld.consts(geo);
+        // The tile's copies have landed (TMA: a bounded wait; a thread whose wait
+        // gave up computes on whatever the tile holds, and the CTA checks every
+        // thread's wait at the release barrier and leaves before writing anything
+        // of this tile).
+        const bool tiles_ok = ld.wait(it, sm, t, codes);
 
         // ---------------- rows from the tile: one pass, 3-row window ----------------
-        const int code_col = li + (k0 & 15);          // this line's byte in a code row
+        const int code_col = li + geo.code_off;       // this line's byte in a code row
         // window slots: 0 = row i-1, 1 = row i, 2 = row i+1.  cur is kept only for IN
         // rows (the reference vector of the increment form is 0 elsewhere).
         R cw[3][4], tw[3][4];
@@ -235,8 +207,7 @@ __global__ void __launch_bounds__(NLT * P, xy_ctas_per_sm((int)sizeof(R), K, NLT
         XY_LOAD_ROW(0, -1)
         XY_LOAD_ROW(1, 0)
         // global offset of this line's node 0: X (0, j, k) = j*nz + k; Y (i, 0, k) = i*ny*nz + k
-        const long long lb =
-            DIR == 0 ? (long long)outer * g.nz + k0 + li : (long long)outer * g.ny * g.nz + k0 + li;
+        const long long lb = geo.lb0 + li;
 #pragma unroll
         for (int i = 0; i < K; i++) {
             XY_LOAD_ROW(2, i + 1)
@@ -296,7 +267,7 @@ __global__ void __launch_bounds__(NLT * P, xy_ctas_per_sm((int)sizeof(R), K, NLT
                     const R cn = from_left ? cw[0][v] : cw[2][v];
                     dv[v][i] = fr ? cn
                                   : (kc.nv_in_temp ? tw[1][v]
-                                                   : __ldg(d.nv[v] + lb + (long long)(p0 + i) * g.stride));
+                                                   : __ldg(ld.nv(geo, v) + lb + (long long)(p0 + i) * geo.stride));
                 }
             }
 #pragma unroll
@@ -348,14 +319,11 @@ __global__ void __launch_bounds__(NLT * P, xy_ctas_per_sm((int)sizeof(R), K, NLT
         // Release barrier: every read of this tile is done, so the next tile's loads
         // may overwrite it; a thread whose wait gave up makes the whole CTA leave.
         if (__syncthreads_or(!tiles_ok)) {
-            if (t == 0) {
-                atomicExch(err_flag, 1);
-                // copies still in flight (none when the loads were never issued)
-                tma::mbar_wait(bar, it & 1, kc.tile_wait_tries < (1 << 10) ? kc.tile_wait_tries : 1 << 10);
-            }
+            if (t == 0) atomicExch(err_flag, 1);
+            ld.abandon(it, sm, t);
             break;
         }
-        if (t == 0 && tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x);
+        if (tile + (int)gridDim.x < ntiles) codes = ld.issue(tile + gridDim.x, sm, fs, t);
         {
             // Lane wc of a P-lane segment holds chunk wc of line wl.  Couplings to rows
             // outside the line are exactly zero (the first row of a line has a = 0, the
@@ -462,7 +430,7 @@ __global__ void __launch_bounds__(NLT * P, xy_ctas_per_sm((int)sizeof(R), K, NLT
         for (int i = 0; i < K; i++) {
             const int kd = (kinds >> (3 * i)) & 7;
             if (kd == R_NONE) continue;
-            const long long off = lb + (long long)(p0 + i) * g.stride;
+            const long long off = lb + (long long)(p0 + i) * geo.stride;
             R c[4];   // correction from the chunk-end unknowns
             if constexpr (sizeof(R) == 4) {
                 float2 c03, c12;
@@ -474,11 +442,13 @@ __global__ void __launch_bounds__(NLT * P, xy_ctas_per_sm((int)sizeof(R), K, NLT
                 }
                 const float2 x03 = add2(p2(dv[0][i], dv[3][i]), neg2(c03));
                 const float2 x12 = add2(p2(dv[1][i], dv[2][i]), neg2(c12));
-                next.f[0][off] = x03.x; next.f[3][off] = x03.y; next.f[1][off] = x12.x; next.f[2][off] = x12.y;
+                R *const n0 = ld.nextp(geo, 0), *const n1 = ld.nextp(geo, 1), *const n2 = ld.nextp(geo, 2), *const n3 = ld.nextp(geo, 3);
+                n0[off] = x03.x; n3[off] = x03.y; n1[off] = x12.x; n2[off] = x12.y;
                 if (kd == R_IN) {
                     const float2 m03 = fma2(bc2(-gm), c03, p2(gv[0][i], gv[3][i]));
                     const float2 m12 = fma2(bc2(-gm), c12, p2(gv[1][i], gv[2][i]));
-                    tout.f[0][off] = m03.x; tout.f[3][off] = m03.y; tout.f[1][off] = m12.x; tout.f[2][off] = m12.y;
+                    R *const t0 = ld.toutp(geo, 0), *const t1 = ld.toutp(geo, 1), *const t2 = ld.toutp(geo, 2), *const t3 = ld.toutp(geo, 3);
+                    t0[off] = m03.x; t3[off] = m03.y; t1[off] = m12.x; t2[off] = m12.y;
                 }
                 (void)c;
             } else {
@@ -486,8 +456,8 @@ __global__ void __launch_bounds__(NLT * P, xy_ctas_per_sm((int)sizeof(R), K, NLT
                 for (int v = 0; v < 4; v++) {
                     const int m = v < 3 ? 0 : 1;
                     c[v] = i == 0 ? -xf[v] : (i == K - 1 ? -xl[v] : ea[m][i] * xf[v] + ec[m][i] * xl[v]);
-                    next.f[v][off] = dv[v][i] - c[v];
-                    if (kd == R_IN) tout.f[v][off] = gv[v][i] - gm * c[v];
+                    ld.nextp(geo, v)[off] = dv[v][i] - c[v];
+                    if (kd == R_IN) ld.toutp(geo, v)[off] = gv[v][i] - gm * c[v];
                 }
             }
         }
@@ -669,15 +639,17 @@ cudaError_t launch_sweep_xytma(int dir, const DomainView<R> &d, const int *line_
     const int threads = nlt * P;
 #define XL(DD, KK, NN, PP)                                                                                       \
     if (dir == DD && K == KK && nlt == NN && P == PP) {                                                          \
-        auto kern = sweep_xytma_kernel<R, DD, KK, NN, PP>;                                                       \
+        using Ld = XYTmaLoader<R, DD, KK, NN, PP, XYTile<R, NN>::WIDE, XYTile<R, NN>::WOFF>;                      \
+        auto kern = sweep_xy_kernel<R, DD, KK, NN, PP, Ld>;                                                      \
         static SmemOptIn opt_in;                                                                                 \
         static PersistentGrid pgrid;                                                                             \
         cudaError_t e = ensure_dynamic_smem(opt_in, kern, smem);                                                 \
         if (e != cudaSuccess) return e;                                                                          \
         const int ctas = persistent_ctas(pgrid, kern, threads, smem);                                            \
         if (ctas <= 0) return cudaErrorInvalidConfiguration;                                                     \
-        kern<<<ctas < ntiles ? ctas : ntiles, threads, smem, s>>>(maps, d, g, next, tout, k, merges, ntiles,     \
-                                                                  err_flag);                                     \
+        Ld ld;                                                                                                   \
+        ld.maps = maps; ld.d = d; ld.next = next; ld.tout = tout; ld.kc = k; ld.kblocks = d.nz / NN;             \
+        kern<<<ctas < ntiles ? ctas : ntiles, threads, smem, s>>>(ld, merges, ntiles, err_flag);                 \
         return cudaGetLastError();                                                                               \
     }
 #define XLP(DD, KK, NN) XL(DD, KK, NN, 4) XL(DD, KK, NN, 8) XL(DD, KK, NN, 16)
@@ -693,11 +665,109 @@ cudaError_t launch_sweep_xytma(int dir, const DomainView<R> &d, const int *line_
     return cudaErrorInvalidConfiguration;
 }
 
+// ---------------------------------------------------------------------------
+// element-wise (cp.async) tiles: any nz and line length, one domain or a batch
+// ---------------------------------------------------------------------------
+
+// Chunks per line of the cp.async shapes: 8 lines per CTA, K = 4 with 16 or 32
+// chunks (lines up to 64 / 128 rows), K = 5 with 32 (up to 160 rows).
+static int xycp_chunks(int L, int K)
+{
+    if (K == 4) return L <= 64 ? 16 : (L <= 128 ? 32 : 0);
+    if (K == 5) return L <= 160 ? 32 : 0;
+    return 0;
+}
+
+bool xycp_supported(int dir, int nx, int ny, int nz, int K, int elem_bytes)
+{
+    if (dir > 1 || nx < 3 || ny < 3 || nz < 3) return false;
+    const int L = dir == 0 ? nx : ny;
+    const int P = xycp_chunks(L, K);
+    if (P == 0) return false;
+    const size_t budget = 228 * 1024 / xy_ctas_per_sm(elem_bytes, K, 8, P) - 1024;
+    return xytma_smem_bytes(P * K, P, 8, elem_bytes) <= (budget < 227 * 1024 ? budget : 227 * 1024);
+}
+
+template <typename R>
+cudaError_t launch_sweep_xycp(int dir, const DomainView<R> &d, CLayer<R> cur, CLayer<R> tin, Layer<R> next,
+                              Layer<R> tout, const SweepConst<R> &k, int merges, int K, int *err_flag, cudaStream_t s)
+{
+    const int es = (int)sizeof(R);
+    if (!xycp_supported(dir, d.nx, d.ny, d.nz, K, es)) return cudaErrorInvalidConfiguration;
+    const int L = dir == 0 ? d.nx : d.ny;
+    const int P = xycp_chunks(L, K);
+    const size_t smem = xytma_smem_bytes(P * K, P, 8, es);
+    const int kblocks = (d.nz + 7) / 8;
+    const int ntiles = (dir == 0 ? d.ny : d.nx) * kblocks;
+    const int threads = 8 * P;
+#define XC(DD, KK, PP)                                                                                           \
+    if (dir == DD && K == KK && P == PP) {                                                                       \
+        using Ld = XYCpLoader<R, DD, KK, 8, PP, XYTile<R, 8>::WIDE, XYTile<R, 8>::WOFF>;                          \
+        auto kern = sweep_xy_kernel<R, DD, KK, 8, PP, Ld>;                                                       \
+        static SmemOptIn opt_in;                                                                                 \
+        static PersistentGrid pgrid;                                                                             \
+        cudaError_t e = ensure_dynamic_smem(opt_in, kern, smem);                                                 \
+        if (e != cudaSuccess) return e;                                                                          \
+        const int ctas = persistent_ctas(pgrid, kern, threads, smem);                                            \
+        if (ctas <= 0) return cudaErrorInvalidConfiguration;                                                     \
+        Ld ld;                                                                                                   \
+        ld.cur = cur; ld.tin = tin; ld.d = d; ld.next = next; ld.tout = tout; ld.kc = k;                         \
+        ld.kblocks = kblocks; ld.L = L;                                                                          \
+        kern<<<ctas < ntiles ? ctas : ntiles, threads, smem, s>>>(ld, merges, ntiles, err_flag);                 \
+        return cudaGetLastError();                                                                               \
+    }
+    XC(0, 4, 16) XC(1, 4, 16) XC(0, 4, 32) XC(1, 4, 32) XC(0, 5, 32) XC(1, 5, 32)
+#undef XC
+    return cudaErrorInvalidConfiguration;
+}
+
+// The X or Y sweep of every domain of a batch in one persistent launch over the
+// (domain, tile) work items; every domain's line length in the direction must be
+// at most 32 K rows.
+template <typename R>
+cudaError_t launch_sweep_xy_batch(int dir, int K, const BatchDomain<R> *doms, const int2 *items, int nitems, int src,
+                                  int tin, int dst, int tout, int merges, int *err_flag, cudaStream_t s)
+{
+    if (nitems == 0) return cudaSuccess;
+    const int es = (int)sizeof(R);
+    constexpr int P = 32;
+    const size_t smem = xytma_smem_bytes(P * K, P, 8, es);
+#define XB(DD, KK)                                                                                               \
+    if (dir == DD && K == KK) {                                                                                  \
+        using Ld = XYBatchLoader<R, DD, KK, 8, P, XYTile<R, 8>::WIDE, XYTile<R, 8>::WOFF>;                        \
+        auto kern = sweep_xy_kernel<R, DD, KK, 8, P, Ld>;                                                        \
+        static SmemOptIn opt_in;                                                                                 \
+        static PersistentGrid pgrid;                                                                             \
+        cudaError_t e = ensure_dynamic_smem(opt_in, kern, smem);                                                 \
+        if (e != cudaSuccess) return e;                                                                          \
+        const int ctas = persistent_ctas(pgrid, kern, 8 * P, smem);                                              \
+        if (ctas <= 0) return cudaErrorInvalidConfiguration;                                                     \
+        Ld ld;                                                                                                   \
+        ld.doms = doms; ld.items = items; ld.src = src; ld.tin = tin; ld.dst = dst; ld.tout = tout;              \
+        kern<<<ctas < nitems ? ctas : nitems, 8 * P, smem, s>>>(ld, merges, nitems, err_flag);                   \
+        return cudaGetLastError();                                                                               \
+    }
+    XB(0, 4) XB(1, 4) XB(0, 5) XB(1, 5)
+#undef XB
+    return cudaErrorInvalidConfiguration;
+}
+
 template cudaError_t launch_sweep_xytma<float>(int, const DomainView<float> &, const int *, CLayer<float>,
                                                CLayer<float>, Layer<float>, Layer<float>, const SweepConst<float> &,
                                                int, int, int, int *, cudaStream_t);
 template cudaError_t launch_sweep_xytma<double>(int, const DomainView<double> &, const int *, CLayer<double>,
                                                 CLayer<double>, Layer<double>, Layer<double>,
                                                 const SweepConst<double> &, int, int, int, int *, cudaStream_t);
+
+template cudaError_t launch_sweep_xycp<float>(int, const DomainView<float> &, CLayer<float>, CLayer<float>,
+                                              Layer<float>, Layer<float>, const SweepConst<float> &, int, int, int *,
+                                              cudaStream_t);
+template cudaError_t launch_sweep_xycp<double>(int, const DomainView<double> &, CLayer<double>, CLayer<double>,
+                                               Layer<double>, Layer<double>, const SweepConst<double> &, int, int,
+                                               int *, cudaStream_t);
+template cudaError_t launch_sweep_xy_batch<float>(int, int, const BatchDomain<float> *, const int2 *, int, int, int,
+                                                  int, int, int, int *, cudaStream_t);
+template cudaError_t launch_sweep_xy_batch<double>(int, int, const BatchDomain<double> *, const int2 *, int, int, int,
+                                                   int, int, int, int *, cudaStream_t);
 
 } // namespace adi

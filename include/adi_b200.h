@@ -271,8 +271,12 @@ adi_status adi_div_error(adi_handle *h, double *out);
  * line.  NL = 0 selects the warp-resident Z kernel (Z only; dimz = P*K with P in
  * {4, 8, 16, 32}, K in {4, 8}); NL = -16 and NL = -8 select the TMA-fed X/Y
  * kernel with 16 or 8 lines per CTA (dimz a multiple of 16, K in {4, 8, 16},
- * line length = P K with P in {4, 8, 16} or P = 32 at K = 4, at most 512 threads,
- * tiles within the shared memory of the CTAs per SM the shape is compiled for);
+ * line length = P K with P in {4, 8, 16} or P = 32 at K = 4, or, in float with
+ * K = 4 and 8 lines, P = 64 or 96 (lines of 256 or 384 rows), tiles within the
+ * shared memory of the CTAs per SM the shape is compiled for); NL = -1 selects
+ * the same X/Y kernel with tiles of 8 lines copied element by element by the
+ * CTA's threads (cp.async), for any dimz and lines up to 128 rows (K = 4) or
+ * 160 rows (K = 5);
  * NL = -32 selects the persistent, double-buffered X/Y kernel with
  * two lines per thread (FP32 only; dimz a multiple of 16, K in {4, 8}, 2 <= P <= 32,
  * both tile buffers within 227 KB of shared memory, e.g. line length <= 136 at
@@ -450,8 +454,12 @@ adi_status adi_batch_step(adi_batch *b, double dt, int num_global, int num_local
 /* Last computed divergence error of each member (n values). */
 adi_status adi_batch_div_errors(adi_batch *b, double *out);
 
-/* Chunk length K in {4, 8} of the batched sweep per direction (segment-to-thread
- * binning), and the autotuner that times both per direction at dt. */
+/* Kernel and chunk length of the batched sweep per direction (segment-to-thread
+ * binning): K in {4, 8} runs the generic chunked kernel over (domain, lines)
+ * items; for X and Y, K = -4 or -5 runs the tile kernel over (domain, tile of 8
+ * lines) items, tiles copied element-wise, chunks of |K| rows, every member's
+ * line length at most 32 |K| (else ADI_ERR_CAPACITY).  The autotuner times every
+ * choice per direction at dt and keeps the fastest. */
 adi_status adi_batch_set_chunk(adi_batch *b, int dir, int K);
 adi_status adi_batch_get_chunk(adi_batch *b, int dir, int *K);
 adi_status adi_batch_autotune(adi_batch *b, double dt, int reps);

@@ -1,9 +1,10 @@
 """GPU checks of batched stepping (adi_batch_*).
 
 A batch runs every member through the generic chunked sweep with the batch's
-chunk length K and lines-per-CTA max(1, 256 // P), so each member must come out
-bit for bit as the same domain stepped alone with that fast-sweep shape; one member
-is also compared with the FP64 oracle at float tolerance (2e-6 of the field scale).
+chunk length K and lines-per-CTA max(1, 256 // P), or, for X and Y with K < 0, the
+tile kernel with element-copied tiles of 8 lines, so each member must come out bit
+for bit as the same domain stepped alone with that fast-sweep shape; one member is
+also compared with the FP64 oracle at float tolerance (2e-6 of the field scale).
 """
 import numpy as np
 import pytest
@@ -36,16 +37,21 @@ def _member(adi_lib, d, solver=None, precision=None):
 
 
 def _alone(adi_lib, d, K):
-    """The same domain stepped by itself with the batch's generic-sweep shape."""
+    """The same domain stepped by itself with the batch's sweep shape per direction:
+    the generic kernel with chunks of K rows and max(1, 256 // P) lines per CTA, or
+    for K < 0 the X/Y tile kernel with element-copied tiles and chunks of -K rows."""
     from adi_b200 import _abi
     s = _member(adi_lib, d, solver=_abi.ADI_SOLVER_FAST)
     for dr in range(3):
+        if K[dr] < 0:
+            s.set_fast_shape(dr, -K[dr], -1)
+            continue
         P = -(-d.shape[dr] // K[dr])
         s.set_fast_shape(dr, K[dr], max(1, 256 // P))
     return s
 
 
-@pytest.mark.parametrize("K", [(4, 4, 4), (8, 8, 8), (4, 8, 4)])
+@pytest.mark.parametrize("K", [(4, 4, 4), (8, 8, 8), (4, 8, 4), (-4, -4, 4), (-5, -5, 8)])
 def test_batch_matches_members_stepped_alone(adi_lib, K):
     ds = _domains(7)
     members = [_member(adi_lib, d) for d in ds]
@@ -91,7 +97,7 @@ def test_batch_graph_replay_and_autotune(adi_lib):
     mb = [_member(adi_lib, d) for d in ds]
     a, b = adi_lib.AdiBatch(ma), adi_lib.AdiBatch(mb)
     a.autotune(6e-4, 2)
-    assert all(k in (4, 8) for k in a.chunks())
+    assert all(k in (4, 8, -4, -5) for k in a.chunks()) and a.chunks()[2] > 0
     for dr, k in enumerate(a.chunks()):
         b.set_chunk(dr, k)
     b.set_graphs(False)

@@ -187,6 +187,31 @@ def test_xytma_lines_over_several_warps(adi_lib, nx):
     assert max(errs_n) < 2e-6, errs_n
 
 
+@pytest.mark.parametrize("dims,xK", [((61, 45, 37), 4), ((150, 37, 29), 5), ((100, 120, 33), 4)],
+                         ids=["61x45x37-K4", "150x37x29-K5", "100x120x33-K4"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_xy_tiles_copied_elementwise_any_dims(adi_lib, dims, xK, precision):
+    """The X/Y tile kernel with tiles copied element by element (NL = -1): dimz not a
+    multiple of the 8-line tile (the last tile of each plane is partly padding) and
+    line lengths that are not P K (rows past the line end are padding rows)."""
+    from adi_b200 import _abi
+    d = G.random_domain(*dims, seed=85, shell=True, n_obstacles=9, rmax=5.0)
+    params = (125.0, 0.72, 1.4)
+    prec = _abi.ADI_FP64 if precision == "fp64" else _abi.ADI_FP32
+    s = solver(adi_lib, d, params, precision=prec, shapes=[(xK, -1), (xK, -1), (4, 8)])
+    assert s.fast_shapes()[0][:2] == (xK, -1) and s.fast_shapes()[1][:2] == (xK, -1)
+    orc = O.OracleSolver(d, precision=8, params=fluid_params_tuple(("normalized", params)))
+    m = non_out(d)
+    for _ in range(3):
+        assert s.step(8e-4, 4, 2, True) == 0
+        assert orc.step(8e-4, 4, 2, True) == 0
+    tol = 1e-11 if precision == "fp64" else 2e-6
+    errs = rel_errors(s.fields(0), orc.fields(0), m)
+    assert max(errs) < tol, errs
+    errs_n = rel_errors(s.fields(1), orc.fields(1), m)
+    assert max(errs_n) < tol, errs_n
+
+
 def _slab_domain(nx, ny, nz, seed):
     """Random shell domain plus a wall slab at k = 1..16, so that the first 16-line
     tile of every X and Y plane holds no segment (the persistent kernel skips it)."""

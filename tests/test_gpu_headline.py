@@ -36,7 +36,7 @@ DT = 5e-4
 # X/Y sweep with 8 / 16 lines per CTA, NL = 0 the warp-resident Z sweep.
 HEADLINE_SHAPES = [
     [(4, -8), (4, -8), (4, 0)],
-    [(4, -16), (4, -16), (8, 0)],
+    [(4, -8), (8, -16), (8, 0)],
     [(8, -8), (8, -8), (4, 0)],
     [(8, -16), (8, -16), (4, 0)],
 ]
