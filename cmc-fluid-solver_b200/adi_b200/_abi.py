@@ -39,7 +39,8 @@ EXPORTED = [
     "adi2d_update_boundaries", "adi2d_time_step", "adi2d_step", "adi2d_get_state", "adi2d_set_state",
     "adi2d_get_layer", "adi2d_last_error", "adi2d_last_error_string",
     "adi_mask_shape3d", "adi_mask_sea", "adi_mask_extrude2d", "adi_get_mask", "adi_mask_shape2d",
-    "adi_set_fault_injection",
+    "adi_set_fault_injection", "adi_phase_begin", "adi_phase_sweep", "adi_phase_div_sum", "adi_phase_end",
+    "adi_role_pointers",
 ]
 
 K_NUM = 7
@@ -99,6 +100,11 @@ def load() -> C.CDLL:
         "adi_set_stream": [vp, vp],
         "adi_set_solver": [vp, i],
         "adi_set_fault_injection": [vp, i],
+        "adi_phase_begin": [vp, i],
+        "adi_phase_sweep": [vp, i, C.c_double, i],
+        "adi_phase_div_sum": [vp, i, C.POINTER(C.c_double), C.POINTER(C.c_uint64)],
+        "adi_phase_end": [vp],
+        "adi_role_pointers": [vp, i, C.c_void_p],
         "adi_set_mask": [vp] + [vp] * 7,
         "adi_mask_shape3d": [vp, vp, i, vp, i, d, C.POINTER(i)],
         "adi_mask_sea": [vp, vp, i, i, C.c_float, d, vp, d],

@@ -334,10 +334,22 @@ cudaError_t launch_fast(adi_handle *h, int dir, CLayer<R> cur, CLayer<R> tin, La
 // Y (next -> half), X (half -> next), each num_local times, every sweep merging
 // into the nonlinear layer; the last X sweep merges twice (the extra merge after
 // X).  The two nonlinear buffers swap roles after every sweep.
+// One sweep of direction dir from layer src into layer dst, reading the nonlinear
+// layer ta and writing tb (the caller swaps them).
+template <typename R>
+cudaError_t launch_sweep_once(adi_handle *h, int dir, int src, int dst, const SweepConst<R> &k, int merges)
+{
+    if (h->solver == ADI_SOLVER_FAST)
+        return launch_fast<R>(h, dir, clayer<R>(h, src), clayer<R>(h, h->ta), layer<R>(h, dst), layer<R>(h, h->tb), k,
+                              merges, h->shape[dir]);
+    return launch_sweep_exact<R>(dir, view<R>(h), h->d_line_lo[dir], h->d_line_hi[dir], clayer<R>(h, src),
+                                 clayer<R>(h, h->ta), layer<R>(h, dst), layer<R>(h, h->tb), (R *)h->d_scratch, k,
+                                 merges, h->stream);
+}
+
 template <typename R>
 adi_status enqueue_global_iteration(adi_handle *h, R dt, int num_local, void *const *tape = nullptr)
 {
-    const DomainView<R> d = view<R>(h);
     const int order[3] = {2, 1, 0};
     const int src[3] = {h->cur, h->nxt, h->half};
     const int dst[3] = {h->nxt, h->half, h->nxt};
@@ -353,14 +365,7 @@ adi_status enqueue_global_iteration(adi_handle *h, R dt, int num_local, void *co
             const size_t fb = (size_t)h->n * sizeof(R);
             if (tape && q == 0 && l == 0)   // the nonlinear layer the first sweep reads
                 CK(launch_copy_fields(4, h->d_L[h->ta], tape, fb, h->stream));
-            CK(timed(h, cls, bytes, [&] {
-                if (h->solver == ADI_SOLVER_FAST)
-                    return launch_fast<R>(h, dir, clayer<R>(h, src[q]), clayer<R>(h, h->ta), layer<R>(h, dst[q]),
-                                          layer<R>(h, h->tb), k, merges, h->shape[dir]);
-                return launch_sweep_exact<R>(dir, d, h->d_line_lo[dir], h->d_line_hi[dir], clayer<R>(h, src[q]),
-                                             clayer<R>(h, h->ta), layer<R>(h, dst[q]), layer<R>(h, h->tb),
-                                             (R *)h->d_scratch, k, merges, h->stream);
-            }));
+            CK(timed(h, cls, bytes, [&] { return launch_sweep_once<R>(h, dir, src[q], dst[q], k, merges); }));
             if (tape) {
                 // the layer it wrote, and (in the same launch) the nonlinear layer it
                 // wrote, which the next sweep of this iteration reads
@@ -866,6 +871,14 @@ adi_status adjoint_run(adi_handle *h, double dt, int ng, int nl, int n_steps, in
     }
     CK(cudaStreamSynchronize(h->stream));
     return check_device_flag(h);
+}
+
+// Layer index of a role: 0 cur, 1 next, 2 half, 3 the nonlinear layer the next
+// sweep reads, 4 the one it writes.
+int role_layer(const adi_handle *h, int role)
+{
+    const int l[5] = {h->cur, h->nxt, h->half, h->ta, h->tb};
+    return l[role];
 }
 
 adi_status check_ready(adi_handle *h)
@@ -1429,6 +1442,71 @@ static adi_status step_impl(adi_handle *h, double dt, int num_global, int num_lo
     if (!(dt > 0) || !std::isfinite(dt)) return fail(h, ADI_ERR_BAD_ARG, "dt must be positive and finite");
     if (h->prec == ADI_FP64) return time_step<double>(h, dt, num_global, num_local, compute_error, bnd);
     return time_step<float>(h, dt, num_global, num_local, compute_error, bnd);
+}
+
+// ---- step phases (decompositions that exchange data between sweeps) ----
+
+adi_status adi_phase_begin(adi_handle *h, int update_boundaries)
+{
+    adi_status s = check_ready(h);
+    if (s != ADI_OK) return s;
+    const bool ub = update_boundaries != 0;
+    if (ub) h->bv_synced = true;   // step_begin applies the boundary values first
+    if (h->prec == ADI_FP64)
+        CK(launch_step_begin<double>(view<double>(h), layer<double>(h, h->cur), layer<double>(h, h->nxt),
+                                     layer<double>(h, h->ta), layer<double>(h, h->tb), ub, h->stream));
+    else
+        CK(launch_step_begin<float>(view<float>(h), layer<float>(h, h->cur), layer<float>(h, h->nxt),
+                                    layer<float>(h, h->ta), layer<float>(h, h->tb), ub, h->stream));
+    h->launches[ADI_K_STEP_BEGIN]++;
+    return ADI_OK;
+}
+
+adi_status adi_phase_sweep(adi_handle *h, int dir, double dt, int merges)
+{
+    adi_status s = check_ready(h);
+    if (s != ADI_OK) return s;
+    if (dir < 0 || dir > 2 || (merges != 1 && merges != 2)) return fail(h, ADI_ERR_BAD_ARG, "bad sweep phase");
+    if (!(dt > 0) || !std::isfinite(dt)) return fail(h, ADI_ERR_BAD_ARG, "dt must be positive and finite");
+    const int src = dir == 2 ? h->cur : (dir == 1 ? h->nxt : h->half);
+    const int dst = dir == 2 ? h->nxt : (dir == 1 ? h->half : h->nxt);
+    if (h->prec == ADI_FP64) CK(launch_sweep_once<double>(h, dir, src, dst, sweep_const<double>(h, dir, dt), merges));
+    else CK(launch_sweep_once<float>(h, dir, src, dst, sweep_const<float>(h, dir, (float)dt), merges));
+    h->launches[dir == 0 ? ADI_K_SWEEP_X : (dir == 1 ? ADI_K_SWEEP_Y : ADI_K_SWEEP_Z)]++;
+    std::swap(h->ta, h->tb);
+    return ADI_OK;
+}
+
+adi_status adi_phase_div_sum(adi_handle *h, int role, double *sum, uint64_t *count)
+{
+    if (!h || !sum || !count || role < 0 || role > 4) return ADI_ERR_BAD_ARG;
+    adi_status s = check_ready(h);
+    if (s != ADI_OK) return s;
+    const int l = role_layer(h, role);
+    s = h->prec == ADI_FP64 ? enqueue_div_error<double>(h, l) : enqueue_div_error<float>(h, l);
+    if (s != ADI_OK) return s;
+    double mean = 0.0;
+    s = read_div_error(h, &mean);
+    *sum = h->h_pin->sum;
+    *count = h->h_pin->cnt;
+    return s;
+}
+
+adi_status adi_phase_end(adi_handle *h)
+{
+    adi_status s = check_ready(h);
+    if (s != ADI_OK) return s;
+    std::swap(h->cur, h->nxt);
+    h->bv_synced = false;   // the new state holds the sweeps' boundary values
+    return ADI_OK;
+}
+
+adi_status adi_role_pointers(adi_handle *h, int role, void **out4)
+{
+    if (!h || !out4 || role < 0 || role > 4) return ADI_ERR_BAD_ARG;
+    const int l = role_layer(h, role);
+    for (int v = 0; v < 4; v++) out4[v] = h->d_L[l][v];
+    return ADI_OK;
 }
 
 adi_status adi_time_step(adi_handle *h, double dt, int num_global, int num_local, int compute_error)

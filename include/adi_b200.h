@@ -244,6 +244,28 @@ adi_status adi_step_tol(adi_handle *h, double dt, int max_global, int num_local,
  * and adi_set_solver.  Default on. */
 adi_status adi_set_graphs(adi_handle *h, int on);
 
+/* ---- step phases --------------------------------------------------------- */
+
+/* The parts of adi_step one at a time, for hosts that split a domain over
+ * several handles and exchange data between sweeps (no counterpart in the
+ * reference's single-process step; the reference's multi-GPU slab solver,
+ * AdiSolver3D.cu:523-881, exchanges inside its sweeps).  A step is:
+ *   adi_phase_begin(h, 1)                 UpdateBoundaries + the step start
+ *   per global iteration: adi_phase_sweep for Z, Y, X, each num_local times
+ *                         (merges = 2 on the last X sweep of the iteration)
+ *   adi_phase_div_sum(h, ADI_ROLE_NEXT)   optional: divergence sum and IN count
+ *   adi_phase_end(h)                      the new state becomes cur
+ * Sweeps read and write the handle's layers by role; adi_role_pointers gives a
+ * role's four field arrays (U, V, W, T) on the device, valid until the roles next
+ * change (every sweep swaps the two nonlinear layers; adi_phase_end swaps cur and
+ * next).  Asynchronous on the handle's stream, except adi_phase_div_sum. */
+enum { ADI_ROLE_CUR = 0, ADI_ROLE_NEXT = 1, ADI_ROLE_HALF = 2, ADI_ROLE_TEMP_IN = 3, ADI_ROLE_TEMP_OUT = 4 };
+adi_status adi_phase_begin(adi_handle *h, int update_boundaries);
+adi_status adi_phase_sweep(adi_handle *h, int dir, double dt, int merges);
+adi_status adi_phase_div_sum(adi_handle *h, int role, double *sum, uint64_t *count);
+adi_status adi_phase_end(adi_handle *h);
+adi_status adi_role_pointers(adi_handle *h, int role, void **out4);
+
 /* ---- fields ------------------------------------------------------------ */
 
 /* Layers: 0 = cur (latest state), 1 = next (scratch layer of the last step). */
