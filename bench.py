@@ -103,7 +103,9 @@ CONFIGS = {
     "batched64": dict(make=_batched64, batch=True, Pr=0.72, lam=1.4, dt=5e-4, ng=4, nl=2,
                       desc="batched: 64 independent 3D FP32 domains, axes U{64..160} (seed 2), 10-60 solid spheres "
                            "each (radii U[4,12]), Re U[50,400], dt=5e-4, num_global=4, num_local=2; all domains "
-                           "in one persistent launch per sweep, step replayed as a CUDA graph"),
+                           "stepped as one batch, the step replayed as one CUDA graph (schedule autotuned: one "
+                           "persistent multi-domain launch per sweep, or every member's own kernels on "
+                           "concurrent graph branches)"),
     "adjoint128": dict(make=_spheres128, adjoint=True, Re=200.0, Pr=0.72, lam=1.4, dt=5e-4, ng=4, nl=2,
                        n_steps=40, ckpt=8, box=((80, 48, 48), (112, 80, 80)), near_box=((2, 48, 48), (34, 80, 80)),
                        desc="adjoint: 128^3 FP32, 40 spheres (seed 0), Re=200, dt=5e-4, num_global=4, num_local=2, "
@@ -400,7 +402,8 @@ def run_reference(args):
         with stdout_to_stderr():
             value, done, el = cpu_reference_batch(domains, cfg, args.ref_budget)
         cores = int(os.environ["OMP_NUM_THREADS"])
-        sample = f"one step of each of the first {done} of {len(domains)} domains ({el:.1f} s), OpenMP {cores} threads"
+        sample = (f"one step of each of {done} of {len(domains)} domains in order ({el:.1f} s; domains with more "
+                  f"segments than the reference's fixed segment lists hold passed over), OpenMP {cores} threads")
         print(json.dumps({
             "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
             "steps": 1, "warmup": 0, "ms_per_step": 1e3 * el, "higher_is_better": True, "scaling": "weak",
@@ -454,13 +457,15 @@ def run_ours(args):
     dt, ng, nl = cfg["dt"], cfg["ng"], cfg["nl"]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
-    def one_step(i):
-        rc = s.step(dt, ng, nl, i % 10 == 0)
+    def one_step(i, ce=None):
+        rc = s.step(dt, ng, nl, i % 10 == 0 if ce is None else ce)
         if rc != 0:
             raise RuntimeError(f"adi_step failed with status {rc}")
 
+    # warm-up: the first two steps with the divergence error (both layer parities),
+    # so no step graph is captured inside the timed region
     for i in range(args.warmup):
-        one_step(i)
+        one_step(i, i < 2 or i % 10 == 0)
     torch.cuda.synchronize()
 
     def barrier():
@@ -649,13 +654,18 @@ def accuracy_batch_member(d, Re, Pr, lam, dt, ng, nl, steps, chunks, stream):
 
 def cpu_reference_batch(domains, cfg, budget_s: float):
     """The reference CPU solver stepping the batch's domains one after another, one
-    step each, until budget_s has passed.  Returns (cell-steps/s, domains stepped, s)."""
+    step each, until budget_s has passed; domains with more segments than the
+    reference's fixed-size segment lists hold are passed over.  Returns (cell-steps/s,
+    domains stepped, s)."""
     import oracle as O
     if not O.have_ref():
         O.build()
     done, cells, el = 0, 0, 0.0
     for d in domains:
-        ref = O.RefSolver(d, Re=d.meta["Re"], Pr=cfg["Pr"], lam=cfg["lam"])
+        try:
+            ref = O.RefSolver(d, Re=d.meta["Re"], Pr=cfg["Pr"], lam=cfg["lam"])
+        except ValueError:
+            continue   # more segments than the reference's fixed-size segment lists hold
         t0 = time.perf_counter()
         ref.step(cfg["dt"], cfg["ng"], cfg["nl"], True)
         el += time.perf_counter() - t0
@@ -688,12 +698,22 @@ def run_batch(args):
     dt, ng, nl = cfg["dt"], cfg["ng"], cfg["nl"]
     members, stats = [], []
     for d in mine:
+        # fast solver: CreateSegments autotunes each member's own kernels, which the
+        # member-graph schedule runs (the persistent schedule uses the batch kernels)
         m = adi_b200.AdiSolver3D(d, Re=d.meta["Re"], Pr=cfg["Pr"], lam=cfg["lam"], precision=adi_b200.ADI_FP32,
-                                 solver=adi_b200.ADI_SOLVER_EXACT, stream=stream.cuda_stream)
+                                 solver=adi_b200.ADI_SOLVER_FAST, stream=stream.cuda_stream)
         stats.append(m.CreateSegments())
         members.append(m)
     batch = adi_b200.AdiBatch(members, stream=stream.cuda_stream)
     batch.autotune(dt, 2)
+    schedule = batch.schedule()
+    # both schedules' whole-step times (graph replays), for the record
+    sched_ms = {}
+    for name, sc, br in (("persistent", adi_b200.ADI_BATCH_PERSISTENT, 1),
+                         ("member_graphs", adi_b200.ADI_BATCH_MEMBER_GRAPHS, schedule[1] if schedule[0] else 2)):
+        batch.set_schedule(sc, br)
+        sched_ms[name] = batch.time_step(dt, ng, nl, 2)
+    batch.set_schedule(*schedule)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     def barrier():
@@ -701,13 +721,15 @@ def run_batch(args):
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
-    def one_step(i):
-        rc = batch.step(dt, ng, nl, i % 10 == 0)
+    def one_step(i, ce=None):
+        rc = batch.step(dt, ng, nl, i % 10 == 0 if ce is None else ce)
         if rc != 0:
             raise RuntimeError(f"adi_batch_step failed with status {rc}")
 
+    # warm-up: both layer parities with and without the divergence error, so no
+    # batch graph is captured inside the timed region
     for i in range(args.warmup):
-        one_step(i)
+        one_step(i, i < 2 or i % 10 == 0)
     barrier()
     clocks = ClockSampler(local)
     clocks.start()
@@ -766,12 +788,9 @@ def run_batch(args):
     # ---- the same domains stepped one at a time (plain per-domain steps) ----
     plain = None
     if world == 1 and not args.no_plain_loop:
-        for m in members:
-            m._check(m.lib.adi_set_solver(m.h, adi_b200.ADI_SOLVER_FAST))
-            m.autotune(1)
-        for i in range(2):
+        for i in range(4):   # every member's step graphs, as for the batch
             for m in members:
-                m.step(dt, ng, nl, False)
+                m.step(dt, ng, nl, i < 2)
         barrier()
         p0 = torch.cuda.Event(enable_timing=True)
         p1 = torch.cuda.Event(enable_timing=True)
@@ -786,6 +805,21 @@ def run_batch(args):
         barrier()
         plain = {"value": my_cells * psteps / (p0.elapsed_time(p1) / 1e3), "unit": METRIC, "steps": psteps,
                  "how": "the same domains, adi_step one domain at a time, each with its own autotuned fast shapes"}
+    # the members' own sweeps (what the member-graph schedule runs): algorithmic
+    # bytes / per-launch CUDA-event time summed over one profiled step of each member
+    member_roof = None
+    if world == 1 and not args.no_plain_loop:
+        mb = mms = 0.0
+        for m in members:
+            m.set_profiling(True)
+            m.profile(reset=True)
+            m.step(dt, ng, nl, False)
+            pr = m.profile(reset=True)
+            m.set_profiling(False)
+            for k in ("sweep_x", "sweep_y", "sweep_z"):
+                mb += pr[k]["bytes"]
+                mms += pr[k]["ms"]
+        member_roof = {"kernel": "members' own sweeps", "achieved": mb / (mms / 1e3) / 1e9}
 
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -793,6 +827,9 @@ def run_batch(args):
         "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(args, cfg, all_cells),
         "run": {"domains": len(domains), "domains_this_rank": len(mine), "chunk_K_xyz": batch.chunks(),
+                "schedule": ("member graphs on %d branches" % schedule[1]) if schedule[0] else
+                            "persistent multi-domain launch per sweep",
+                "schedule_ms_per_step": sched_ms,
                 "parallelism": (f"domains LPT-sharded over {world} ranks (loads "
                                 f"{[int(x) for x in part_loads(costs, parts)]})" if world > 1 else "one batch")},
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 16 * my_cells,
@@ -803,8 +840,12 @@ def run_batch(args):
                                                                                      "sweep_fast_batch_kernel"),
                      "kernel": "sweep_fast_batch_kernel", "peak_source": peak_kind,
                      "per_direction_ms_per_launch": sweep_ms,
-                     "algorithmic_bytes_per_launch": sweep_bytes},
+                     "algorithmic_bytes_per_launch": sweep_bytes,
+                     "note": "the persistent schedule's batched sweep (time_sweeps)"},
         "plain_per_domain": plain,
+        "roofline_member_sweeps": (dict(member_roof, peak=peak, unit="GB/s",
+                                        frac=member_roof["achieved"] / peak if peak else None)
+                                   if member_roof else None),
         "clocks": clk,
     }
     if rank == 0:
@@ -822,8 +863,10 @@ def run_batch(args):
             v, done, el = cpu_reference_batch(domains, cfg, args.cpu_budget)
         line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": int(os.environ["OMP_NUM_THREADS"]),
                                 "kind": "reference",
-                                "sample": f"one step of each of the first {done} domains ({el:.1f} s) on the "
-                                          f"reference CPU solver, OpenMP {os.environ['OMP_NUM_THREADS']} threads"}
+                                "sample": f"one step of each of {done} domains in order ({el:.1f} s; domains "
+                                          f"with more segments than the reference's fixed segment lists hold "
+                                          f"passed over) on the reference CPU solver, OpenMP "
+                                          f"{os.environ['OMP_NUM_THREADS']} threads"}
     if rank == 0:
         emit(args, line)
     batch.close()
@@ -1203,8 +1246,10 @@ def main():
                     help='fast sweep shapes "K,NL;K,NL;K,NL" for X;Y;Z instead of the autotuned ones '
                          '(profiling runs pin them: timings under a profiler mislead the autotuner)')
     args = ap.parse_args()
-    if args.warmup < 3 and args.impl == "ours":
-        args.warmup = 3
+    if args.warmup < 4 and args.impl == "ours":
+        # the warm-up steps replay-capture every step graph the timed steps use:
+        # with and without the divergence error, for both layer parities
+        args.warmup = 4
     if args.impl == "reference":
         return run_reference(args)
     if CONFIGS[args.config].get("batch"):
@@ -1252,7 +1297,9 @@ def run_extras(args):
         "workload": b["config"]["workload"], "cells": b["config"]["cells"], "value": b["value"], "unit": METRIC,
         "ms_per_step": b["ms_per_step"], "steps": b["steps"], "plain_per_domain_value": plain,
         "batched_over_plain": b["value"] / plain if plain else None,
+        "schedule": b["run"]["schedule"], "schedule_ms_per_step": b["run"]["schedule_ms_per_step"],
         "roofline": {k: b["roofline"][k] for k in ("kernel", "achieved", "peak", "frac", "unit")},
+        "roofline_member_sweeps": b.get("roofline_member_sweeps"),
         "accuracy_max_rel_err_vs_fp64": max(b["accuracy"]["max_rel_err_vs_fp64"].values()),
         "e2e": b["e2e"], "gpu_launches": b["gpu_launches"], "clocks": b["clocks"], "wall_s": wall,
     }

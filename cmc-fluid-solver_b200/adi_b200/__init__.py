@@ -12,7 +12,8 @@ import ctypes as C
 import numpy as np
 
 from . import _abi
-from ._abi import ADI_FP32, ADI_FP64, ADI_SOLVER_EXACT, ADI_SOLVER_FAST, AdiError  # noqa: F401
+from ._abi import (ADI_FP32, ADI_FP64, ADI_SOLVER_EXACT, ADI_SOLVER_FAST, ADI_BATCH_PERSISTENT,  # noqa: F401
+                   ADI_BATCH_MEMBER_GRAPHS, AdiError)
 
 __all__ = ["AdiSolver3D", "AdiError", "fluid_params_normalized", "ADI_FP32", "ADI_FP64",
            "ADI_SOLVER_EXACT", "ADI_SOLVER_FAST", "library_path", "AdiBatch", "AdiSolver2D"]
@@ -290,6 +291,23 @@ class AdiBatch:
         v = C.c_int64()
         self._check(self.lib.adi_batch_launches(self.b, C.byref(v)))
         return v.value
+
+    def set_schedule(self, schedule: int, branches: int = 1):
+        """ADI_BATCH_PERSISTENT (one multi-domain launch per sweep) or
+        ADI_BATCH_MEMBER_GRAPHS (each member's own step on `branches` graph branches)."""
+        self._check(self.lib.adi_batch_set_schedule(self.b, schedule, branches))
+
+    def schedule(self):
+        """(schedule, branches)."""
+        s, br = C.c_int(), C.c_int()
+        self._check(self.lib.adi_batch_get_schedule(self.b, C.byref(s), C.byref(br)))
+        return s.value, br.value
+
+    def time_step(self, dt: float, num_global: int, num_local: int, reps: int = 3) -> float:
+        """Mean ms of one whole batch step with the current schedule (graph replays)."""
+        ms = C.c_float()
+        self._check(self.lib.adi_batch_time_step(self.b, dt, num_global, num_local, reps, C.byref(ms)))
+        return ms.value
 
     def time_sweeps(self, dt: float, reps: int = 3):
         """Mean ms of one batched sweep launch per direction X, Y, Z."""

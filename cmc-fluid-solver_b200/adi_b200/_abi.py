@@ -22,6 +22,7 @@ globals().update({name: code for code, name in STATUS_NAMES.items()})
 ADI_FP32, ADI_FP64 = 4, 8
 ADI_SOLVER_EXACT, ADI_SOLVER_FAST = 0, 1
 ADI_FAULT_NONE, ADI_FAULT_SKIP_TILE_LOADS = 0, 1
+ADI_BATCH_PERSISTENT, ADI_BATCH_MEMBER_GRAPHS = 0, 1
 
 # every entry point include/adi_b200.h declares
 EXPORTED = [
@@ -33,7 +34,8 @@ EXPORTED = [
     "adi_sweep_exact_static", "adi_static_scratch_bytes", "adi_step_tol", "adi_set_graphs",
     "adi_batch_create", "adi_batch_destroy", "adi_batch_set_stream", "adi_batch_step", "adi_batch_div_errors",
     "adi_batch_set_chunk", "adi_batch_get_chunk", "adi_batch_autotune", "adi_batch_set_graphs",
-    "adi_batch_launches", "adi_batch_last_error_string", "adi_batch_time_sweeps", "adi_adjoint_run",
+    "adi_batch_launches", "adi_batch_last_error_string", "adi_batch_time_sweeps", "adi_batch_set_schedule",
+    "adi_batch_get_schedule", "adi_batch_time_step", "adi_adjoint_run",
     "adi_set_node_values", "adi_set_adjoint_chunk", "adi2d_create", "adi2d_destroy", "adi2d_set_stream", "adi2d_set_grid",
     "adi2d_set_segments", "adi2d_step_tol",
     "adi2d_update_boundaries", "adi2d_time_step", "adi2d_step", "adi2d_get_state", "adi2d_set_state",
@@ -130,6 +132,9 @@ def load() -> C.CDLL:
         "adi_batch_set_graphs": [vp, i],
         "adi_batch_launches": [vp, C.POINTER(C.c_int64)],
         "adi_batch_time_sweeps": [vp, d, i, vp],
+        "adi_batch_set_schedule": [vp, i, i],
+        "adi_batch_get_schedule": [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)],
+        "adi_batch_time_step": [vp, d, i, i, i, C.POINTER(C.c_float)],
         "adi_adjoint_run": [vp, d, i, i, i, i, vp, vp, C.POINTER(d), vp, vp],
         "adi_set_node_values": [vp, vp, vp, vp, vp],
         "adi_set_adjoint_chunk": [vp, i],

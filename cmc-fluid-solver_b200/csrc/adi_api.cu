@@ -1712,6 +1712,15 @@ struct adi_batch {
     int2 *d_items[3] = {};
     int nitems[3] = {0, 0, 0};
     int K[3] = {4, 4, 4};
+    // schedule: ADI_BATCH_PERSISTENT (one multi-domain launch per sweep) or
+    // ADI_BATCH_MEMBER_GRAPHS (every member's own step, members spread over
+    // `branches` concurrent graph branches)
+    int schedule = 0;
+    int branches = 1;
+    static constexpr int MAX_BRANCHES = 4;
+    cudaStream_t br[MAX_BRANCHES] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[MAX_BRANCHES] = {};
+    std::vector<std::vector<int>> branch_members;   // members per branch, largest first
     int grid[3] = {0, 0, 0};
     long long max_cells = 0;
     double dt_loaded = NAN;                 // dt the uploaded sweep constants are for
@@ -1722,9 +1731,10 @@ struct adi_batch {
     std::vector<double> diff_error;
     bool graphs_on = true;
     struct GraphEntry {
-        uint64_t key[4];
+        uint64_t key[5];
         cudaGraphExec_t exec;
         int post_ta, post_tb;
+        int64_t launches;
     };
     std::vector<GraphEntry> graphs;
     int64_t launches = 0;
@@ -1852,9 +1862,75 @@ cudaError_t batch_sweep(adi_batch *b, int dir, int K, int src, int tin, int dst,
                                       merges, b->stream);
 }
 
+// Members over branches: longest processing time first by cells, each branch's
+// members largest first.
+void batch_assign_branches(adi_batch *b)
+{
+    const int n = (int)b->hs.size();
+    std::vector<int> order(n);
+    for (int q = 0; q < n; q++) order[q] = q;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return b->hs[x]->n > b->hs[y]->n; });
+    b->branch_members.assign(b->branches, {});
+    std::vector<long long> load(b->branches, 0);
+    for (int q : order) {
+        int w = 0;
+        for (int v = 1; v < b->branches; v++)
+            if (load[v] < load[w]) w = v;
+        b->branch_members[w].push_back(q);
+        load[w] += b->hs[q]->n;
+    }
+}
+
+// The member-graph schedule: every member's own step (its solver, kernels and
+// shapes, as adi_step enqueues it) on one of `branches` streams forked from and
+// joined back into the batch stream, so one member's launch tails and gaps
+// overlap another member's sweeps.  Inside a capture the streams become parallel
+// graph branches.
+template <typename R>
+adi_status batch_enqueue_members(adi_batch *b, int num_global, int num_local, int compute_error, int &ta, int &tb)
+{
+    BCK(cudaEventRecord(b->ev_fork, b->stream));
+    const int ta0 = ta, tb0 = tb;
+    for (int w = 0; w < b->branches; w++) {
+        if (b->branch_members[w].empty()) continue;
+        BCK(cudaStreamWaitEvent(b->br[w], b->ev_fork, 0));
+        for (int q : b->branch_members[w]) {
+            adi_handle *h = b->hs[q];
+            const cudaStream_t own = h->stream;
+            int64_t l0[ADI_K_NUM], b0[ADI_K_NUM];
+            memcpy(l0, h->launches, sizeof l0);
+            memcpy(b0, h->bytes, sizeof b0);
+            const bool prof = h->prof_on;
+            h->prof_on = false;   // per-launch events do not belong in a batch graph
+            h->stream = b->br[w];
+            h->ta = ta0;
+            h->tb = tb0;
+            h->bv_synced = true;
+            const adi_status s = enqueue_step<R>(h, (R)b->dt_loaded, num_global, num_local, compute_error, true);
+            h->stream = own;
+            h->prof_on = prof;
+            int64_t nl = 0;
+            for (int c = 0; c < ADI_K_NUM; c++) nl += h->launches[c] - l0[c];
+            b->launches += nl;
+            memcpy(h->launches, l0, sizeof l0);   // the batch counts these launches, not the member
+            memcpy(h->bytes, b0, sizeof b0);
+            ta = h->ta;
+            tb = h->tb;
+            h->ta = ta0;
+            h->tb = tb0;
+            if (s != ADI_OK) return bfail(b, s, std::string("member step: ") + h->err);
+        }
+        BCK(cudaEventRecord(b->ev_join[w], b->br[w]));
+        BCK(cudaStreamWaitEvent(b->stream, b->ev_join[w], 0));
+    }
+    return ADI_OK;
+}
+
 template <typename R>
 adi_status batch_enqueue(adi_batch *b, int num_global, int num_local, int compute_error, int &ta, int &tb)
 {
+    if (b->schedule == ADI_BATCH_MEMBER_GRAPHS)
+        return batch_enqueue_members<R>(b, num_global, num_local, compute_error, ta, tb);
     const adi_handle *h0 = b->hs[0];
     const int n = (int)b->hs.size();
     const BatchDomain<R> *doms = (const BatchDomain<R> *)b->d_doms;
@@ -1891,12 +1967,13 @@ adi_status batch_step(adi_batch *b, double dt, int num_global, int num_local, in
     adi_handle *h0 = b->hs[0];
     int ta = h0->ta, tb = h0->tb;
     if (b->graphs_on) {
-        uint64_t key[4] = {0, 0, 0, 0};
+        uint64_t key[5] = {0, 0, 0, 0, 0};
         memcpy(&key[0], &dt, sizeof dt);
         key[1] = (uint64_t)num_global | ((uint64_t)num_local << 20) | ((uint64_t)(compute_error != 0) << 40);
         key[2] = (uint64_t)h0->cur | ((uint64_t)h0->nxt << 4) | ((uint64_t)h0->half << 8) | ((uint64_t)ta << 12) |
                  ((uint64_t)tb << 16);
         key[3] = (uint64_t)b->stream;
+        key[4] = (uint64_t)b->schedule | ((uint64_t)b->branches << 8);
         adi_batch::GraphEntry *ge = nullptr;
         for (auto &g : b->graphs)
             if (!memcmp(g.key, key, sizeof key)) ge = &g;
@@ -1912,8 +1989,8 @@ adi_status batch_step(adi_batch *b, double dt, int num_global, int num_local, in
             s = batch_enqueue<R>(b, num_global, num_local, compute_error, ta2, tb2);
             cudaError_t ec = cudaStreamEndCapture(b->stream, &graph);
             b->stream = user;
-            b->launches = l0;
             if (s != ADI_OK) {
+                b->launches = l0;
                 if (graph) cudaGraphDestroy(graph);
                 return s;
             }
@@ -1923,6 +2000,8 @@ adi_status batch_step(adi_batch *b, double dt, int num_global, int num_local, in
             if (ei != cudaSuccess) return bfail(b, ADI_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(ei));
             e.post_ta = ta2;
             e.post_tb = tb2;
+            e.launches = b->launches - l0;
+            b->launches = l0;
             if (b->graphs.size() >= 8) {
                 cudaGraphExecDestroy(b->graphs.front().exec);
                 b->graphs.erase(b->graphs.begin());
@@ -1931,7 +2010,7 @@ adi_status batch_step(adi_batch *b, double dt, int num_global, int num_local, in
             ge = &b->graphs.back();
         }
         BCK(cudaGraphLaunch(ge->exec, b->stream));
-        b->launches += 1 + (int64_t)num_global * num_local * 3 + (compute_error ? 2 : 0);
+        b->launches += ge->launches;
         ta = ge->post_ta;
         tb = ge->post_tb;
     } else {
@@ -1942,7 +2021,20 @@ adi_status batch_step(adi_batch *b, double dt, int num_global, int num_local, in
     bool diverged = false;
     if (compute_error) {
         BCK(cudaStreamSynchronize(b->stream));
-        for (int q = 0; q < n; q++) b->diff_error[q] = b->h_cnt[q] ? b->h_sum[q] / (double)b->h_cnt[q] : 0.0;
+        for (int q = 0; q < n; q++) {
+            if (b->schedule == ADI_BATCH_MEMBER_GRAPHS) {
+                // each member's own divergence sum and wait flag (its enqueue_div_error)
+                adi_handle *h = b->hs[q];
+                b->diff_error[q] = h->h_pin->cnt ? h->h_pin->sum / (double)h->h_pin->cnt : 0.0;
+                if (h->h_pin->err) {
+                    h->h_pin->err = 0;
+                    BCK(cudaMemsetAsync(h->d_err, 0, sizeof(int), b->stream));
+                    return bfail(b, ADI_ERR_TIMEOUT, "a member sweep's bounded wait for its input tiles gave up");
+                }
+            } else {
+                b->diff_error[q] = b->h_cnt[q] ? b->h_sum[q] / (double)b->h_cnt[q] : 0.0;
+            }
+        }
     }
     for (int q = 0; q < n; q++) diverged |= b->diff_error[q] > 0.01;
     for (int q = 0; q < n; q++) {
@@ -1959,10 +2051,60 @@ adi_status batch_step(adi_batch *b, double dt, int num_global, int num_local, in
     return ADI_OK;
 }
 
+// Mean time of one whole step with the current schedule and chunk lengths,
+// replayed from a graph captured for it; the layer roles are left as they were
+// (the step is not finished: cur keeps the state).
+template <typename R>
+adi_status batch_time_step(adi_batch *b, double dt, int num_global, int num_local, int reps, float *ms)
+{
+    adi_status s = batch_load_dt<R>(b, dt);
+    if (s != ADI_OK) return s;
+    const adi_handle *h0 = b->hs[0];
+    int ta = h0->ta, tb = h0->tb;
+    const cudaStream_t user = b->stream;
+    const int64_t l0 = b->launches;
+    b->stream = b->cap_stream;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    s = batch_enqueue<R>(b, num_global, num_local, 0, ta, tb);
+    cudaError_t ec = cudaStreamEndCapture(b->stream, &graph);
+    b->stream = user;
+    b->launches = l0;
+    if (s != ADI_OK || ec != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return s != ADI_OK ? s : bfail(b, ADI_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(ec));
+    }
+    cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) return bfail(b, ADI_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(ei));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e == cudaSuccess) e = cudaGraphLaunch(exec, b->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(e0, b->stream);
+    for (int r = 0; r < reps && e == cudaSuccess; r++) e = cudaGraphLaunch(exec, b->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, b->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float t = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaGraphExecDestroy(exec);
+    BCK(e);
+    *ms = t / reps;
+    return ADI_OK;
+}
+
 void batch_free(adi_batch *b)
 {
     batch_invalidate(b);
     if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+    for (int w = 0; w < adi_batch::MAX_BRANCHES; w++) {
+        if (b->br[w]) cudaStreamDestroy(b->br[w]);
+        if (b->ev_join[w]) cudaEventDestroy(b->ev_join[w]);
+    }
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
     cudaFree(b->d_doms);
     for (int d = 0; d < 3; d++) cudaFree(b->d_items[d]);
     cudaFree(b->d_psum);
@@ -2002,6 +2144,12 @@ adi_status adi_batch_create(adi_handle *const *handles, int n, adi_batch **out)
     b->diff_error.assign(n, 0.0);
     for (int q = 0; q < n; q++) b->diff_error[q] = handles[q]->diff_error;
     cudaError_t e = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking);
+    for (int w = 0; w < adi_batch::MAX_BRANCHES; w++) {
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->br[w], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_join[w], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
+    batch_assign_branches(b);
     if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_psum, sizeof(double) * BATCH_DIV_BLOCKS * n);
     if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_pcnt, sizeof(unsigned long long) * BATCH_DIV_BLOCKS * n);
     if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_sum, sizeof(double) * n);
@@ -2117,7 +2265,57 @@ adi_status adi_batch_autotune(adi_batch *b, double dt, int reps)
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    return b->prec == ADI_FP64 ? batch_build<double>(b) : batch_build<float>(b);
+    adi_status s = b->prec == ADI_FP64 ? batch_build<double>(b) : batch_build<float>(b);
+    if (s != ADI_OK) return s;
+    // the schedule: whole steps of every candidate
+    const int n = (int)b->hs.size();
+    float best = 1e30f;
+    int best_sched = ADI_BATCH_PERSISTENT, best_br = 1;
+    for (int c = 0; c <= adi_batch::MAX_BRANCHES; c++) {
+        const int sched = c == 0 ? ADI_BATCH_PERSISTENT : ADI_BATCH_MEMBER_GRAPHS;
+        const int brs = c == 0 ? 1 : c;
+        if (brs > n) break;
+        b->schedule = sched;
+        b->branches = brs;
+        batch_assign_branches(b);
+        float ms = 0.f;
+        s = b->prec == ADI_FP64 ? batch_time_step<double>(b, dt, 1, 2, reps, &ms)
+                                : batch_time_step<float>(b, dt, 1, 2, reps, &ms);
+        if (s != ADI_OK) return s;
+        if (ms < best) { best = ms; best_sched = sched; best_br = brs; }
+    }
+    b->schedule = best_sched;
+    b->branches = best_br;
+    batch_assign_branches(b);
+    batch_invalidate(b);
+    return ADI_OK;
+}
+
+adi_status adi_batch_set_schedule(adi_batch *b, int schedule, int branches)
+{
+    if (!b || (schedule != ADI_BATCH_PERSISTENT && schedule != ADI_BATCH_MEMBER_GRAPHS) || branches < 1 ||
+        branches > adi_batch::MAX_BRANCHES)
+        return ADI_ERR_BAD_ARG;
+    b->schedule = schedule;
+    b->branches = branches;
+    batch_assign_branches(b);
+    batch_invalidate(b);
+    return ADI_OK;
+}
+
+adi_status adi_batch_get_schedule(adi_batch *b, int *schedule, int *branches)
+{
+    if (!b || !schedule || !branches) return ADI_ERR_BAD_ARG;
+    *schedule = b->schedule;
+    *branches = b->branches;
+    return ADI_OK;
+}
+
+adi_status adi_batch_time_step(adi_batch *b, double dt, int num_global, int num_local, int reps, float *ms_out)
+{
+    if (!b || reps < 1 || !(dt > 0) || num_global < 1 || num_local < 1 || !ms_out) return ADI_ERR_BAD_ARG;
+    return b->prec == ADI_FP64 ? batch_time_step<double>(b, dt, num_global, num_local, reps, ms_out)
+                               : batch_time_step<float>(b, dt, num_global, num_local, reps, ms_out);
 }
 
 adi_status adi_batch_time_sweeps(adi_batch *b, double dt, int reps, float *ms_out)

@@ -484,7 +484,30 @@ adi_status adi_batch_div_errors(adi_batch *b, double *out);
  * choice per direction at dt and keeps the fastest. */
 adi_status adi_batch_set_chunk(adi_batch *b, int dir, int K);
 adi_status adi_batch_get_chunk(adi_batch *b, int dir, int *K);
+
+/* How a batch step is scheduled.  ADI_BATCH_PERSISTENT (the default): the
+ * multi-domain launches above, one per sweep.  ADI_BATCH_MEMBER_GRAPHS: every
+ * member's own step (its solver, its autotuned kernels and shapes: what adi_step
+ * runs), the members spread over `branches` (1..4) concurrent streams, largest
+ * first by cells, forked from and joined back into the batch's stream; captured,
+ * the streams are parallel branches of one graph, so one member's launch tails
+ * and launch gaps overlap another member's sweeps.  Results are those of each
+ * member's adi_step; the divergence guard is the same (no member advances). */
+enum { ADI_BATCH_PERSISTENT = 0, ADI_BATCH_MEMBER_GRAPHS = 1 };
+adi_status adi_batch_set_schedule(adi_batch *b, int schedule, int branches);
+adi_status adi_batch_get_schedule(adi_batch *b, int *schedule, int *branches);
+
+/* Picks the chunk length per direction by timing one batched sweep per choice,
+ * then the schedule by timing whole steps (num_global 1, num_local 2) of the
+ * persistent schedule and of the member-graph schedule with 1 to 4 branches
+ * (replayed graphs, reps each after one untimed).  The timed steps rewrite the
+ * next, half and nonlinear layers only and apply the boundary update to the
+ * current state, as the next step would. */
 adi_status adi_batch_autotune(adi_batch *b, double dt, int reps);
+
+/* Mean time in ms of one whole batch step (num_global, num_local, no divergence
+ * error) with the current schedule: reps replays of its graph after one untimed. */
+adi_status adi_batch_time_step(adi_batch *b, double dt, int num_global, int num_local, int reps, float *ms_out);
 
 /* Mean time in ms of one batched sweep launch per direction X, Y, Z (reps timed
  * launches after one untimed, at dt; the launches write half and the nonlinear

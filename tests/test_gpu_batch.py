@@ -5,6 +5,8 @@ chunk length K and lines-per-CTA max(1, 256 // P), or, for X and Y with K < 0, t
 tile kernel with element-copied tiles of 8 lines, so each member must come out bit
 for bit as the same domain stepped alone with that fast-sweep shape; one member is
 also compared with the FP64 oracle at float tolerance (2e-6 of the field scale).
+The member-graph schedule runs each member's own step on concurrent graph
+branches, so it must equal each member's adi_step bit for bit.
 """
 import numpy as np
 import pytest
@@ -133,3 +135,68 @@ def test_batch_divergence_guard_and_lock_step(adi_lib):
     m64 = _member(adi_lib, ds[0], precision=_abi.ADI_FP64)
     with pytest.raises(_abi.AdiError):
         adi_lib.AdiBatch([members[0], m64])
+
+
+@pytest.mark.parametrize("branches", [1, 2, 3])
+def test_member_graph_schedule_matches_members_stepped_alone(adi_lib, branches):
+    """ADI_BATCH_MEMBER_GRAPHS runs each member's own step (its fast kernels and
+    shapes) on concurrent graph branches: bit for bit the member's adi_step."""
+    from adi_b200 import _abi
+    ds = _domains(11, n=6)
+    members = [_member(adi_lib, d, solver=_abi.ADI_SOLVER_FAST) for d in ds]
+    alone = [_member(adi_lib, d, solver=_abi.ADI_SOLVER_FAST) for d in ds]
+    for m, s in zip(members, alone):
+        for dr, (K, NL, _) in enumerate(m.fast_shapes()):
+            s.set_fast_shape(dr, K, NL)
+    b = adi_lib.AdiBatch(members)
+    b.set_schedule(_abi.ADI_BATCH_MEMBER_GRAPHS, branches)
+    assert b.schedule() == (_abi.ADI_BATCH_MEMBER_GRAPHS, branches)
+    for graphs in (True, False):
+        b.set_graphs(graphs)
+        for i in range(3):
+            ce = i in (0, 2)
+            assert b.step(6e-4, 2, 2, ce) == 0, b.last_error()
+            for s in alone:
+                assert s.step(6e-4, 2, 2, ce) == 0
+        for q, (m, s) in enumerate(zip(members, alone)):
+            for f in range(4):
+                assert np.array_equal(m.fields(0)[f], s.fields(0)[f]), (graphs, q, f)
+        assert np.array_equal(b.div_errors(), np.array([s.div_error() for s in alone]))
+
+
+def test_member_graph_divergence_guard_and_autotune(adi_lib):
+    from adi_b200 import _abi
+    ds = _domains(12, n=4)
+    members = [_member(adi_lib, d, solver=_abi.ADI_SOLVER_FAST) for d in ds]
+    b = adi_lib.AdiBatch(members)
+    b.autotune(6e-4, 2)
+    sched, br = b.schedule()
+    assert sched in (_abi.ADI_BATCH_PERSISTENT, _abi.ADI_BATCH_MEMBER_GRAPHS) and 1 <= br <= 4
+    # timing steps did not advance anything: a step after autotune equals one without
+    ref = [_member(adi_lib, d, solver=_abi.ADI_SOLVER_FAST) for d in ds]
+    b.set_schedule(_abi.ADI_BATCH_MEMBER_GRAPHS, 2)
+    for m, s in zip(members, ref):
+        for dr, (K, NL, _) in enumerate(m.fast_shapes()):
+            s.set_fast_shape(dr, K, NL)
+    assert b.time_step(6e-4, 1, 2, 2) > 0
+    assert b.step(6e-4, 2, 2, True) == 0
+    for s in ref:
+        assert s.step(6e-4, 2, 2, True) == 0
+    for m, s in zip(members, ref):
+        for f in range(4):
+            assert np.array_equal(m.fields(0)[f], s.fields(0)[f])
+    # a wild member trips the guard; nobody advances (the boundary update at the
+    # step start has been applied, as a driver's UpdateBoundaries before a throwing
+    # TimeStep would, so fluid cells are compared)
+    before = [m.fields(0) for m in members]
+    rng = np.random.default_rng(1)
+    wild = [(a + 100.0 * rng.standard_normal(a.shape)).astype(np.float32) for a in members[1].fields(0)]
+    members[1].set_state(*wild)
+    assert b.step(6e-4, 1, 1, True) == _abi.ADI_ERR_DIVERGENCE
+    assert b.div_errors()[1] > 0.01
+    for q in (0, 2, 3):
+        fluid = ds[q].type == G.NODE_IN
+        for f in range(4):
+            assert np.array_equal(members[q].fields(0)[f][fluid], before[q][f][fluid])
+    with pytest.raises(_abi.AdiError):
+        b.set_schedule(_abi.ADI_BATCH_MEMBER_GRAPHS, 5)
