@@ -94,7 +94,7 @@ struct adi_handle {
     std::vector<GraphEntry> graphs;
     bool graphs_on = true;
     cudaStream_t cap_stream = nullptr;
-    int adjoint_K = 4;   // chunk length of the adjoint sweep; 0: one thread per line
+    int adjoint_K = -4;  // adjoint sweep: chunk length (< 0: split solve + accumulation); 0: one thread per line
     // adjoint workspace (checkpoints, tape, adjoint layers), kept between
     // adi_adjoint_run calls and grown when a call needs more; freed by adi_destroy
     char *adj_mem = nullptr;
@@ -348,7 +348,34 @@ cudaError_t launch_sweep_once(adi_handle *h, int dir, int src, int dst, const Sw
 }
 
 template <typename R>
-adi_status enqueue_global_iteration(adi_handle *h, R dt, int num_local, void *const *tape = nullptr)
+Layer<R> layer_of(void *const *f)
+{
+    Layer<R> x;
+    for (int v = 0; v < 4; v++) x.f[v] = (R *)f[v];
+    return x;
+}
+
+template <typename R>
+CLayer<R> clayer_of(void *const *f)
+{
+    CLayer<R> x;
+    for (int v = 0; v < 4; v++) x.f[v] = (const R *)f[v];
+    return x;
+}
+
+// One global iteration (Z, Y, X sweeps, num_local each).  With a tape (the
+// adjoint's record of this iteration: per sweep k, slot k holds the nonlinear
+// layer the sweep reads in fields 0-3 and the layer it writes in fields 4-7), the
+// nonlinear layers live in the tape itself: sweep k reads slot k's layer and
+// writes its merged nonlinear layer straight into slot k + 1's (the next sweep's
+// input), except the step's last sweep (last_iteration), whose output nothing
+// reads.  Slot 0 of a step is the step start's copy of cur; the other slots'
+// off-NODE_IN cells, which no sweep writes, must hold what every nonlinear layer
+// holds there (cur after the boundary update: node values, unchanged OUT cells),
+// which adjoint_run copies in once.  The written layer is copied into the tape.
+template <typename R>
+adi_status enqueue_global_iteration(adi_handle *h, R dt, int num_local, void *const *tape = nullptr,
+                                    bool last_iteration = true)
 {
     const int order[3] = {2, 1, 0};
     const int src[3] = {h->cur, h->nxt, h->half};
@@ -363,21 +390,21 @@ adi_status enqueue_global_iteration(adi_handle *h, R dt, int num_local, void *co
         for (int l = 0; l < num_local; l++) {
             const int merges = (dir == 0 && l == num_local - 1) ? 2 : 1;
             const size_t fb = (size_t)h->n * sizeof(R);
-            if (tape && q == 0 && l == 0)   // the nonlinear layer the first sweep reads
-                CK(launch_copy_fields(4, h->d_L[h->ta], tape, fb, h->stream));
-            CK(timed(h, cls, bytes, [&] { return launch_sweep_once<R>(h, dir, src[q], dst[q], k, merges); }));
-            if (tape) {
-                // the layer it wrote, and (in the same launch) the nonlinear layer it
-                // wrote, which the next sweep of this iteration reads
-                const bool more = q < 2 || l < num_local - 1;
-                void *src8[8], *dst8[8];
-                for (int v = 0; v < 4; v++) {
-                    src8[v] = h->d_L[dst[q]][v];
-                    dst8[v] = tape[4 + v];
-                    src8[4 + v] = h->d_L[h->tb][v];
-                    dst8[4 + v] = tape[8 + v];
-                }
-                CK(launch_copy_fields(more ? 8 : 4, src8, dst8, fb, h->stream));
+            if (!tape) {
+                CK(timed(h, cls, bytes, [&] { return launch_sweep_once<R>(h, dir, src[q], dst[q], k, merges); }));
+            } else {
+                const bool final_sweep = last_iteration && q == 2 && l == num_local - 1;
+                const CLayer<R> tin = clayer_of<R>(tape);
+                const Layer<R> tout = final_sweep ? layer<R>(h, h->tb) : layer_of<R>(tape + 8);
+                CK(timed(h, cls, bytes, [&] {
+                    if (h->solver == ADI_SOLVER_FAST)
+                        return launch_fast<R>(h, dir, clayer<R>(h, src[q]), tin, layer<R>(h, dst[q]), tout, k,
+                                              merges, h->shape[dir]);
+                    return launch_sweep_exact<R>(dir, view<R>(h), h->d_line_lo[dir], h->d_line_hi[dir],
+                                                 clayer<R>(h, src[q]), tin, layer<R>(h, dst[q]), tout,
+                                                 (R *)h->d_scratch, k, merges, h->stream);
+                }));
+                CK(launch_copy_fields(4, h->d_L[dst[q]], tape + 4, fb, h->stream));   // the layer it wrote
                 tape += 8;
             }
             std::swap(h->ta, h->tb);
@@ -737,22 +764,6 @@ struct DevArena {
 };
 
 template <typename R>
-Layer<R> layer_of(void *const *f)
-{
-    Layer<R> x;
-    for (int v = 0; v < 4; v++) x.f[v] = (R *)f[v];
-    return x;
-}
-
-template <typename R>
-CLayer<R> clayer_of(void *const *f)
-{
-    CLayer<R> x;
-    for (int v = 0; v < 4; v++) x.f[v] = (const R *)f[v];
-    return x;
-}
-
-template <typename R>
 adi_status adjoint_run(adi_handle *h, double dt, int ng, int nl, int n_steps, int ck, const int lo[3], const int hi[3],
                        double *J, void *nv_grad, void *state_grad)
 {
@@ -762,14 +773,14 @@ adi_status adjoint_run(adi_handle *h, double dt, int ng, int nl, int n_steps, in
     const int win = ck < n_steps ? ck : n_steps;
     const size_t fbr = (fb + 255) / 256 * 256;
     DevArena mem;
-    cudaError_t e = mem.reserve(h, fbr * ((size_t)nck * 4 + 4 * 6 + 2 + (size_t)win * S * 8) + 256 * (DIV_BLOCKS + 16));
+    cudaError_t e = mem.reserve(h, fbr * ((size_t)nck * 4 + 4 * 7 + 2 + (size_t)win * S * 8) + 256 * (DIV_BLOCKS + 16));
     auto layer4 = [&](void **out) {
         for (int v = 0; v < 4; v++) out[v] = mem.get(fb, e);
     };
-    std::vector<void *> ckpt((size_t)nck * 4), fin(4), cb(4), nb(4), hb(4), tb(4), nvb(4);
+    std::vector<void *> ckpt((size_t)nck * 4), fin(4), cb(4), nb(4), hb(4), tb(4), nvb(4), lamb(4);
     for (int c = 0; c < nck; c++) layer4(&ckpt[(size_t)c * 4]);
     layer4(fin.data()); layer4(cb.data()); layer4(nb.data()); layer4(hb.data()); layer4(tb.data());
-    layer4(nvb.data());
+    layer4(nvb.data()); layer4(lamb.data());
     R *ga = (R *)mem.get(fb, e), *gbp = (R *)mem.get(fb, e);
     double *psum = (double *)mem.get(sizeof(double) * DIV_BLOCKS, e), *dJ = (double *)mem.get(sizeof(double), e);
     std::vector<void *> tape((size_t)win * S * 8);
@@ -792,19 +803,29 @@ adi_status adjoint_run(adi_handle *h, double dt, int ng, int nl, int n_steps, in
     // one step with its tape (the recomputation of a window does the same)
     auto taped_step = [&](int t, int t0) -> adi_status {
         h->bv_synced = true;
+        void *const *tp = &tape[(size_t)(t - t0) * S * 8];
+        // the step start writes its nonlinear layer (cur after the boundary update)
+        // straight into the tape slot the first sweep reads
         CK(timed(h, ADI_K_STEP_BEGIN, (int64_t)h->n * (1 + 8 * (int64_t)sizeof(R)), [&] {
-            return launch_step_begin<R>(view<R>(h), layer<R>(h, h->cur), layer<R>(h, h->nxt), layer<R>(h, h->ta),
+            return launch_step_begin<R>(view<R>(h), layer<R>(h, h->cur), layer<R>(h, h->nxt), layer_of<R>(tp),
                                         layer<R>(h, h->tb), true, h->stream);
         }));
-        void *const *tp = &tape[(size_t)(t - t0) * S * 8];
         for (int it = 0; it < ng; it++) {
-            const adi_status s2 = enqueue_global_iteration<R>(h, dtr, nl, tp + (size_t)it * nl * 3 * 8);
+            const adi_status s2 = enqueue_global_iteration<R>(h, dtr, nl, tp + (size_t)it * nl * 3 * 8, it == ng - 1);
             if (s2 != ADI_OK) return s2;
         }
         std::swap(h->cur, h->nxt);
         h->bv_synced = false;
         return ADI_OK;
     };
+    // The tape's nonlinear-layer slots hold, off NODE_IN, what every nonlinear layer
+    // holds there: cur after the boundary update (node values on BOUND / VALVE,
+    // OUT cells as they are), the same in every step of the run.  One step start
+    // into the handle's temp layers gives it; the sweeps then write only NODE_IN.
+    CK(launch_step_begin<R>(view<R>(h), layer<R>(h, h->cur), layer<R>(h, h->nxt), layer<R>(h, h->ta),
+                            layer<R>(h, h->tb), true, h->stream));
+    for (size_t q = 0; q < (size_t)win * S; q++)
+        if ((st = copy4(&tape[q * 8], h->d_L[h->ta])) != ADI_OK) return st;
     // ---- forward, keeping checkpoints; the last window records its tape directly ----
     const int last_t0 = (nck - 1) * ck;
     for (int t = 0; t < n_steps; t++) {
@@ -853,7 +874,8 @@ adi_status adjoint_run(adi_handle *h, double dt, int ng, int nl, int n_steps, in
                                                            clayer_of<R>(tp + (size_t)q * 8 + 4), layer_of<R>(sb),
                                                            layer_of<R>(db), layer_of<R>(tb.data()),
                                                            layer_of<R>(nvb.data()), ga, gbp, (R *)h->d_scratch, k,
-                                                           merges, h->adjoint_K, h->stream);
+                                                           merges, h->adjoint_K, layer_of<R>(lamb.data()),
+                                                           h->stream);
                         }));
                     }
                 }
@@ -1564,7 +1586,7 @@ adi_status adi_adjoint_run(adi_handle *h, double dt, int num_global, int num_loc
 
 adi_status adi_set_adjoint_chunk(adi_handle *h, int K)
 {
-    if (!h || (K != 0 && K != 4 && K != 8)) return ADI_ERR_BAD_ARG;
+    if (!h || (K != 0 && K != 4 && K != 8 && K != -4 && K != -8)) return ADI_ERR_BAD_ARG;
     h->adjoint_K = K;
     return ADI_OK;
 }

@@ -235,20 +235,25 @@ cudaError_t launch_segment_write(int dir, int nx, int ny, int nz, const uint8_t 
 // the sweep read, xs: the layer it wrote): dbar consumed on the segment nodes,
 // tbar turned from the adjoint of the written temp into that of the read temp,
 // sbar and nvbar accumulated; ga, gb are two full-size work planes.
-// chunk_K > 0 selects the chunked kernel (adjoint_fast.cu) when the line length
-// allows it; 0 the one-thread-per-line kernel.
+// chunk_K > 0 selects the fused chunked kernel (adjoint_fast.cu) when the line
+// length allows it, chunk_K < 0 the split chunked kernels (a solve with chunks of
+// -chunk_K rows that stores lambda into lam, then one thread per cell for the
+// accumulations), 0 the one-thread-per-line kernel.
 template <typename R>
 cudaError_t launch_adjoint_sweep(int dir, const DomainView<R> &d, const int *lo, const int *hi, CLayer<R> ti,
                                  CLayer<R> xs, Layer<R> sbar, Layer<R> dbar, Layer<R> tbar, Layer<R> nvbar, R *ga, R *gb,
-                                 R *scratch, const SweepConst<R> &k, int merges, int chunk_K, cudaStream_t s);
+                                 R *scratch, const SweepConst<R> &k, int merges, int chunk_K, Layer<R> lam,
+                                 cudaStream_t s);
 // The same adjoint sweep with the chunked parallel structure of the fast forward
-// sweep (adjoint_fast.cu); K in {4, 8}; lines up to 256 * K.  The caller zeroes
-// ga, gb and folds them in afterwards (launch_adjoint_sweep does both).
+// sweep (adjoint_fast.cu); K in {4, 8}; lines up to 256 * K.  Fused (split
+// false): the caller zeroes ga, gb and folds them in afterwards
+// (launch_adjoint_sweep does both).  Split: the solve stores lambda into lamo and
+// the accumulation kernel does the rest, off-line terms included (ga, gb unused).
 bool adjoint_chunk_supported(int len, int K, int elem_bytes, int &NL, int &P);
 template <typename R>
 cudaError_t launch_adjoint_chunk(int dir, int K, const DomainView<R> &d, const int *lo, const int *hi, CLayer<R> ti,
                                  CLayer<R> xs, Layer<R> sbar, Layer<R> dbar, Layer<R> tbar, Layer<R> nvbar, R *ga, R *gb,
-                                 const SweepConst<R> &k, int merges, cudaStream_t s);
+                                 const SweepConst<R> &k, int merges, bool split, Layer<R> lamo, cudaStream_t s);
 // Adjoint of the step start and UpdateBoundaries (cbar: in, adjoint of cur after
 // them; out, before them).
 template <typename R>

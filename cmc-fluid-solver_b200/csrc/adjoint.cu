@@ -254,16 +254,31 @@ __global__ void adjoint_step_start_kernel(DomainView<R> d, Layer<R> cbar, Layer<
     for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < d.n;
          id += (long long)gridDim.x * blockDim.x) {
         const bool bv = code_is_bv(d.code[id]);
+        // every load of the cell first: the four layers are distinct arrays, but the
+        // compiler cannot know that and would order each load after the last store
+        R c[4], t[4];
 #pragma unroll
         for (int v = 0; v < 4; v++) {
-            R c = cbar.f[v][id] + tbar.f[v][id];
-            if (bv) {
-                c += nbar.f[v][id];
-                nbar.f[v][id] = R(0);
-                nvbar.f[v][id] += c;
-                c = R(0);
+            c[v] = cbar.f[v][id];
+            t[v] = tbar.f[v][id];
+        }
+        if (bv) {
+            R nb[4], nv[4];
+#pragma unroll
+            for (int v = 0; v < 4; v++) {
+                nb[v] = nbar.f[v][id];
+                nv[v] = nvbar.f[v][id];
             }
-            cbar.f[v][id] = c;
+#pragma unroll
+            for (int v = 0; v < 4; v++) {
+                const R x = c[v] + t[v] + nb[v];
+                nbar.f[v][id] = R(0);
+                nvbar.f[v][id] = nv[v] + x;
+                cbar.f[v][id] = R(0);
+            }
+        } else {
+#pragma unroll
+            for (int v = 0; v < 4; v++) cbar.f[v][id] = c[v] + t[v];
         }
     }
 }
@@ -311,9 +326,16 @@ __global__ void objective_final_kernel(const double *psum, int nblocks, double *
 template <typename R>
 cudaError_t launch_adjoint_sweep(int dir, const DomainView<R> &d, const int *lo, const int *hi, CLayer<R> ti,
                                  CLayer<R> xs, Layer<R> sbar, Layer<R> dbar, Layer<R> tbar, Layer<R> nvbar, R *ga, R *gb,
-                                 R *scratch, const SweepConst<R> &k, int merges, int chunk_K, cudaStream_t s)
+                                 R *scratch, const SweepConst<R> &k, int merges, int chunk_K, Layer<R> lam,
+                                 cudaStream_t s)
 {
     const LineGeom g = line_geom(dir, d.nx, d.ny, d.nz);
+    {
+        int NL = 0, P = 0;
+        if (chunk_K < 0 && adjoint_chunk_supported(g.len, -chunk_K, (int)sizeof(R), NL, P))
+            return launch_adjoint_chunk<R>(dir, -chunk_K, d, lo, hi, ti, xs, sbar, dbar, tbar, nvbar, ga, gb, k,
+                                           merges, true, lam, s);
+    }
     cudaError_t e = cudaMemsetAsync(ga, 0, sizeof(R) * d.n, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(gb, 0, sizeof(R) * d.n, s);
     if (e != cudaSuccess) return e;
@@ -326,7 +348,7 @@ cudaError_t launch_adjoint_sweep(int dir, const DomainView<R> &d, const int *lo,
     if (dir == DD) {                                                                                             \
         if (chunked)                                                                                             \
             e = launch_adjoint_chunk<R>(DD, chunk_K, d, lo, hi, ti, xs, sbar, dbar, tbar, nvbar, ga, gb, k,       \
-                                        merges, s);                                                              \
+                                        merges, false, lam, s);                                                  \
         else {                                                                                                   \
             adjoint_sweep_kernel<R, DD><<<blocks, 128, 0, s>>>(d, g, lo, hi, ti, xs, sbar, dbar, tbar, nvbar, ga, \
                                                                gb, scratch, k, merges);                          \
@@ -366,7 +388,7 @@ cudaError_t launch_objective(const DomainView<R> &d, CLayer<R> x, const int lo[3
 #define INST(R)                                                                                                     \
     template cudaError_t launch_adjoint_sweep<R>(int, const DomainView<R> &, const int *, const int *, CLayer<R>,   \
                                                  CLayer<R>, Layer<R>, Layer<R>, Layer<R>, Layer<R>, R *, R *, R *,  \
-                                                 const SweepConst<R> &, int, int, cudaStream_t);                    \
+                                                 const SweepConst<R> &, int, int, Layer<R>, cudaStream_t);          \
     template cudaError_t launch_adjoint_step_start<R>(const DomainView<R> &, Layer<R>, Layer<R>, Layer<R>, Layer<R>, \
                                                       cudaStream_t);                                                \
     template cudaError_t launch_objective<R>(const DomainView<R> &, CLayer<R>, const int *, const int *, Layer<R>,  \

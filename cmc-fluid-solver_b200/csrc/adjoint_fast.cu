@@ -60,6 +60,14 @@ __device__ __forceinline__ void fwd_entries(int kind, uint8_t code, int m, R r, 
     }
 }
 
+template <typename R>
+CLayer<R> clayer_view(const Layer<R> &x)
+{
+    CLayer<R> c;
+    for (int v = 0; v < 4; v++) c.f[v] = x.f[v];
+    return c;
+}
+
 template <int DIR>
 __device__ __forceinline__ int aslot(int li, int c, int q, int NL, int P)
 {
@@ -69,12 +77,16 @@ __device__ __forceinline__ int aslot(int li, int c, int q, int NL, int P)
 
 } // namespace
 
-template <typename R, int DIR, int K>
-__global__ void __launch_bounds__(256, 2)
+// SPLIT: the solve only.  The kernel stores the line's adjoint solution lambda
+// (lamo, four fields, at every row that is not NONE), consumes dbar and
+// accumulates nvbar on the boundary rows, and leaves the IN rows' accumulations
+// to adjoint_accum_kernel, which runs over the cells with full occupancy.
+template <typename R, int DIR, int K, bool SPLIT>
+__global__ void __launch_bounds__(256, SPLIT ? 4 : 2)
     adjoint_chunk_kernel(DomainView<R> d, LineGeom g, int NL, int P, const int *__restrict__ line_lo,
                          const int *__restrict__ line_hi, CLayer<R> ti, CLayer<R> xs, Layer<R> sbar, Layer<R> dbar,
                          Layer<R> tbar, Layer<R> nvbar, R *__restrict__ ga, R *__restrict__ gb, SweepConst<R> kc,
-                         int merges)
+                         int merges, Layer<R> lamo)
 {
     using namespace sweep;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -166,7 +178,88 @@ __global__ void __launch_bounds__(256, 2)
     Reduced<R> red;
     eliminate_abc<R, K>(A, B, C, xb, ea, ec, red);
 
-    // ---------------- reduced system: one CR step + PCR (as in sweep_fast.cu) ----------------
+    // ---------------- reduced system: one CR step + PCR ----------------
+    R lf[4], ll[4];
+    int nstep = 0;
+    // Split kernel, P a power of two up to 32: each line's chunks as one P-lane
+    // segment of a warp, CR and PCR in shuffles (couplings to rows outside the line
+    // are exactly zero, so a lane whose partner lies outside takes its own row:
+    // finite values times 0).  Z lines already sit that way (lane = chunk); X and Y
+    // lines, one chunk per line across the lanes, go through shared memory once.
+    const bool warp_pcr = SPLIT && P <= 32 && (P & (P - 1)) == 0;
+    if (warp_pcr) {
+        auto shuffled = [&](const Reduced<R> &wr, int wc, R (&xo)[8]) {
+            auto up = [&](R x, int dd) { return __shfl_up_sync(0xffffffffu, x, dd, P); };
+            auto dn = [&](R x, int dd) { return __shfl_down_sync(0xffffffffu, x, dd, P); };
+            R ea_[2], ec_[2], ed[4];
+            {
+                R pv[8] = {up(wr.Al[0], 1), up(wr.Cl[0], 1), up(wr.Al[1], 1), up(wr.Cl[1], 1),
+                           up(wr.Dl[0], 1), up(wr.Dl[1], 1), up(wr.Dl[2], 1), up(wr.Dl[3], 1)};
+                if (wc == 0) {
+#pragma unroll
+                    for (int q = 0; q < 8; q++) pv[q] = R(0);
+                }
+                cr_step<R>(wr, pv, ea_, ec_, ed);
+            }
+            for (int st = 1; st < P; st <<= 1) {
+                const R mv[8] = {up(ea_[0], st), up(ec_[0], st), up(ea_[1], st), up(ec_[1], st),
+                                 up(ed[0], st),  up(ed[1], st),  up(ed[2], st),  up(ed[3], st)};
+                const R pv[8] = {dn(ea_[0], st), dn(ec_[0], st), dn(ea_[1], st), dn(ec_[1], st),
+                                 dn(ed[0], st),  dn(ed[1], st),  dn(ed[2], st),  dn(ed[3], st)};
+                pcr_update<R>(mv, pv, ea_, ec_, ed);
+            }
+#pragma unroll
+            for (int v = 0; v < 4; v++) {
+                R nf = dn(ed[v], 1);
+                if (wc == P - 1) nf = R(0);
+                const int m = v < 3 ? 0 : 1;
+                xo[v] = ed[v];
+                xo[4 + v] = wr.Dl[v] - wr.Al[m] * ed[v] - wr.Cl[m] * nf;   // Cl = 0 on the last chunk
+            }
+        };
+        R xo[8];
+        if (DIR == 2) {
+            shuffled(red, ch, xo);
+        } else {
+            // 16 planes of NL (P + 1) values: a thread's reduced rows at (li, ch), read
+            // back by the warp lane (t / P, t % P) that owns that line's chunk
+            const int NQ = NL * (P + 1);
+            const int slot = li * (P + 1) + ch;
+            const R rv[16] = {red.Af[0], red.Af[1], red.Cf[0], red.Cf[1], red.Al[0], red.Al[1], red.Cl[0], red.Cl[1],
+                              red.Df[0], red.Df[1], red.Df[2], red.Df[3], red.Dl[0], red.Dl[1], red.Dl[2], red.Dl[3]};
+#pragma unroll
+            for (int q = 0; q < 16; q++) buf0[q * NQ + slot] = rv[q];
+            __syncthreads();
+            const int wl = t / P, wc = t - (t / P) * P;
+            const int wslot = wl * (P + 1) + wc;
+            Reduced<R> wr;
+#pragma unroll
+            for (int m = 0; m < 2; m++) {
+                wr.Af[m] = buf0[m * NQ + wslot];
+                wr.Cf[m] = buf0[(2 + m) * NQ + wslot];
+                wr.Al[m] = buf0[(4 + m) * NQ + wslot];
+                wr.Cl[m] = buf0[(6 + m) * NQ + wslot];
+            }
+#pragma unroll
+            for (int v = 0; v < 4; v++) {
+                wr.Df[v] = buf0[(8 + v) * NQ + wslot];
+                wr.Dl[v] = buf0[(12 + v) * NQ + wslot];
+            }
+            R wx[8];
+            shuffled(wr, wc, wx);
+            __syncthreads();   // every plane read is done
+#pragma unroll
+            for (int q = 0; q < 8; q++) buf0[q * NQ + wslot] = wx[q];
+            __syncthreads();
+#pragma unroll
+            for (int q = 0; q < 8; q++) xo[q] = buf0[q * NQ + slot];
+        }
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            lf[v] = xo[v];
+            ll[v] = xo[4 + v];
+        }
+    } else {
     buf0[aslot<DIR>(li, ch, 0, NL, P)] = red.Al[0];
     buf0[aslot<DIR>(li, ch, 1, NL, P)] = red.Cl[0];
     buf0[aslot<DIR>(li, ch, 2, NL, P)] = red.Al[1];
@@ -183,7 +276,6 @@ __global__ void __launch_bounds__(256, 2)
         }
         cr_step<R>(red, pv, ea_, ec_, ed);
     }
-    int nstep = 0;
     for (int s = 1; s < P; s <<= 1, nstep++) {
         R *bw = (nstep & 1) ? buf0 : buf1;
         bw[aslot<DIR>(li, ch, 0, NL, P)] = ea_[0];
@@ -209,7 +301,6 @@ __global__ void __launch_bounds__(256, 2)
 #pragma unroll
     for (int v = 0; v < 4; v++) bx[aslot<DIR>(li, ch, v, NL, P)] = ed[v];
     __syncthreads();
-    R lf[4], ll[4];
     {
         R nf[4] = {R(0), R(0), R(0), R(0)};
         if (ch + 1 < P) {
@@ -223,6 +314,7 @@ __global__ void __launch_bounds__(256, 2)
             ll[v] = red.Dl[v] - red.Al[m] * lf[v] - red.Cl[m] * nf[v];
         }
     }
+    }   // shared-memory PCR
 
     // ---------------- accumulations per owned row ----------------
     R up[4][K], dn[4][K];   // contributions of row i to rows p+1 (up) and p-1 (dn): u, v, w, T
@@ -243,6 +335,10 @@ __global__ void __launch_bounds__(256, 2)
         if (!active || kd[q] == Q_NONE) continue;
 #pragma unroll
         for (int v = 0; v < 4; v++) dbar.f[v][off] = R(0);   // the sweep overwrote the destination here
+        if constexpr (SPLIT) {
+#pragma unroll
+            for (int v = 0; v < 4; v++) lamo.f[v][off] = lam[v];
+        }
         if (kd[q] != Q_IN) {
             const uint8_t c = cc[q + 1];
             const bool shared = kd[q] == Q_SHARED;
@@ -254,6 +350,7 @@ __global__ void __launch_bounds__(256, 2)
             if (!tf) nvbar.f[3][off] += lam[3];
             continue;
         }
+        if constexpr (!SPLIT) {
 #pragma unroll
         for (int v = 0; v < 4; v++) sbar.f[v][off] += kc.three_dt * lam[v];
         R w = R(0);
@@ -285,7 +382,9 @@ __global__ void __launch_bounds__(256, 2)
         up[2][i] = gw * s_h; dn[2][i] = -gw * s_h;
         ga[off] = gl * g1;
         gb[off] = gl * g2;
+        }   // !SPLIT
     }
+    if constexpr (!SPLIT) {
     // chunk-boundary neighbours: the previous chunk's last row sends up, the next
     // chunk's first row sends down
     R *bz = (nstep & 1) ? buf1 : buf0;   // not bx: stage (c) may still be reading it
@@ -320,6 +419,15 @@ __global__ void __launch_bounds__(256, 2)
             tbar.f[v][off] = x;
         }
     }
+    }   // !SPLIT
+}
+
+// Dynamic shared memory of adjoint_chunk_kernel: the two PCR buffers of 8 values
+// per chunk, or the split kernel's 16 planes of NL (P + 1) reduced-row values.
+size_t adjoint_chunk_smem(int NL, int P, int elem_bytes)
+{
+    const size_t pcr = (size_t)2 * NL * P * 8 * elem_bytes, planes = (size_t)16 * NL * (P + 1) * elem_bytes;
+    return pcr > planes ? pcr : planes;
 }
 
 bool adjoint_chunk_supported(int len, int K, int elem_bytes, int &NL, int &P)
@@ -329,24 +437,189 @@ bool adjoint_chunk_supported(int len, int K, int elem_bytes, int &NL, int &P)
     if (P < 1 || P > 256) return false;
     NL = 256 / P;
     if (NL < 1) return false;
-    return (size_t)2 * NL * P * 8 * elem_bytes <= 48 * 1024;
+    return adjoint_chunk_smem(NL, P, elem_bytes) <= 48 * 1024;
+}
+
+// Accumulations of the split adjoint sweep, one thread per cell: with lambda of
+// the rows (adjoint_chunk_kernel<..., SPLIT>) it adds, at a cell p of a line,
+//   NONE rows:  nothing but the off-line dissipation terms below;
+//   other rows: tbar = (IN ? mt : 1) tbar + [v == DIR] wb(p) + up(p-1) + dn(p+1),
+//   IN rows:    sbar += 3/dt lambda(p),
+// where wb, up and dn are the terms of the fused kernel (advection, pressure and
+// along-line dissipation of IN rows p-1, p, p+1, recomputed here from lambda and
+// the tape), and tbar[DIR] += the off-line dissipation terms of the four
+// off-line neighbours n that are IN (ga(n) = t_phi lambda_T(n) g1(n) and gb(n)
+// likewise), which the fused path writes into two planes and gathers in a
+// second kernel.  Every cell has one writer, so no order of blocks matters.
+template <typename R, int DIR>
+__global__ void __launch_bounds__(256)
+    adjoint_accum_kernel(DomainView<R> d, CLayer<R> lam, CLayer<R> ti, CLayer<R> xs, Layer<R> sbar, Layer<R> tbar,
+                         SweepConst<R> kc, int merges)
+{
+    // threadIdx.x: z; threadIdx.y: the along-line coordinate for X lines, y for Y and Z
+    // lines, so a block's along-line neighbours mostly sit in the same block
+    const int kk = blockIdx.x * 32 + threadIdx.x;
+    const int ya = blockIdx.y * 8 + threadIdx.y;
+    const int i = DIR == 0 ? ya : (int)blockIdx.z;
+    const int j = DIR == 0 ? (int)blockIdx.z : ya;
+    if (kk >= d.nz || i >= d.nx || j >= d.ny) return;
+    const long long sx = (long long)d.ny * d.nz, sy = d.nz;
+    const long long c = (long long)i * sx + (long long)j * sy + kk;
+    const int p = DIR == 0 ? i : (DIR == 1 ? j : kk);
+    const int len = DIR == 0 ? d.nx : (DIR == 1 ? d.ny : d.nz);
+    const long long sl = DIR == 0 ? sx : (DIR == 1 ? sy : 1);
+    const long long s1 = DIR == 0 ? sy : sx, s2 = DIR == 2 ? sy : 1;
+    const int c1 = DIR == 0 ? j : i, n1 = DIR == 0 ? d.ny : d.nx;
+    const int c2 = DIR == 2 ? j : kk, n2 = DIR == 2 ? d.ny : d.nz;
+    const R h1 = DIR == 0 ? kc.inv_two_dy : kc.inv_two_dx;
+    const R h2 = DIR == 2 ? kc.inv_two_dy : kc.inv_two_dz;
+    // lambda, the tape and the codes are read-only here (non-coherent loads, free to
+    // move ahead of the stores); sbar and tbar are read, then written, by this thread
+    const R *U = ti.f[0], *V = ti.f[1], *W = ti.f[2], *Fd = ti.f[DIR];
+    const uint8_t *code = d.code;
+
+    // ---- codes: the line window p-2 .. p+2 and the four off-line neighbours ----
+    bool in[5];
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+        const int pp = p - 2 + q;
+        in[q] = pp >= 0 && pp < len && code_is_in(__ldg(code + c + (long long)(q - 2) * sl));
+    }
+    const long long nb[4] = {c - s1, c + s1, c - s2, c + s2};
+    const bool nok[4] = {c1 > 0, c1 + 1 < n1, c2 > 0, c2 + 1 < n2};
+    bool nin[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) nin[q] = nok[q] && code_is_in(__ldg(code + nb[q]));
+    const int k0 = qkind(in[1], in[2], in[3]);
+    const bool in0 = k0 == Q_IN, km = in[1], kp = in[3];   // p-1, p+1 are IN rows exactly when IN cells
+
+    // ---- every load ----
+    R gl_n[4], gd_n[4];   // off-line neighbours: t_phi lambda_T and the in-line difference of g1 / g2
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        gl_n[q] = R(0);
+        gd_n[q] = R(0);
+        if (nin[q]) {
+            const R *G = q >= 2 ? (DIR == 2 ? V : W) : (DIR == 0 ? V : U);
+            gl_n[q] = __ldg(lam.f[3] + nb[q]);
+            gd_n[q] = __ldg(G + nb[q] + sl) - __ldg(G + nb[q] - sl);
+        }
+    }
+    // rows p-1 (m) and p+1 (p): lambda, the in-line differences of U, V, W and the
+    // off-line differences of Fd
+    R lr[2][4], du[2][3], df[2][2];
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+        const bool on = r == 0 ? km : kp;
+        const long long cq = c + (r == 0 ? -sl : sl);
+#pragma unroll
+        for (int v = 0; v < 4; v++) lr[r][v] = on ? __ldg(lam.f[v] + cq) : R(0);
+        du[r][0] = on ? __ldg(U + cq + sl) - __ldg(U + cq - sl) : R(0);
+        du[r][1] = on ? __ldg(V + cq + sl) - __ldg(V + cq - sl) : R(0);
+        du[r][2] = on ? __ldg(W + cq + sl) - __ldg(W + cq - sl) : R(0);
+        df[r][0] = on ? __ldg(Fd + cq + s1) - __ldg(Fd + cq - s1) : R(0);
+        df[r][1] = on ? __ldg(Fd + cq + s2) - __ldg(Fd + cq - s2) : R(0);
+    }
+    R l0[4] = {R(0), R(0), R(0), R(0)}, dx[4] = {R(0), R(0), R(0), R(0)}, sb[4] = {R(0), R(0), R(0), R(0)};
+    if (in0) {
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            l0[v] = __ldg(lam.f[v] + c);
+            dx[v] = __ldg(xs.f[v] + c - sl) - __ldg(xs.f[v] + c + sl);
+            sb[v] = sbar.f[v][c];
+        }
+    }
+    R tb[4] = {R(0), R(0), R(0), R(0)};
+    if (k0 != Q_NONE) {
+#pragma unroll
+        for (int v = 0; v < 4; v++) tb[v] = tbar.f[v][c];
+    } else {
+        tb[DIR] = tbar.f[DIR][c];
+    }
+
+    // ---- off-line dissipation terms (ga / gb of the neighbours) ----
+    R acc = R(0);
+    {
+        R g[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) g[q] = nin[q] ? (kc.t_phi * gl_n[q]) * (gd_n[q] * kc.inv_two_h) : R(0);
+        if (nok[0]) acc += g[0] * h1;
+        if (nok[1]) acc -= g[1] * h1;
+        if (nok[2]) acc += g[2] * h2;
+        if (nok[3]) acc -= g[3] * h2;
+    }
+    if (k0 == Q_NONE) {
+        if (acc != R(0)) tbar.f[DIR][c] = tb[DIR] + acc;
+        return;
+    }
+
+    // ---- the along-line terms rows p-1 and p+1 send here (up from p-1, dn = -up from p+1) ----
+    R up[2][4];
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+        const R pt = kc.v_T * lr[r][DIR] * kc.inv_two_h;
+        const R gl = kc.t_phi * lr[r][3];
+        const R ua = du[r][0] * kc.inv_two_h, va = du[r][1] * kc.inv_two_h, wa = du[r][2] * kc.inv_two_h;
+        const R f1 = df[r][0] * h1, f2 = df[r][1] * h2;
+        R gu, gv, gw;
+        if (DIR == 0) {
+            gu = R(4) * ua; gv = R(2) * va + f1; gw = R(2) * wa + f2;
+        } else if (DIR == 1) {
+            gu = R(2) * ua + f1; gv = R(4) * va; gw = R(2) * wa + f2;
+        } else {
+            gu = R(2) * ua + f1; gv = R(2) * va + f2; gw = R(4) * wa;
+        }
+        const R s_h = gl * kc.inv_two_h;
+        up[r][0] = gu * s_h;
+        up[r][1] = gv * s_h;
+        up[r][2] = gw * s_h;
+        up[r][3] = -pt;
+    }
+    R wb = R(0);
+    if (in0) {
+        R w = R(0);
+#pragma unroll
+        for (int v = 0; v < 4; v++) w += l0[v] * dx[v];
+        wb = w * kc.inv_two_h;
+#pragma unroll
+        for (int v = 0; v < 4; v++) sbar.f[v][c] = sb[v] + kc.three_dt * l0[v];
+    }
+    const R mt = merges == 2 ? R(0.25) : R(0.5);
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+        R x = (in0 ? mt : R(1)) * tb[v];
+        if (v == DIR) x += wb;
+        x += km ? up[0][v] : R(0);
+        x += kp ? -up[1][v] : R(0);
+        if (v == DIR && acc != R(0)) x += acc;
+        tbar.f[v][c] = x;
+    }
 }
 
 template <typename R>
 cudaError_t launch_adjoint_chunk(int dir, int K, const DomainView<R> &d, const int *lo, const int *hi, CLayer<R> ti,
                                  CLayer<R> xs, Layer<R> sbar, Layer<R> dbar, Layer<R> tbar, Layer<R> nvbar, R *ga, R *gb,
-                                 const SweepConst<R> &k, int merges, cudaStream_t s)
+                                 const SweepConst<R> &k, int merges, bool split, Layer<R> lamo, cudaStream_t s)
 {
     const LineGeom g = line_geom(dir, d.nx, d.ny, d.nz);
     int NL = 0, P = 0;
     if (!adjoint_chunk_supported(g.len, K, (int)sizeof(R), NL, P)) return cudaErrorInvalidConfiguration;
     const int threads = NL * P;
     const int blocks = (g.nlines + NL - 1) / NL;
-    const size_t smem = (size_t)2 * NL * P * 8 * sizeof(R);
+    const size_t smem = adjoint_chunk_smem(NL, P, (int)sizeof(R));
 #define AC(DD, KK)                                                                                                 \
     if (dir == DD && K == KK) {                                                                                    \
-        adjoint_chunk_kernel<R, DD, KK><<<blocks, threads, smem, s>>>(d, g, NL, P, lo, hi, ti, xs, sbar, dbar,   \
-                                                                     tbar, nvbar, ga, gb, k, merges);             \
+        if (split)                                                                                                 \
+            adjoint_chunk_kernel<R, DD, KK, true><<<blocks, threads, smem, s>>>(                                  \
+                d, g, NL, P, lo, hi, ti, xs, sbar, dbar, tbar, nvbar, ga, gb, k, merges, lamo);                   \
+        else                                                                                                       \
+            adjoint_chunk_kernel<R, DD, KK, false><<<blocks, threads, smem, s>>>(                                 \
+                d, g, NL, P, lo, hi, ti, xs, sbar, dbar, tbar, nvbar, ga, gb, k, merges, lamo);                   \
+        cudaError_t e = cudaGetLastError();                                                                        \
+        if (e != cudaSuccess || !split) return e;                                                                  \
+        const dim3 ab(32, 8);                                                                                      \
+        const dim3 agrid((d.nz + 31) / 32, ((DD == 0 ? d.nx : d.ny) + 7) / 8, DD == 0 ? d.ny : d.nx);             \
+        adjoint_accum_kernel<R, DD><<<agrid, ab, 0, s>>>(d, clayer_view(lamo), ti, xs, sbar, tbar, k, merges);    \
         return cudaGetLastError();                                                                                 \
     }
     AC(0, 4) AC(0, 8) AC(1, 4) AC(1, 8) AC(2, 4) AC(2, 8)
@@ -354,13 +627,12 @@ cudaError_t launch_adjoint_chunk(int dir, int K, const DomainView<R> &d, const i
     return cudaErrorInvalidConfiguration;
 }
 
-template cudaError_t launch_adjoint_chunk<float>(int, int, const DomainView<float> &, const int *, const int *,
-                                                 CLayer<float>, CLayer<float>, Layer<float>, Layer<float>, Layer<float>,
-                                                 Layer<float>, float *, float *, const SweepConst<float> &, int,
-                                                 cudaStream_t);
-template cudaError_t launch_adjoint_chunk<double>(int, int, const DomainView<double> &, const int *, const int *,
-                                                  CLayer<double>, CLayer<double>, Layer<double>, Layer<double>,
-                                                  Layer<double>, Layer<double>, double *, double *,
-                                                  const SweepConst<double> &, int, cudaStream_t);
+#define INST(R)                                                                                                     \
+    template cudaError_t launch_adjoint_chunk<R>(int, int, const DomainView<R> &, const int *, const int *,         \
+                                                 CLayer<R>, CLayer<R>, Layer<R>, Layer<R>, Layer<R>, Layer<R>, R *, \
+                                                 R *, const SweepConst<R> &, int, bool, Layer<R>, cudaStream_t);
+INST(float)
+INST(double)
+#undef INST
 
 } // namespace adi

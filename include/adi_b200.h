@@ -366,9 +366,12 @@ adi_status adi_device_pointers(adi_handle *h, void *out8[8]);
 adi_status adi_adjoint_run(adi_handle *h, double dt, int num_global, int num_local, int n_steps, int ckpt_every,
                            const int box_lo[3], const int box_hi[3], double *J, void *nv_grad, void *state_grad);
 
-/* Adjoint sweep variant: K = 4 or 8 (default 4) runs the chunked transposed solve
- * (K rows per thread, cyclic reduction across chunks; lines up to 256 * K); K = 0
- * one thread per line (any length). */
+/* Adjoint sweep variant: K = 4 or 8 runs the chunked transposed solve fused with
+ * its accumulations (K rows per thread, cyclic reduction across chunks; lines up
+ * to 256 * K); K = -4 or -8 the same solve split from the accumulations (the
+ * solve stores the adjoint solution, one thread per cell then accumulates it,
+ * off-line terms included); K = 0 one thread per line (any length).  Lines too
+ * long for a chunked variant take the one-thread-per-line kernel. */
 adi_status adi_set_adjoint_chunk(adi_handle *h, int K);
 
 /* Replaces the node values (the boundary data of every node; Grid3D node v, T)

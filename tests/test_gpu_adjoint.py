@@ -112,13 +112,15 @@ def test_inflow_gradient_through_autograd_matches_finite_differences(adi_lib):
     assert np.max(np.abs(g - fd)) <= 1e-4 * scale, (g, fd)
 
 
-@pytest.mark.parametrize("K", [0, 8])
+@pytest.mark.parametrize("K", [0, 8, -4, -8])
 def test_adjoint_sweep_variants_agree(adi_lib, K):
-    """The chunked adjoint sweep (K = 4, the default, and 8) and the one-thread-per-line
+    """The fused chunked adjoint sweep (K = 4, 8), the split one (solve, then one
+    thread per cell for the accumulations: K = -4, -8) and the one-thread-per-line
     sweep (K = 0) solve the same transposed systems: FP64 gradients agree to 1e-12."""
     from adi_b200 import _abi
     d = _domain()
     a = _gpu(adi_lib, d, _abi.ADI_FP64)
+    a.set_adjoint_chunk(4)
     b = _gpu(adi_lib, d, _abi.ADI_FP64)
     b.set_adjoint_chunk(K)
     Ja, gnva, gsta = a.adjoint_run(DT, NG, NL, STEPS, 2, *BOX)
