@@ -478,64 +478,75 @@ __global__ void __launch_bounds__(256)
     const R *U = ti.f[0], *V = ti.f[1], *W = ti.f[2], *Fd = ti.f[DIR];
     const uint8_t *code = d.code;
 
-    // ---- codes: the line window p-2 .. p+2 and the four off-line neighbours ----
+    // Every load is issued at once, without waiting for the codes: offsets that
+    // would leave the line or the box are clamped to the cell itself (the values
+    // loaded there are then discarded), so one memory round trip serves the cell.
+    const long long om1 = p >= 1 ? -sl : 0, om2 = p >= 2 ? -2 * sl : 0;
+    const long long op1 = p + 1 < len ? sl : 0, op2 = p + 2 < len ? 2 * sl : 0;
+    const bool nok[4] = {c1 > 0, c1 + 1 < n1, c2 > 0, c2 + 1 < n2};
+    const long long nb[4] = {c - (nok[0] ? s1 : 0), c + (nok[1] ? s1 : 0), c - (nok[2] ? s2 : 0),
+                             c + (nok[3] ? s2 : 0)};
+    const long long cm = c + om1, cp = c + op1;
+    // off-line offsets of the rows p-1 and p+1 (their cells are IN when used, so
+    // their off-line neighbours exist; clamped here only for the unused loads)
+    const long long f1m = nok[0] ? s1 : 0, f1p = nok[1] ? s1 : 0, f2m = nok[2] ? s2 : 0, f2p = nok[3] ? s2 : 0;
+
+    uint8_t cw[5], cn[4];
+    cw[0] = __ldg(code + c + om2);
+    cw[1] = __ldg(code + cm);
+    cw[2] = __ldg(code + c);
+    cw[3] = __ldg(code + cp);
+    cw[4] = __ldg(code + c + op2);
+#pragma unroll
+    for (int q = 0; q < 4; q++) cn[q] = __ldg(code + nb[q]);
+    R gl_n[4], gd_n[4];   // off-line neighbours: lambda_T and the in-line difference of g1 / g2
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const R *G = q >= 2 ? (DIR == 2 ? V : W) : (DIR == 0 ? V : U);
+        gl_n[q] = __ldg(lam.f[3] + nb[q]);
+        gd_n[q] = __ldg(G + nb[q] + op1) - __ldg(G + nb[q] + om1);
+    }
+    // rows p-1 and p+1: lambda, the in-line differences of U, V, W and the off-line
+    // differences of Fd
+    R lr[2][4], du[2][3], df[2][2];
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+        lr[0][v] = __ldg(lam.f[v] + cm);
+        lr[1][v] = __ldg(lam.f[v] + cp);
+    }
+    {
+        const R u0 = __ldg(U + c), v0 = __ldg(V + c), w0 = __ldg(W + c);
+        du[0][0] = u0 - __ldg(U + c + om2);
+        du[0][1] = v0 - __ldg(V + c + om2);
+        du[0][2] = w0 - __ldg(W + c + om2);
+        du[1][0] = __ldg(U + c + op2) - u0;
+        du[1][1] = __ldg(V + c + op2) - v0;
+        du[1][2] = __ldg(W + c + op2) - w0;
+    }
+    df[0][0] = __ldg(Fd + cm + f1p) - __ldg(Fd + cm - f1m);
+    df[0][1] = __ldg(Fd + cm + f2p) - __ldg(Fd + cm - f2m);
+    df[1][0] = __ldg(Fd + cp + f1p) - __ldg(Fd + cp - f1m);
+    df[1][1] = __ldg(Fd + cp + f2p) - __ldg(Fd + cp - f2m);
+    R l0[4], dx[4], sb[4], tb[4];
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+        l0[v] = __ldg(lam.f[v] + c);
+        dx[v] = __ldg(xs.f[v] + cm) - __ldg(xs.f[v] + cp);
+        sb[v] = sbar.f[v][c];
+        tb[v] = tbar.f[v][c];
+    }
+
     bool in[5];
 #pragma unroll
     for (int q = 0; q < 5; q++) {
         const int pp = p - 2 + q;
-        in[q] = pp >= 0 && pp < len && code_is_in(__ldg(code + c + (long long)(q - 2) * sl));
+        in[q] = pp >= 0 && pp < len && code_is_in(cw[q]);
     }
-    const long long nb[4] = {c - s1, c + s1, c - s2, c + s2};
-    const bool nok[4] = {c1 > 0, c1 + 1 < n1, c2 > 0, c2 + 1 < n2};
     bool nin[4];
 #pragma unroll
-    for (int q = 0; q < 4; q++) nin[q] = nok[q] && code_is_in(__ldg(code + nb[q]));
+    for (int q = 0; q < 4; q++) nin[q] = nok[q] && code_is_in(cn[q]);
     const int k0 = qkind(in[1], in[2], in[3]);
     const bool in0 = k0 == Q_IN, km = in[1], kp = in[3];   // p-1, p+1 are IN rows exactly when IN cells
-
-    // ---- every load ----
-    R gl_n[4], gd_n[4];   // off-line neighbours: t_phi lambda_T and the in-line difference of g1 / g2
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-        gl_n[q] = R(0);
-        gd_n[q] = R(0);
-        if (nin[q]) {
-            const R *G = q >= 2 ? (DIR == 2 ? V : W) : (DIR == 0 ? V : U);
-            gl_n[q] = __ldg(lam.f[3] + nb[q]);
-            gd_n[q] = __ldg(G + nb[q] + sl) - __ldg(G + nb[q] - sl);
-        }
-    }
-    // rows p-1 (m) and p+1 (p): lambda, the in-line differences of U, V, W and the
-    // off-line differences of Fd
-    R lr[2][4], du[2][3], df[2][2];
-#pragma unroll
-    for (int r = 0; r < 2; r++) {
-        const bool on = r == 0 ? km : kp;
-        const long long cq = c + (r == 0 ? -sl : sl);
-#pragma unroll
-        for (int v = 0; v < 4; v++) lr[r][v] = on ? __ldg(lam.f[v] + cq) : R(0);
-        du[r][0] = on ? __ldg(U + cq + sl) - __ldg(U + cq - sl) : R(0);
-        du[r][1] = on ? __ldg(V + cq + sl) - __ldg(V + cq - sl) : R(0);
-        du[r][2] = on ? __ldg(W + cq + sl) - __ldg(W + cq - sl) : R(0);
-        df[r][0] = on ? __ldg(Fd + cq + s1) - __ldg(Fd + cq - s1) : R(0);
-        df[r][1] = on ? __ldg(Fd + cq + s2) - __ldg(Fd + cq - s2) : R(0);
-    }
-    R l0[4] = {R(0), R(0), R(0), R(0)}, dx[4] = {R(0), R(0), R(0), R(0)}, sb[4] = {R(0), R(0), R(0), R(0)};
-    if (in0) {
-#pragma unroll
-        for (int v = 0; v < 4; v++) {
-            l0[v] = __ldg(lam.f[v] + c);
-            dx[v] = __ldg(xs.f[v] + c - sl) - __ldg(xs.f[v] + c + sl);
-            sb[v] = sbar.f[v][c];
-        }
-    }
-    R tb[4] = {R(0), R(0), R(0), R(0)};
-    if (k0 != Q_NONE) {
-#pragma unroll
-        for (int v = 0; v < 4; v++) tb[v] = tbar.f[v][c];
-    } else {
-        tb[DIR] = tbar.f[DIR][c];
-    }
 
     // ---- off-line dissipation terms (ga / gb of the neighbours) ----
     R acc = R(0);
