@@ -122,6 +122,10 @@ CONFIGS = {
     "adjoint64": dict(make=_spheres64_adj, adjoint=True, Re=200.0, Pr=0.72, lam=1.4, dt=5e-4, ng=4, nl=2,
                       n_steps=8, ckpt=4, box=((40, 16, 16), (56, 48, 48)), near_box=((2, 16, 16), (18, 48, 48)),
                       desc="small adjoint for profiling: 64^3 FP32, 10 spheres, 8 steps checkpointed every 4"),
+    "adjoint128s": dict(make=_spheres128, adjoint=True, Re=200.0, Pr=0.72, lam=1.4, dt=5e-4, ng=4, nl=2,
+                        n_steps=2, ckpt=1, box=((80, 48, 48), (112, 80, 80)), near_box=((2, 48, 48), (34, 80, 80)),
+                        desc="short adjoint for profiling: the adjoint128 domain (128^3 FP32, 40 spheres), 2 steps "
+                             "checkpointed every step (a 1.5 GB tape)"),
     "masks262": dict(make=None, masks=True, dx=0.0029,
                      desc="mask builders: Grid3D::Build of a closed triangle mesh (jittered latitude-longitude "
                           "sphere, 1656 triangles, radius 0.36) rasterised and flood-filled on a 262x262x264 "
