@@ -1,10 +1,14 @@
 // Z sweep with warp-resident lines.
 //
-// Z lines are contiguous in memory.  A line of L = P*K nodes is held by P
-// consecutive lanes of one warp (P in {4, 8, 16, 32}, 32/P lines per warp), lane
-// `ch` owning rows [ch*K, ch*K + K).  Every global access is a 16-byte vector
-// access: the own rows of cur and temp, the four off-line neighbour lines of the
-// advecting component (x+-1, y+-1), and the stores when a whole chunk is written.
+// Z lines are contiguous in memory.  A line of L = dimz nodes is held by P
+// consecutive lanes of one warp (P in {4, 8, 16, 32}, the smallest with P*K >= L;
+// 32/P lines per warp), lane `ch` owning rows [ch*K, ch*K + K) of the line; rows
+// at or beyond L are padding (NODE_OUT, no loads or stores).  Where a lane's
+// chunk lies whole inside the line and dimz keeps it 16-byte aligned, every
+// global access is a 16-byte vector access: the own rows of cur and temp, the
+// four off-line neighbour lines of the advecting component (x+-1, y+-1), and the
+// stores when a whole chunk is written; otherwise the lane accesses its rows one
+// by one.
 // The rows just outside a chunk (stencil halo) come from the neighbouring lanes
 // by shuffle, and the reduced system of the line -- one cyclic-reduction step
 // then parallel cyclic reduction over the P chunk-first unknowns -- runs entirely
@@ -14,8 +18,8 @@
 // generic fast sweep (sweep_fast.cu); see the comments there.  The chunk
 // elimination, the cyclic-reduction step and the PCR updates are the shared ones
 // of sweep_common.cuh (packed FP32 in float).  Requirements
-// (checked by the launcher): dimz == P*K, K*sizeof(R) a multiple of 16 bytes,
-// 16-byte aligned field arrays.
+// (checked by the launcher): K in {4, 5, 8}, dimz <= 32*K, 16-byte aligned field
+// arrays.
 #include "adi_internal.cuh"
 #include "sweep_common.cuh"
 
@@ -76,16 +80,21 @@ __device__ __forceinline__ T sh_down(T v, int d, int P) { return __shfl_down_syn
 
 } // namespace
 
-template <typename R, int K, int P>
+// FIT: dimz == P K with 16-byte vector chunks (the launcher checks), so every lane
+// holds a whole aligned chunk and the general row-by-row paths compile away.
+template <typename R, int K, int P, bool FIT>
 __global__ void __launch_bounds__(128)
     sweep_zwarp_kernel(DomainView<R> d, int nlines, const int *__restrict__ line_lo, const int *__restrict__ line_hi,
                        CLayer<R> cur, CLayer<R> tin, Layer<R> next, Layer<R> tout, SweepConst<R> kc, int merges)
 {
     constexpr int LPW = 32 / P;  // lines per warp
+    // a K-row chunk can be moved as 16-byte vectors
+    constexpr bool KVEC = (K * sizeof(R)) % 16 == 0;
+    constexpr bool FITV = FIT && KVEC;
     const int lane = threadIdx.x & 31;
     const int ch = lane % P;
     const int line = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * LPW + lane / P;
-    const int L = P * K;
+    const int L = d.nz;
     bool has = false;
     long long base = 0;
     if (line < nlines) {
@@ -97,6 +106,10 @@ __global__ void __launch_bounds__(128)
     const int p0 = ch * K;
     const long long off0 = base + p0;
     const long long sx = (long long)d.ny * d.nz, sy = d.nz;
+    // rows of this lane inside the line; vector accesses for a whole chunk when
+    // dimz keeps every chunk start 16-byte aligned
+    const int nr = FITV ? K : (p0 >= L ? 0 : (p0 + K <= L ? K : L - p0));
+    const bool vec = FITV || (KVEC && nr == K && (L % (16 / (int)sizeof(R))) == 0);
 
     // ---- loads: own rows, four off-line neighbour chunks, codes ----
     R tv[4][K], cu[4][K], wxp[K], wxm[K], wyp[K], wym[K];
@@ -107,22 +120,41 @@ __global__ void __launch_bounds__(128)
         for (int i = 0; i < K; i++) { tv[v][i] = R(0); cu[v][i] = R(0); }
 #pragma unroll
     for (int i = 0; i < K; i++) { wxp[i] = wxm[i] = wyp[i] = wym[i] = R(0); cc[i] = NODE_OUT; }
-    if (has) {
+    const R *W = tin.f[2];
+    if constexpr (KVEC) {
+        if (has && vec) {
 #pragma unroll
-        for (int v = 0; v < 4; v++) {
-            vload<R, K>(tin.f[v] + off0, tv[v]);
-            vload<R, K>(cur.f[v] + off0, cu[v]);
+            for (int v = 0; v < 4; v++) {
+                vload<R, K>(tin.f[v] + off0, tv[v]);
+                vload<R, K>(cur.f[v] + off0, cu[v]);
+            }
+            vload<R, K>(W + off0 + sx, wxp);
+            vload<R, K>(W + off0 - sx, wxm);
+            vload<R, K>(W + off0 + sy, wyp);
+            vload<R, K>(W + off0 - sy, wym);
         }
-        const R *W = tin.f[2];
-        vload<R, K>(W + off0 + sx, wxp);
-        vload<R, K>(W + off0 - sx, wxm);
-        vload<R, K>(W + off0 + sy, wyp);
-        vload<R, K>(W + off0 - sy, wym);
-        if (K == 4) {
+    }
+    if (has && !vec) {
+#pragma unroll
+        for (int i = 0; i < K; i++)
+            if (i < nr) {
+#pragma unroll
+                for (int v = 0; v < 4; v++) {
+                    tv[v][i] = __ldg(tin.f[v] + off0 + i);
+                    cu[v][i] = __ldg(cur.f[v] + off0 + i);
+                }
+                wxp[i] = __ldg(W + off0 + i + sx);
+                wxm[i] = __ldg(W + off0 + i - sx);
+                wyp[i] = __ldg(W + off0 + i + sy);
+                wym[i] = __ldg(W + off0 + i - sy);
+            }
+    }
+    if (has) {
+        if (K == 4 && (FITV || (nr == K && L % 4 == 0))) {
             const uint32_t c4 = __ldg(reinterpret_cast<const uint32_t *>(d.code + off0));
 #pragma unroll
             for (int i = 0; i < K; i++) cc[i] = (c4 >> (8 * i)) & 0xff;
-        } else {
+        } else if (K == 8 && (FITV || (nr == K && L % 8 == 0))) {
 #pragma unroll
             for (int q = 0; q < K / 8; q++) {
                 const uint2 c8 = __ldg(reinterpret_cast<const uint2 *>(d.code + off0) + q);
@@ -132,6 +164,10 @@ __global__ void __launch_bounds__(128)
                     cc[8 * q + 4 + i] = (c8.y >> (8 * i)) & 0xff;
                 }
             }
+        } else {
+#pragma unroll
+            for (int i = 0; i < K; i++)
+                if (i < nr) cc[i] = __ldg(d.code + off0 + i);
         }
     }
     // halo rows from the neighbouring lanes of the line
@@ -262,10 +298,22 @@ __global__ void __launch_bounds__(128)
             mo[v][i] = mm;
         }
     }
-    if (all_seg) {
+    // (padding rows are NONE: the row at L-1 is never IN, so the row at L is not a
+    // segment end)
+    bool done_next = false, done_tout = false;
+    if constexpr (KVEC) {
+        if (vec && all_seg) {
 #pragma unroll
-        for (int v = 0; v < 4; v++) vstore<R, K>(next.f[v] + off0, xo[v]);
-    } else {
+            for (int v = 0; v < 4; v++) vstore<R, K>(next.f[v] + off0, xo[v]);
+            done_next = true;
+        }
+        if (vec && all_in) {
+#pragma unroll
+            for (int v = 0; v < 4; v++) vstore<R, K>(tout.f[v] + off0, mo[v]);
+            done_tout = true;
+        }
+    }
+    if (!done_next) {
 #pragma unroll
         for (int i = 0; i < K; i++)
             if (kind[i] != Z_NONE) {
@@ -273,10 +321,7 @@ __global__ void __launch_bounds__(128)
                 for (int v = 0; v < 4; v++) next.f[v][off0 + i] = xo[v][i];
             }
     }
-    if (all_in) {
-#pragma unroll
-        for (int v = 0; v < 4; v++) vstore<R, K>(tout.f[v] + off0, mo[v]);
-    } else {
+    if (!done_tout) {
 #pragma unroll
         for (int i = 0; i < K; i++)
             if (kind[i] == Z_IN) {
@@ -286,12 +331,19 @@ __global__ void __launch_bounds__(128)
     }
 }
 
+// Lanes per line: the smallest of 4, 8, 16, 32 whose chunks cover dimz (0: none).
+int zwarp_lanes(int nz, int K)
+{
+    if (K != 4 && K != 5 && K != 8) return 0;
+    for (int P = 4; P <= 32; P *= 2)
+        if (P * K >= nz) return P;
+    return 0;
+}
+
 bool zwarp_supported(int nz, int K, int elem_bytes)
 {
-    if (K * elem_bytes % 16 != 0) return false;
-    if (nz % K != 0) return false;
-    const int P = nz / K;
-    return P == 4 || P == 8 || P == 16 || P == 32;
+    (void)elem_bytes;
+    return nz >= 1 && zwarp_lanes(nz, K) > 0;
 }
 
 template <typename R>
@@ -304,20 +356,21 @@ cudaError_t launch_sweep_zwarp(const DomainView<R> &d, const int *line_lo, const
         if (((uintptr_t)cur.f[v] | (uintptr_t)tin.f[v] | (uintptr_t)next.f[v] | (uintptr_t)tout.f[v]) % 16)
             return cudaErrorInvalidConfiguration;
     const int nlines = d.nx * d.ny;
-    const int P = d.nz / K;
+    const int P = zwarp_lanes(d.nz, K);
     const int lines_per_block = 4 * (32 / P);  // 4 warps per block
     const int blocks = (nlines + lines_per_block - 1) / lines_per_block;
+    const bool fit = d.nz == P * K && (K * sizeof(R)) % 16 == 0;
 #define ZL(KK, PP)                                                                                              \
     if (K == KK && P == PP) {                                                                                   \
-        sweep_zwarp_kernel<R, KK, PP><<<blocks, 128, 0, s>>>(d, nlines, line_lo, line_hi, cur, tin, next, tout, k, \
-                                                            merges);                                           \
+        if (fit)                                                                                                \
+            sweep_zwarp_kernel<R, KK, PP, true><<<blocks, 128, 0, s>>>(d, nlines, line_lo, line_hi, cur, tin, next, \
+                                                                      tout, k, merges);                         \
+        else                                                                                                    \
+            sweep_zwarp_kernel<R, KK, PP, false><<<blocks, 128, 0, s>>>(d, nlines, line_lo, line_hi, cur, tin,     \
+                                                                       next, tout, k, merges);                  \
         return cudaGetLastError();                                                                              \
     }
-    if (sizeof(R) == 4) {
-        ZL(4, 4) ZL(4, 8) ZL(4, 16) ZL(4, 32) ZL(8, 4) ZL(8, 8) ZL(8, 16) ZL(8, 32)
-    } else {
-        ZL(4, 4) ZL(4, 8) ZL(4, 16) ZL(4, 32) ZL(8, 4) ZL(8, 8) ZL(8, 16) ZL(8, 32)
-    }
+    ZL(4, 4) ZL(4, 8) ZL(4, 16) ZL(4, 32) ZL(5, 4) ZL(5, 8) ZL(5, 16) ZL(5, 32) ZL(8, 4) ZL(8, 8) ZL(8, 16) ZL(8, 32)
 #undef ZL
     return cudaErrorInvalidConfiguration;
 }

@@ -212,6 +212,33 @@ def test_xy_tiles_copied_elementwise_any_dims(adi_lib, dims, xK, precision):
     assert max(errs_n) < tol, errs_n
 
 
+@pytest.mark.parametrize("nz,zK", [(50, 4), (52, 4), (50, 5), (77, 8), (160, 5), (36, 8)],
+                         ids=["nz50-K4-scalar", "nz52-K4-vector-ragged", "nz50-K5", "nz77-K8", "nz160-K5-full",
+                              "nz36-K8-vector-ragged"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_zwarp_any_dimz(adi_lib, nz, zK, precision):
+    """The warp-resident Z sweep on lines that are not P K long: the smallest P in
+    {4, 8, 16, 32} with P K >= dimz, rows past the line end as padding, chunks moved
+    as vectors where dimz keeps them aligned and row by row elsewhere."""
+    from adi_b200 import _abi
+    d = G.random_domain(30, 26, nz, seed=86 + nz, shell=True, n_obstacles=7, rmax=4.5)
+    params = (140.0, 0.72, 1.4)
+    prec = _abi.ADI_FP64 if precision == "fp64" else _abi.ADI_FP32
+    s = solver(adi_lib, d, params, precision=prec)
+    s.set_fast_shape(2, zK, 0)
+    assert s.fast_shapes()[2][:2] == (zK, 0)
+    orc = O.OracleSolver(d, precision=8, params=fluid_params_tuple(("normalized", params)))
+    m = non_out(d)
+    for _ in range(3):
+        assert s.step(8e-4, 4, 2, True) == 0
+        assert orc.step(8e-4, 4, 2, True) == 0
+    tol = 1e-11 if precision == "fp64" else 2e-6
+    errs = rel_errors(s.fields(0), orc.fields(0), m)
+    assert max(errs) < tol, errs
+    errs_n = rel_errors(s.fields(1), orc.fields(1), m)
+    assert max(errs_n) < tol, errs_n
+
+
 def _slab_domain(nx, ny, nz, seed):
     """Random shell domain plus a wall slab at k = 1..16, so that the first 16-line
     tile of every X and Y plane holds no segment (the persistent kernel skips it)."""
