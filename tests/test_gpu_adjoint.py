@@ -57,8 +57,10 @@ def test_fp32_adjoint_and_checkpoint_windows(adi_lib):
     o = O.OracleSolver(d, precision=8, params=fluid_params_tuple(("normalized", RE)))
     Jo, gnvo, gsto = o.adjoint_run(DT, NG, NL, STEPS, *BOX)
     res = []
+    s = _gpu(adi_lib, d, _abi.ADI_FP32)   # one handle: the same autotuned kernels for every run
+    init = [a.copy() for a in s.fields(0)]
     for ck in (1, 3, STEPS):
-        s = _gpu(adi_lib, d, _abi.ADI_FP32)
+        s.set_state(*init)
         res.append(s.adjoint_run(DT, NG, NL, STEPS, ck, *BOX))
     for J, gnv, gst in res[1:]:
         assert J == res[0][0]
@@ -122,6 +124,8 @@ def test_adjoint_sweep_variants_agree(adi_lib, K):
     a = _gpu(adi_lib, d, _abi.ADI_FP64)
     a.set_adjoint_chunk(4)
     b = _gpu(adi_lib, d, _abi.ADI_FP64)
+    for dr, (k, nl, _) in enumerate(a.fast_shapes()):
+        b.set_fast_shape(dr, k, nl)          # the same forward kernels in both
     b.set_adjoint_chunk(K)
     Ja, gnva, gsta = a.adjoint_run(DT, NG, NL, STEPS, 2, *BOX)
     Jb, gnvb, gstb = b.adjoint_run(DT, NG, NL, STEPS, 2, *BOX)
