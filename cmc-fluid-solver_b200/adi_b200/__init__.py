@@ -198,6 +198,20 @@ class AdiSolver3D:
         arrs = [np.ascontiguousarray(a, self.dtype) for a in (u, v, w, T)]
         self._check(self.lib.adi_set_state(self.h, *[_ptr(a) for a in arrs]))
 
+    def step_io(self, inputs, outputs, dt, num_global, num_local, compute_error=False) -> int:
+        """adi_step_io: upload `inputs` (u, v, w, T host arrays of the handle's dtype),
+        step, download into `outputs`; asynchronous until io_wait().  Returns the status."""
+        for a in list(inputs) + list(outputs):
+            if not (isinstance(a, np.ndarray) and a.dtype == self.dtype and a.flags.c_contiguous
+                    and a.shape == tuple(self.shape)):
+                raise ValueError("step_io takes C-contiguous arrays of the handle's shape and dtype")
+        ins = (C.c_void_p * 4)(*[a.ctypes.data for a in inputs])
+        outs = (C.c_void_p * 4)(*[a.ctypes.data for a in outputs])
+        return self.lib.adi_step_io(self.h, ins, outs, dt, num_global, num_local, int(compute_error))
+
+    def io_wait(self):
+        self._check(self.lib.adi_io_wait(self.h))
+
     def div_error(self) -> float:
         out = C.c_double()
         self._check(self.lib.adi_div_error(self.h, C.byref(out)))

@@ -94,6 +94,14 @@ struct adi_handle {
     std::vector<GraphEntry> graphs;
     bool graphs_on = true;
     cudaStream_t cap_stream = nullptr;
+    // pipelined host I/O (adi_step_io): upload and download streams, one event per
+    // downloaded piece, the result's device copy that the download reads
+    static constexpr int IO_PIECES = 4;   // pieces per field
+    cudaStream_t io_up = nullptr, io_down = nullptr;
+    cudaEvent_t ev_io_up = nullptr, ev_io_ready = nullptr, ev_io_down = nullptr;
+    cudaEvent_t ev_io_piece[4 * IO_PIECES] = {};
+    void *d_io[4] = {};
+    bool io_used = false;
     int adjoint_K = -4;  // adjoint sweep: chunk length (< 0: split solve + accumulation); 0: one thread per line
     // adjoint workspace (checkpoints, tape, adjoint layers), kept between
     // adi_adjoint_run calls and grown when a call needs more; freed by adi_destroy
@@ -258,6 +266,14 @@ void free_all(adi_handle *h)
     h->graphs.clear();
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
     h->cap_stream = nullptr;
+    if (h->io_up) cudaStreamDestroy(h->io_up);
+    if (h->io_down) cudaStreamDestroy(h->io_down);
+    for (cudaEvent_t e : {h->ev_io_up, h->ev_io_ready, h->ev_io_down})
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : h->ev_io_piece)
+        if (e) cudaEventDestroy(e);
+    for (int v = 0; v < 4; v++) cudaFree(h->d_io[v]);
+    h->io_up = h->io_down = nullptr;
     cudaFreeHost(h->h_pin);
     cudaFree(h->d_res);
     cudaFree(h->d_scratch);
@@ -1642,6 +1658,84 @@ adi_status adi_set_state(adi_handle *h, const void *u, const void *v, const void
     CK(cudaStreamSynchronize(h->stream));
     h->bv_synced = false;
     return ADI_OK;
+}
+
+adi_status adi_step_io(adi_handle *h, const void *const *in4, void *const *out4, double dt, int num_global,
+                       int num_local, int compute_error)
+{
+    if (!h || !in4 || !out4) return ADI_ERR_BAD_ARG;
+    for (int f = 0; f < 4; f++)
+        if (!in4[f] || !out4[f]) return ADI_ERR_BAD_ARG;
+    adi_status st = check_ready(h);
+    if (st != ADI_OK) return st;
+    const size_t fb = (size_t)h->n * esize(h);
+    constexpr int NP = adi_handle::IO_PIECES;
+    if (!h->io_up) {
+        cudaError_t e = cudaStreamCreateWithFlags(&h->io_up, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->io_down, cudaStreamNonBlocking);
+        for (cudaEvent_t *ev : {&h->ev_io_up, &h->ev_io_ready, &h->ev_io_down})
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+        for (cudaEvent_t &ev : h->ev_io_piece)
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        for (int v = 0; v < 4 && e == cudaSuccess; v++) e = cudaMalloc(&h->d_io[v], fb);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(h, ADI_ERR_CUDA, std::string("step_io buffers: ") + cudaGetErrorString(e));
+        }
+    }
+    // pieces of a field: byte ranges [q*pb, min((q+1)*pb, fb))
+    const size_t pb = ((fb + NP - 1) / NP + 255) / 256 * 256;
+    auto range = [&](int q, size_t &o, size_t &len) {
+        o = std::min(fb, (size_t)q * pb);
+        len = std::min(fb, o + pb) - o;
+    };
+    // upload into cur: after everything queued on the handle's stream (the previous
+    // step and its copy-out read cur), and each piece after the previous call's
+    // download of the same piece (the host buffer may be that call's output)
+    CK(cudaEventRecord(h->ev_io_ready, h->stream));   // everything queued on the handle so far
+    CK(cudaStreamWaitEvent(h->io_up, h->ev_io_ready, 0));
+    for (int f = 0; f < 4; f++)
+        for (int q = 0; q < NP; q++) {
+            size_t o, len;
+            range(q, o, len);
+            if (!len) continue;
+            if (h->io_used) CK(cudaStreamWaitEvent(h->io_up, h->ev_io_piece[f * NP + q], 0));
+            CK(cudaMemcpyAsync((char *)h->d_L[h->cur][f] + o, (const char *)in4[f] + o, len, cudaMemcpyHostToDevice,
+                               h->io_up));
+        }
+    CK(cudaEventRecord(h->ev_io_up, h->io_up));
+    CK(cudaStreamWaitEvent(h->stream, h->ev_io_up, 0));
+    h->bv_synced = false;
+    st = step_impl(h, dt, num_global, num_local, compute_error, true);
+    if (st != ADI_OK) return st;
+    // copy the result out of the layers (after the previous download has read the
+    // copy), then download it piece by piece
+    if (h->io_used) CK(cudaStreamWaitEvent(h->stream, h->ev_io_down, 0));
+    CK(launch_copy_fields(4, h->d_L[h->cur], h->d_io, fb, h->stream));
+    CK(cudaEventRecord(h->ev_io_ready, h->stream));
+    CK(cudaStreamWaitEvent(h->io_down, h->ev_io_ready, 0));
+    for (int f = 0; f < 4; f++)
+        for (int q = 0; q < NP; q++) {
+            size_t o, len;
+            range(q, o, len);
+            if (len) CK(cudaMemcpyAsync((char *)out4[f] + o, (const char *)h->d_io[f] + o, len,
+                                        cudaMemcpyDeviceToHost, h->io_down));
+            CK(cudaEventRecord(h->ev_io_piece[f * NP + q], h->io_down));
+        }
+    CK(cudaEventRecord(h->ev_io_down, h->io_down));
+    h->io_used = true;
+    return ADI_OK;
+}
+
+adi_status adi_io_wait(adi_handle *h)
+{
+    if (!h) return ADI_ERR_BAD_ARG;
+    if (!h->io_used) return ADI_OK;
+    // the handle's stream too, so work queued after this call (or an event a caller
+    // records on it) follows the last download
+    CK(cudaStreamWaitEvent(h->stream, h->ev_io_down, 0));
+    CK(cudaEventSynchronize(h->ev_io_down));
+    return check_device_flag(h);
 }
 
 adi_status adi_get_layer(adi_handle *h, int outdimx, int outdimy, int outdimz, void *vout, double *Tout)

@@ -272,6 +272,23 @@ adi_status adi_role_pointers(adi_handle *h, int role, void **out4);
 adi_status adi_get_state(adi_handle *h, int layer, void *u, void *v, void *w, void *T);
 adi_status adi_set_state(adi_handle *h, const void *u, const void *v, const void *w, const void *T);
 
+/* adi_set_state + adi_step + adi_get_state(h, 0, ...) as one pipelined call: the
+ * state is uploaded from in4[0..3] (u, v, w, T host arrays) on an upload stream,
+ * the step runs on the handle's stream, the result is copied aside on the device
+ * and downloaded into out4[0..3] on a download stream, each field in four pieces.
+ * Returns once the work is queued (after the divergence check when
+ * compute_error, which waits for the step); call adi_io_wait before reading out4.
+ * Each upload piece waits for the same piece of the previous call's download, so
+ * a call may take the previous call's out4 as its in4 (a host-side time march):
+ * the download of one piece then overlaps the upload of the one before it.  Host
+ * arrays should be page-locked (cudaHostAlloc / cudaHostRegister) for the copies
+ * to run asynchronously; results equal the three separate calls bit for bit. */
+adi_status adi_step_io(adi_handle *h, const void *const *in4, void *const *out4, double dt, int num_global,
+                       int num_local, int compute_error);
+/* Waits for the last adi_step_io download; work queued on the handle's stream
+ * afterwards follows it. */
+adi_status adi_io_wait(adi_handle *h);
+
 /* Solver3D::GetLayer (Solver3D.cpp:21-25 + TimeLayer3D::FilterToArrays,
  * TimeLayer3D.h:819-924): OUT cells of the layer the reference reads (`next`,
  * which after a step holds the state the step started from) are set to 99999

@@ -332,3 +332,41 @@ def test_time_step_with_boundary_state_off_node_values(adi_lib, precision):
         assert orc.time_step(7e-4, 3, 2, True) == 0
     errs = rel_errors(s.fields(0), orc.fields(0), m)
     assert max(errs) < (1e-11 if precision == "fp64" else 2e-6), errs
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_step_io_pipelined_time_march_equals_separate_calls(adi_lib, precision):
+    """adi_step_io chained through host buffers (each call uploads the previous
+    call's download) equals adi_set_state + adi_step + adi_get_state bit for bit,
+    with and without the divergence error, and adi_io_wait orders later work."""
+    import torch
+    from adi_b200 import _abi
+    d = G.random_domain(40, 36, 44, seed=91, shell=True, n_obstacles=6, rmax=4.5)
+    params = (150.0, 0.72, 1.4)
+    prec = _abi.ADI_FP64 if precision == "fp64" else _abi.ADI_FP32
+    a = solver(adi_lib, d, params, precision=prec)
+    b = solver(adi_lib, d, params, precision=prec)
+    for dr, (K, NL, _) in enumerate(a.fast_shapes()):
+        b.set_fast_shape(dr, K, NL)
+    dt_ = np.float32 if precision == "fp32" else np.float64
+    pin = [torch.empty(d.shape, dtype=torch.float32 if precision == "fp32" else torch.float64,
+                       pin_memory=True).numpy() for _ in range(8)]
+    for x, y in zip(pin[:4], a.fields(0)):
+        x[...] = y
+    start = [x.copy() for x in pin[:4]]
+    bufs_in, bufs_out = pin[:4], pin[4:]
+    for i in range(4):
+        assert a.step_io(bufs_in, bufs_out, 7e-4, 3, 2, i in (0, 3)) == 0
+        bufs_in, bufs_out = bufs_out, bufs_in
+    a.io_wait()
+    state = start
+    for i in range(4):
+        b.set_state(*state)
+        assert b.step(7e-4, 3, 2, i in (0, 3)) == 0
+        state = [x.copy() for x in b.fields(0)]
+    for f in range(4):
+        assert bufs_in[f].dtype == dt_
+        assert np.array_equal(bufs_in[f], state[f]), f
+    assert a.div_error() == b.div_error()
+    for f in range(4):
+        assert np.array_equal(a.fields(0)[f], b.fields(0)[f])
