@@ -18,7 +18,8 @@ the oracle on the full-size domain:
   steps.
 
 The large single domain (ellipsoids384, one step) and a member of the batched
-workload (batched64) are compared the same way with the shapes their autotuners pick.
+workload (batched64) are compared the same way with the shapes their autotuners pick,
+and the FP64 adjoint of two spheres128 steps against the FP64 adjoint restatement.
 """
 import numpy as np
 import pytest
@@ -178,3 +179,24 @@ def test_batched64_member_against_oracle(adi_lib):
     errs = _rel(members[q].fields(0), o.fields(0), non_out(ds[q]))
     assert max(errs) <= 1e-5, errs
     assert abs(b.div_errors()[q] - o.div_error()) < 1e-6
+
+
+def test_fp64_adjoint_spheres128_against_oracle_adjoint(adi_lib, spheres128):
+    """The adjoint at the adjoint workload's size: two steps of spheres128 (Re 200,
+    dt 5e-4, num_global 4, num_local 2, windows of one step), J over the 32^3 box
+    next to the inflow, FP64 GPU adjoint with the default (split) sweep against the
+    FP64 CPU adjoint restatement.  (The fused and split sweeps agree to 1e-12 on
+    small domains, test_gpu_adjoint.py.)"""
+    from adi_b200 import _abi
+    d = spheres128
+    lo, hi = (2, 48, 48), (34, 80, 80)
+    s = _solver(adi_lib, d, _abi.ADI_FP64, _abi.ADI_SOLVER_FAST)
+    J, gnv, gst = s.adjoint_run(DT, 4, 2, 2, 1, lo, hi)
+    o = O.OracleSolver(d, precision=8, params=fluid_params_tuple(PARAMS))
+    Jo, gnvo, gsto = o.adjoint_run(DT, 4, 2, 2, lo, hi)
+    o.close()
+    assert abs(J - Jo) <= 1e-12 * abs(Jo)
+    for a, b in ((gnv, gnvo), (gst, gsto)):
+        scale = np.max(np.abs(b))
+        assert scale > 0
+        assert np.max(np.abs(a - b)) <= 1e-9 * scale
