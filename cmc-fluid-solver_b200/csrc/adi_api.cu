@@ -266,6 +266,7 @@ void free_all(adi_handle *h)
     h->graphs.clear();
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
     h->cap_stream = nullptr;
+    if (h->io_used) cudaEventSynchronize(h->ev_io_down);   // a download may still be writing host memory
     if (h->io_up) cudaStreamDestroy(h->io_up);
     if (h->io_down) cudaStreamDestroy(h->io_down);
     for (cudaEvent_t e : {h->ev_io_up, h->ev_io_ready, h->ev_io_down})
@@ -352,14 +353,18 @@ cudaError_t launch_fast(adi_handle *h, int dir, CLayer<R> cur, CLayer<R> tin, La
 // X).  The two nonlinear buffers swap roles after every sweep.
 // One sweep of direction dir from layer src into layer dst, reading the nonlinear
 // layer ta and writing tb (the caller swaps them).
+// tin: the layer read as the nonlinear layer (h->ta, or cur for the first sweep of
+// a step whose start wrote the boundary values only).
 template <typename R>
-cudaError_t launch_sweep_once(adi_handle *h, int dir, int src, int dst, const SweepConst<R> &k, int merges)
+cudaError_t launch_sweep_once(adi_handle *h, int dir, int src, int dst, const SweepConst<R> &k, int merges,
+                              int tin = -1)
 {
+    if (tin < 0) tin = h->ta;
     if (h->solver == ADI_SOLVER_FAST)
-        return launch_fast<R>(h, dir, clayer<R>(h, src), clayer<R>(h, h->ta), layer<R>(h, dst), layer<R>(h, h->tb), k,
+        return launch_fast<R>(h, dir, clayer<R>(h, src), clayer<R>(h, tin), layer<R>(h, dst), layer<R>(h, h->tb), k,
                               merges, h->shape[dir]);
     return launch_sweep_exact<R>(dir, view<R>(h), h->d_line_lo[dir], h->d_line_hi[dir], clayer<R>(h, src),
-                                 clayer<R>(h, h->ta), layer<R>(h, dst), layer<R>(h, h->tb), (R *)h->d_scratch, k,
+                                 clayer<R>(h, tin), layer<R>(h, dst), layer<R>(h, h->tb), (R *)h->d_scratch, k,
                                  merges, h->stream);
 }
 
@@ -391,7 +396,7 @@ CLayer<R> clayer_of(void *const *f)
 // which adjoint_run copies in once.  The written layer is copied into the tape.
 template <typename R>
 adi_status enqueue_global_iteration(adi_handle *h, R dt, int num_local, void *const *tape = nullptr,
-                                    bool last_iteration = true)
+                                    bool last_iteration = true, bool first_reads_cur = false)
 {
     const int order[3] = {2, 1, 0};
     const int src[3] = {h->cur, h->nxt, h->half};
@@ -407,7 +412,8 @@ adi_status enqueue_global_iteration(adi_handle *h, R dt, int num_local, void *co
             const int merges = (dir == 0 && l == num_local - 1) ? 2 : 1;
             const size_t fb = (size_t)h->n * sizeof(R);
             if (!tape) {
-                CK(timed(h, cls, bytes, [&] { return launch_sweep_once<R>(h, dir, src[q], dst[q], k, merges); }));
+                const int tin = first_reads_cur && q == 0 && l == 0 ? h->cur : h->ta;
+                CK(timed(h, cls, bytes, [&] { return launch_sweep_once<R>(h, dir, src[q], dst[q], k, merges, tin); }));
             } else {
                 const bool final_sweep = last_iteration && q == 2 && l == num_local - 1;
                 const CLayer<R> tin = clayer_of<R>(tape);
@@ -562,12 +568,22 @@ adi_status div_error_of(adi_handle *h, int l, double *out)
 template <typename R>
 adi_status enqueue_step(adi_handle *h, R dt, int num_global, int num_local, int compute_error, bool update_bnd)
 {
-    CK(timed(h, ADI_K_STEP_BEGIN, (int64_t)h->n * (1 + 8 * (int64_t)sizeof(R)), [&] {
-        return launch_step_begin<R>(view<R>(h), layer<R>(h, h->cur), layer<R>(h, h->nxt), layer<R>(h, h->ta),
-                                    layer<R>(h, h->tb), update_bnd, h->stream);
-    }));
+    if (update_bnd) {
+        // cur gets the node values first, so the nonlinear layer the first sweep
+        // reads (temp = cur) is cur itself: only BOUND / VALVE cells are written
+        // (layer_ops.cu, step_begin_at, says why that keeps every value a sweep reads)
+        CK(timed(h, ADI_K_STEP_BEGIN, (int64_t)h->n + 20 * (int64_t)sizeof(R) * (h->n - h->num_in), [&] {
+            return launch_step_begin<R>(view<R>(h), layer<R>(h, h->cur), layer<R>(h, h->nxt), layer<R>(h, h->ta),
+                                        layer<R>(h, h->tb), true, h->stream, true);
+        }));
+    } else {
+        CK(timed(h, ADI_K_STEP_BEGIN, (int64_t)h->n * (1 + 8 * (int64_t)sizeof(R)), [&] {
+            return launch_step_begin<R>(view<R>(h), layer<R>(h, h->cur), layer<R>(h, h->nxt), layer<R>(h, h->ta),
+                                        layer<R>(h, h->tb), false, h->stream);
+        }));
+    }
     for (int it = 0; it < num_global; it++) {
-        adi_status s = enqueue_global_iteration<R>(h, dt, num_local);
+        adi_status s = enqueue_global_iteration<R>(h, dt, num_local, nullptr, true, update_bnd && it == 0);
         if (s != ADI_OK) return s;
     }
     if (compute_error) return enqueue_div_error<R>(h, h->nxt);

@@ -150,9 +150,12 @@ struct BatchDomain {
 };
 
 // ---- launchers (each returns cudaGetLastError()) ----
+// bv_only: a step whose first sweep reads cur as its nonlinear layer; only groups
+// of four cells with a BOUND / VALVE cell are written (layer_ops.cu says why that
+// keeps every value a sweep reads).
 template <typename R>
 cudaError_t launch_step_begin(const DomainView<R> &d, Layer<R> cur, Layer<R> next, Layer<R> ta, Layer<R> tb,
-                              bool update_boundaries, cudaStream_t s);
+                              bool update_boundaries, cudaStream_t s, bool bv_only = false);
 template <typename R>
 cudaError_t launch_update_boundaries(const DomainView<R> &d, Layer<R> cur, cudaStream_t s);
 template <typename R>

@@ -34,12 +34,20 @@ __global__ void update_boundaries_kernel(DomainView<R> d, Layer<R> cur)
 // copy, because the sweeps only ever write IN nodes of the buffer they fill.
 // With update_boundaries, cur[BOUND|VALVE] is first refreshed from the node values
 // (the driver calls UpdateBoundaries right before TimeStep, FluidSolver3D.cpp:241-242).
+//
+// bv_only (a step whose first sweep reads cur itself as its nonlinear layer, so
+// the copy temp = cur is needed only where no sweep writes temp): cells that are
+// not BOUND / VALVE are left alone.  The nonlinear buffers then differ from cur
+// only where no sweep reads them: NODE_IN cells, which the first sweep reads from
+// cur and every sweep writes before the next one reads them, and NODE_OUT cells,
+// which no stencil of a NODE_IN row reaches.
 template <typename R>
 __device__ __forceinline__ void step_begin_at(const DomainView<R> &d, const Layer<R> &cur, const Layer<R> &next,
                                               const Layer<R> &ta, const Layer<R> &tb, bool update_boundaries,
-                                              long long i)
+                                              long long i, bool bv_only = false)
 {
     bool bv = code_is_bv(d.code[i]);
+    if (bv_only && !bv) return;
 #pragma unroll
     for (int v = 0; v < 4; v++) {
         R x;
@@ -57,17 +65,20 @@ __device__ __forceinline__ void step_begin_at(const DomainView<R> &d, const Laye
 
 template <typename R>
 __global__ void step_begin_kernel(DomainView<R> d, Layer<R> cur, Layer<R> next, Layer<R> ta, Layer<R> tb,
-                                  bool update_boundaries)
+                                  bool update_boundaries, bool bv_only)
 {
-    for (long long i = gtid(); i < d.n; i += gstride()) step_begin_at(d, cur, next, ta, tb, update_boundaries, i);
+    for (long long i = gtid(); i < d.n; i += gstride())
+        step_begin_at(d, cur, next, ta, tb, update_boundaries, i, bv_only);
 }
 
 // step_begin_at for four consecutive cells with 16-byte accesses (n a multiple
 // of 4, every array 16-byte aligned; checked by the launcher).  Same values as
 // four step_begin_at calls; cur and next are written only where those write.
+// bv_only skips groups of four without a BOUND / VALVE cell and copies the groups
+// with one whole (the extra temp cells are ones no sweep reads before writing).
 template <typename R>
 __global__ void step_begin_vec4_kernel(DomainView<R> d, Layer<R> cur, Layer<R> next, Layer<R> ta, Layer<R> tb,
-                                       bool update_boundaries)
+                                       bool update_boundaries, bool bv_only)
 {
     const long long n4 = d.n / 4;
     for (long long q = gtid(); q < n4; q += gstride()) {
@@ -80,6 +91,7 @@ __global__ void step_begin_vec4_kernel(DomainView<R> d, Layer<R> cur, Layer<R> n
             bv[e] = code_is_bv((uint8_t)(c4 >> (8 * e)));
             any |= bv[e];
         }
+        if (bv_only && !any) continue;
 #pragma unroll
         for (int v = 0; v < 4; v++) {
             R x[4];
@@ -360,7 +372,7 @@ cudaError_t launch_update_boundaries(const DomainView<R> &d, Layer<R> cur, cudaS
 
 template <typename R>
 cudaError_t launch_step_begin(const DomainView<R> &d, Layer<R> cur, Layer<R> next, Layer<R> ta, Layer<R> tb,
-                              bool update_boundaries, cudaStream_t s)
+                              bool update_boundaries, cudaStream_t s, bool bv_only)
 {
     bool vec = d.n % 4 == 0 && (reinterpret_cast<uintptr_t>(d.code) & 3) == 0;
     for (int v = 0; v < 4; v++)
@@ -368,9 +380,10 @@ cudaError_t launch_step_begin(const DomainView<R> &d, Layer<R> cur, Layer<R> nex
                               (const void *)tb.f[v], (const void *)d.nv[v]})
             vec &= (reinterpret_cast<uintptr_t>(p) & 15) == 0;
     if (vec)
-        step_begin_vec4_kernel<R><<<grid_for(d.n / 4, 256), 256, 0, s>>>(d, cur, next, ta, tb, update_boundaries);
+        step_begin_vec4_kernel<R><<<grid_for(d.n / 4, 256), 256, 0, s>>>(d, cur, next, ta, tb, update_boundaries,
+                                                                         bv_only);
     else
-        step_begin_kernel<R><<<grid_for(d.n, 256), 256, 0, s>>>(d, cur, next, ta, tb, update_boundaries);
+        step_begin_kernel<R><<<grid_for(d.n, 256), 256, 0, s>>>(d, cur, next, ta, tb, update_boundaries, bv_only);
     return cudaGetLastError();
 }
 
@@ -485,7 +498,7 @@ cudaError_t launch_copy_fields(int nf, const void *const *src, void *const *dst,
                                             cudaStream_t);                                                        \
     template cudaError_t launch_update_boundaries<R>(const DomainView<R> &, Layer<R>, cudaStream_t);            \
     template cudaError_t launch_step_begin<R>(const DomainView<R> &, Layer<R>, Layer<R>, Layer<R>, Layer<R>,    \
-                                              bool, cudaStream_t);                                                \
+                                              bool, cudaStream_t, bool);                                          \
     template cudaError_t launch_merge<R>(const DomainView<R> &, CLayer<R>, Layer<R>, cudaStream_t);             \
     template cudaError_t launch_div_error<R>(const DomainView<R> &, CLayer<R>, R, R, R, double *,                \
                                              unsigned long long *, int, double *, unsigned long long *,          \
