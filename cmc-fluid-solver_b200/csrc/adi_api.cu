@@ -811,7 +811,15 @@ adi_status adjoint_run(adi_handle *h, double dt, int ng, int nl, int n_steps, in
     };
     std::vector<void *> ckpt((size_t)nck * 4), fin(4), cb(4), nb(4), hb(4), tb(4), nvb(4), lamb(4);
     for (int c = 0; c < nck; c++) layer4(&ckpt[(size_t)c * 4]);
-    layer4(fin.data()); layer4(cb.data()); layer4(nb.data()); layer4(hb.data()); layer4(tb.data());
+    layer4(fin.data()); layer4(nb.data());
+    // the three adjoint layers every backward step starts from zero, as one block
+    // (one memset per step)
+    char *zblk = (char *)mem.get(12 * fbr, e);
+    for (int v = 0; v < 4 && zblk; v++) {
+        cb[v] = zblk + v * fbr;
+        hb[v] = zblk + (4 + v) * fbr;
+        tb[v] = zblk + (8 + v) * fbr;
+    }
     layer4(nvb.data()); layer4(lamb.data());
     R *ga = (R *)mem.get(fb, e), *gbp = (R *)mem.get(fb, e);
     double *psum = (double *)mem.get(sizeof(double) * DIV_BLOCKS, e), *dJ = (double *)mem.get(sizeof(double), e);
@@ -889,9 +897,7 @@ adi_status adjoint_run(adi_handle *h, double dt, int ng, int nl, int n_steps, in
         for (int t = t1 - 1; t >= t0; t--) {
             void *const *tp = &tape[(size_t)(t - t0) * S * 8];
             if ((st = copy4(nb.data(), cb.data())) != ADI_OK) return st;
-            if ((st = zero4(cb.data())) != ADI_OK) return st;
-            if ((st = zero4(hb.data())) != ADI_OK) return st;
-            if ((st = zero4(tb.data())) != ADI_OK) return st;
+            CK(cudaMemsetAsync(zblk, 0, 12 * fbr, h->stream));   // cb, hb, tb
             int q = S - 1;
             for (int it = ng - 1; it >= 0; it--)
                 for (int dir = 0; dir < 3; dir++) {

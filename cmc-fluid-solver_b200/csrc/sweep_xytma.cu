@@ -46,6 +46,7 @@
 #include "sweep_xyload.cuh"
 
 #include <mutex>
+#include <unordered_map>
 #include <type_traits>
 #include <vector>
 
@@ -499,20 +500,27 @@ struct MapKey {
     }
 };
 
+struct MapKeyHash {
+    size_t operator()(const MapKey &k) const
+    {
+        size_t h = std::hash<const void *>()(k.base);
+        for (int v : {k.kind, k.dir, k.nx, k.ny, k.nz, k.w, k.n, k.es, k.dt}) h = h * 1000003u ^ (size_t)(unsigned)v;
+        return h;
+    }
+};
+
 // Encodes (or finds in the cache) a map of the given rank, dims, strides and box.
+// The cache is a hash map: the adjoint's taped steps sweep over hundreds of tape
+// slots, each with its own maps, and every launch looks up about ten.
 bool encode_cached(CUtensorMap *m, const MapKey &key, int rank, const cuuint64_t *dims, const cuuint64_t *strides,
                    const cuuint32_t *box)
 {
-    struct Ent {
-        MapKey k;
-        CUtensorMap m;
-    };
-    static std::vector<Ent> cache;
+    static std::unordered_map<MapKey, CUtensorMap, MapKeyHash> cache;
     static std::mutex mu;
     {
         std::lock_guard<std::mutex> g(mu);
-        for (const Ent &e : cache)
-            if (e.k == key) { *m = e.m; return true; }
+        auto it = cache.find(key);
+        if (it != cache.end()) { *m = it->second; return true; }
     }
     auto enc = get_encoder_fn();
     if (!enc) return false;
@@ -522,8 +530,8 @@ bool encode_cached(CUtensorMap *m, const MapKey &key, int rank, const cuuint64_t
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return false;
     std::lock_guard<std::mutex> g(mu);
-    if (cache.size() > 4096) cache.clear();
-    cache.push_back({key, *m});
+    if (cache.size() > 16384) cache.clear();
+    cache.emplace(key, *m);
     return true;
 }
 } // namespace

@@ -334,13 +334,15 @@ def test_time_step_with_boundary_state_off_node_values(adi_lib, precision):
     assert max(errs) < (1e-11 if precision == "fp64" else 2e-6), errs
 
 
-@pytest.mark.parametrize("precision", ["fp32", "fp64"])
-def test_step_io_pipelined_time_march_equals_separate_calls(adi_lib, precision):
+@pytest.mark.parametrize("case", ["fp32", "fp64", "fp32-exact-direct"])
+def test_step_io_pipelined_time_march_equals_separate_calls(adi_lib, case):
     """adi_step_io chained through host buffers (each call uploads the previous
     call's download) equals adi_set_state + adi_step + adi_get_state bit for bit,
-    with and without the divergence error, and adi_io_wait orders later work."""
+    with and without the divergence error (graph replay, and direct launches with
+    the exact solver), and adi_io_wait orders later work."""
     import torch
     from adi_b200 import _abi
+    precision = "fp64" if case == "fp64" else "fp32"
     d = G.random_domain(40, 36, 44, seed=91, shell=True, n_obstacles=6, rmax=4.5)
     params = (150.0, 0.72, 1.4)
     prec = _abi.ADI_FP64 if precision == "fp64" else _abi.ADI_FP32
@@ -348,6 +350,10 @@ def test_step_io_pipelined_time_march_equals_separate_calls(adi_lib, precision):
     b = solver(adi_lib, d, params, precision=prec)
     for dr, (K, NL, _) in enumerate(a.fast_shapes()):
         b.set_fast_shape(dr, K, NL)
+    if case == "fp32-exact-direct":
+        for s_ in (a, b):
+            s_._check(s_.lib.adi_set_solver(s_.h, _abi.ADI_SOLVER_EXACT))
+            s_.set_graphs(False)
     dt_ = np.float32 if precision == "fp32" else np.float64
     pin = [torch.empty(d.shape, dtype=torch.float32 if precision == "fp32" else torch.float64,
                        pin_memory=True).numpy() for _ in range(8)]
