@@ -452,7 +452,7 @@ bool adjoint_chunk_supported(int len, int K, int elem_bytes, int &NL, int &P)
 // likewise), which the fused path writes into two planes and gathers in a
 // second kernel.  Every cell has one writer, so no order of blocks matters.
 template <typename R, int DIR>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
     adjoint_accum_kernel(DomainView<R> d, CLayer<R> lam, CLayer<R> ti, CLayer<R> xs, Layer<R> sbar, Layer<R> tbar,
                          SweepConst<R> kc, int merges)
 {
