@@ -38,9 +38,12 @@ accuracy: max relative field error of 10 FP32 steps (the timed path) against 10
 cpu_baseline: the reference's own CPU solver (oracle/_ref/libref3d.so, compiled
          from its sources) on the same workload on this host's cores (rank 0, N=1).
 
-Multi-GPU: the single-domain step does not shard (the reference's slab
-decomposition is out of scope), so N ranks run N independent replicas
-("replicas only"); value = all ranks' cell-steps / max-over-ranks time.
+Multi-GPU: N ranks run N independent replicas of the single-domain workloads
+("replicas only": weak scaling, no data-path collective); value = all ranks'
+cell-steps / max-over-ranks time.  batched64 shards its domains over the ranks
+(LPT by cost), each rank stepping its share as one batch.  The split of one
+domain over several solvers (adi_b200.slabs: X slabs, Y pencils, ghost planes)
+is tested on one GPU and over gloo ranks, not timed here.
 --impl reference times the reference CPU solver instead (rank 0 only).
 """
 from __future__ import annotations
