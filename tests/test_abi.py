@@ -47,3 +47,27 @@ def test_fluid_params_match_reference_formulas(adi_lib):
     assert p.t_phi == (1.4 - 1.0) / (1.4 * 200.0)
     q = adi_lib.fluid_params_dimensional(0.05, 1000.0, 461.495, 0.6, 4200.0)
     assert (q.v_T, q.v_vis, q.t_vis, q.t_phi) == (461.495, 0.05 / 1000.0, 0.6 / (1000.0 * 4200.0), 0.05 / (1000.0 * 4200.0))
+
+
+def test_entry_points_reject_a_null_handle(adi_lib):
+    """Handle-taking entry points answer ADI_ERR_BAD_ARG for a NULL handle or batch
+    before they touch the device (so this runs without a GPU)."""
+    from adi_b200 import _abi
+    lib = _abi.load()
+    vp = ctypes.c_void_p
+    four = (vp * 4)()
+    d, i = ctypes.c_double(1e-3), ctypes.c_int(0)
+    calls = [
+        ("adi_step_io", (None, four, four, d, 1, 1, 0)),
+        ("adi_io_wait", (None,)),
+        ("adi_phase_begin", (None, 1)),
+        ("adi_phase_sweep", (None, 0, d, 1)),
+        ("adi_phase_end", (None,)),
+        ("adi_set_fault_injection", (None, 0)),
+        ("adi_set_adjoint_chunk", (None, -4)),
+        ("adi_batch_set_schedule", (None, 1, 2)),
+        ("adi_batch_get_schedule", (None, ctypes.byref(i), ctypes.byref(i))),
+        ("adi_batch_time_step", (None, d, 1, 1, 1, ctypes.byref(ctypes.c_float()))),
+    ]
+    for name, args in calls:
+        assert getattr(lib, name)(*args) == _abi.ADI_ERR_BAD_ARG, name
