@@ -39,6 +39,7 @@ SOURCES = [
     ("adjoint_fast.cu", []),
     ("adi2d.cu", ["--fmad=false"]),
     ("masks.cu", ["--fmad=false"]),
+    ("netcdf_out.cu", []),
 ]
 
 

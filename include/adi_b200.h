@@ -604,6 +604,35 @@ size_t adi_static_scratch_bytes(void);
 /* Library build/version string. */
 const char *adi_version(void);
 
+/* ---- result files ------------------------------------------------------- */
+
+/* The reference's result file (Common/IO.h:136-276 OutputNetCDF3D_header and
+ * :340-377 OutputNetCDF3D_layer, called from FluidSolver3D.cpp:206 and :258) with the
+ * same dimensions (x, y, z, unlimited t), variables (x, y, z float axes; time double
+ * [t]; u, v, w, T double [t][x][y][z]; d float [x][y]), attributes and values,
+ * written as a NetCDF classic file (64-bit offset format) because no NetCDF-4 /
+ * HDF5 library is available here; any NetCDF reader opens it.  Host code, no
+ * device.
+ *
+ * adi_nc_write_header: creates `path`; vars is the reference's out_vars list as
+ * comma-separated short names ("u,v,w,T,d"); the time axis holds time / timestep
+ * records (their data the fill value until written); depth (depth_nx x depth_ny,
+ * [x][y]) is point-sampled to the output grid as DepthInfo3D does and needed only
+ * when vars names "d"; xy_degree_units: the x / y axes' units are degree_north /
+ * degree_east instead of metres.
+ * adi_nc_write_layer: writes record `layer` of every data variable vars names
+ * (except d) from vel (3 values per cell, float or double: vel_elem_bytes 4 or 8,
+ * as Vec3D holds FTYPE) and T (double), cells [x][y][z] as GetLayer gives them;
+ * a layer past the last record extends the record count. */
+typedef struct {
+    float pmin[3], pmax[3];   /* BBox3D pMin, pMax */
+} adi_bbox3d;
+adi_status adi_nc_write_header(const char *path, const adi_bbox3d *bbox, const float *depth, int depth_nx,
+                               int depth_ny, double timestep, double time, int outdimx, int outdimy, int outdimz,
+                               const char *vars, int xy_degree_units);
+adi_status adi_nc_write_layer(const char *path, const void *vel, int vel_elem_bytes, const double *T, int layer,
+                              int outdimx, int outdimy, int outdimz, const char *vars);
+
 #ifdef __cplusplus
 }
 #endif
