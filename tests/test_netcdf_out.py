@@ -87,3 +87,30 @@ def test_layers_past_the_time_axis_and_a_subset_of_variables(adi_lib, tmp_path):
         assert np.all(f.variables["time"][2:] == FILL)
     with pytest.raises(Exception):
         ncout.write_layer(path, vel[:2], T[:2], 0, ["u", "T"])   # dims differ from the file's
+
+
+@pytest.mark.gpu
+def test_driver_output_path_getlayer_to_result_file(adi_lib, tmp_path):
+    """The reference driver's output path (FluidSolver3D.cpp:206, 248-258): header,
+    then every out_time_steps-th step GetLayer on the output grid and one layer of
+    the result file; the file holds exactly what GetLayer returned."""
+    from scipy.io import netcdf_file
+    from adi_b200 import geometry as G, ncout
+    d = G.spheres_channel(dims=(40, 24, 28), n_spheres=3, rmin=3.0, rmax=5.0, seed=9)
+    s = adi_lib.AdiSolver3D(d, Re=150.0, Pr=0.72, lam=1.4)
+    s.CreateSegments()
+    out_dims, out_vars, dt = (20, 12, 14), ["u", "v", "w", "T"], 5e-4
+    path = str(tmp_path / "run_res.nc")
+    ncout.write_header(path, (0.0, 0.0, 0.0), (1.0, 0.6, 0.7), 2 * dt, 6 * dt, out_dims, out_vars)
+    layers = []
+    for i in range(6):
+        assert s.step(dt, 4, 2, i % 10 == 0) == 0
+        if i % 2 == 0:
+            v, T = s.GetLayer(*out_dims)
+            ncout.write_layer(path, v, T, len(layers), out_vars)
+            layers.append((v.copy(), T.copy()))
+    with netcdf_file(path, "r", mmap=False) as f:
+        for r, (v, T) in enumerate(layers):
+            for c, k in enumerate("uvw"):
+                np.testing.assert_array_equal(f.variables[k][r], v[..., c].astype(np.float64))
+            np.testing.assert_array_equal(f.variables["T"][r], T)
