@@ -337,7 +337,8 @@ adi_status adi_nc_write_header(const char *path, const adi_bbox3d *bbox, const f
                                const char *vars, int xy_degree_units)
 {
     bool use[5];
-    if (!path || !bbox || !parse_vars(vars, use) || outdimx < 1 || outdimy < 1 || outdimz < 1 || !(timestep > 0))
+    if (!path || !bbox || !parse_vars(vars, use) || outdimx < 1 || outdimy < 1 || outdimz < 1 || !(timestep > 0) ||
+        !(time >= 0) || time / timestep > 1e7)
         return ADI_ERR_BAD_ARG;
     if (use[4] && (!depth || depth_nx < 1 || depth_ny < 1)) return ADI_ERR_BAD_ARG;
     Layout L;
