@@ -306,6 +306,26 @@ class AdiBatch:
         self._check(self.lib.adi_batch_launches(self.b, C.byref(v)))
         return v.value
 
+    def step_io(self, inputs, outputs, dt, num_global, num_local, compute_error=False) -> int:
+        """adi_batch_step_io: inputs / outputs hold, per member, its (u, v, w, T) host
+        arrays (the member's shape and dtype); asynchronous until io_wait()."""
+        n = len(self.members)
+        flat_in = [a for m in inputs for a in m]
+        flat_out = [a for m in outputs for a in m]
+        if len(flat_in) != 4 * n or len(flat_out) != 4 * n:
+            raise ValueError("four arrays per member in and out")
+        for q, m in enumerate(self.members):
+            for a in list(inputs[q]) + list(outputs[q]):
+                if not (isinstance(a, np.ndarray) and a.dtype == m.dtype and a.flags.c_contiguous
+                        and a.shape == tuple(m.shape)):
+                    raise ValueError("step_io takes C-contiguous arrays of each member's shape and dtype")
+        ins = (C.c_void_p * (4 * n))(*[a.ctypes.data for a in flat_in])
+        outs = (C.c_void_p * (4 * n))(*[a.ctypes.data for a in flat_out])
+        return self.lib.adi_batch_step_io(self.b, ins, outs, dt, num_global, num_local, int(compute_error))
+
+    def io_wait(self):
+        self._check(self.lib.adi_batch_io_wait(self.b))
+
     def set_schedule(self, schedule: int, branches: int = 1):
         """ADI_BATCH_PERSISTENT (one multi-domain launch per sweep) or
         ADI_BATCH_MEMBER_GRAPHS (each member's own step on `branches` graph branches)."""

@@ -35,7 +35,7 @@ EXPORTED = [
     "adi_batch_create", "adi_batch_destroy", "adi_batch_set_stream", "adi_batch_step", "adi_batch_div_errors",
     "adi_batch_set_chunk", "adi_batch_get_chunk", "adi_batch_autotune", "adi_batch_set_graphs",
     "adi_batch_launches", "adi_batch_last_error_string", "adi_batch_time_sweeps", "adi_batch_set_schedule",
-    "adi_batch_get_schedule", "adi_batch_time_step", "adi_step_io", "adi_io_wait", "adi_nc_write_header", "adi_nc_write_layer", "adi_adjoint_run",
+    "adi_batch_get_schedule", "adi_batch_time_step", "adi_step_io", "adi_io_wait", "adi_batch_step_io", "adi_batch_io_wait", "adi_nc_write_header", "adi_nc_write_layer", "adi_adjoint_run",
     "adi_set_node_values", "adi_set_adjoint_chunk", "adi2d_create", "adi2d_destroy", "adi2d_set_stream", "adi2d_set_grid",
     "adi2d_set_segments", "adi2d_step_tol",
     "adi2d_update_boundaries", "adi2d_time_step", "adi2d_step", "adi2d_get_state", "adi2d_set_state",
@@ -137,6 +137,8 @@ def load() -> C.CDLL:
         "adi_batch_time_step": [vp, d, i, i, i, C.POINTER(C.c_float)],
         "adi_step_io": [vp, C.POINTER(vp), C.POINTER(vp), d, i, i, i],
         "adi_io_wait": [vp],
+        "adi_batch_step_io": [vp, C.POINTER(vp), C.POINTER(vp), d, i, i, i],
+        "adi_batch_io_wait": [vp],
         "adi_nc_write_header": [C.c_char_p, vp, vp, i, i, d, d, i, i, i, C.c_char_p, i],
         "adi_nc_write_layer": [C.c_char_p, vp, i, vp, i, i, i, i, C.c_char_p],
         "adi_adjoint_run": [vp, d, i, i, i, i, vp, vp, C.POINTER(d), vp, vp],

@@ -2189,6 +2189,103 @@ adi_status batch_step(adi_batch *b, double dt, int num_global, int num_local, in
     return ADI_OK;
 }
 
+// A batch step with host buffers: every member's state uploaded from in[4 q + f],
+// the step, the new state downloaded into out[4 q + f].  Member-graph schedule:
+// each branch stream runs, member after member, the upload, the member's own step
+// and the download, so one branch's copies overlap the other branches' sweeps
+// (members are independent).  Persistent schedule: all uploads, the batch step,
+// all downloads.  The next call's work waits for this call's (its uploads may read
+// this call's downloads).
+template <typename R>
+adi_status batch_step_io(adi_batch *b, const void *const *in, void *const *out, double dt, int num_global,
+                         int num_local, int compute_error)
+{
+    const int n = (int)b->hs.size();
+    adi_handle *h0 = b->hs[0];
+    if (b->schedule != ADI_BATCH_MEMBER_GRAPHS) {
+        for (int q = 0; q < n; q++) {
+            adi_handle *h = b->hs[q];
+            const size_t fb = (size_t)h->n * sizeof(R);
+            for (int f = 0; f < 4; f++)
+                BCK(cudaMemcpyAsync(h->d_L[h->cur][f], in[4 * q + f], fb, cudaMemcpyHostToDevice, b->stream));
+        }
+        adi_status s = batch_step<R>(b, dt, num_global, num_local, compute_error);
+        if (s != ADI_OK) return s;
+        for (int q = 0; q < n; q++) {
+            adi_handle *h = b->hs[q];
+            const size_t fb = (size_t)h->n * sizeof(R);
+            for (int f = 0; f < 4; f++)
+                BCK(cudaMemcpyAsync(out[4 * q + f], h->d_L[h->cur][f], fb, cudaMemcpyDeviceToHost, b->stream));
+        }
+        return ADI_OK;
+    }
+    adi_status s = batch_load_dt<R>(b, dt);
+    if (s != ADI_OK) return s;
+    const int cur = h0->cur, nxt = h0->nxt, ta0 = h0->ta, tb0 = h0->tb;
+    int ta = ta0, tb = tb0;
+    BCK(cudaEventRecord(b->ev_fork, b->stream));
+    for (int w = 0; w < b->branches; w++) {
+        if (b->branch_members[w].empty()) continue;
+        BCK(cudaStreamWaitEvent(b->br[w], b->ev_fork, 0));
+        for (int q : b->branch_members[w]) {
+            adi_handle *h = b->hs[q];
+            const size_t fb = (size_t)h->n * sizeof(R);
+            for (int f = 0; f < 4; f++)
+                BCK(cudaMemcpyAsync(h->d_L[cur][f], in[4 * q + f], fb, cudaMemcpyHostToDevice, b->br[w]));
+            const cudaStream_t own = h->stream;
+            const bool prof = h->prof_on;
+            int64_t l0[ADI_K_NUM], b0[ADI_K_NUM];
+            memcpy(l0, h->launches, sizeof l0);
+            memcpy(b0, h->bytes, sizeof b0);
+            h->prof_on = false;
+            h->stream = b->br[w];
+            h->ta = ta0;
+            h->tb = tb0;
+            const adi_status st = enqueue_step<R>(h, (R)dt, num_global, num_local, compute_error, true);
+            h->stream = own;
+            h->prof_on = prof;
+            for (int c = 0; c < ADI_K_NUM; c++) b->launches += h->launches[c] - l0[c];
+            memcpy(h->launches, l0, sizeof l0);   // the batch counts these launches, not the member
+            memcpy(h->bytes, b0, sizeof b0);
+            ta = h->ta;
+            tb = h->tb;
+            h->ta = ta0;
+            h->tb = tb0;
+            if (st != ADI_OK) return bfail(b, st, std::string("member step: ") + h->err);
+            for (int f = 0; f < 4; f++)   // the new state: next until the roles swap below
+                BCK(cudaMemcpyAsync(out[4 * q + f], h->d_L[nxt][f], fb, cudaMemcpyDeviceToHost, b->br[w]));
+        }
+        BCK(cudaEventRecord(b->ev_join[w], b->br[w]));
+        BCK(cudaStreamWaitEvent(b->stream, b->ev_join[w], 0));
+    }
+    bool diverged = false;
+    if (compute_error) {
+        BCK(cudaStreamSynchronize(b->stream));
+        for (int q = 0; q < n; q++) {
+            adi_handle *h = b->hs[q];
+            b->diff_error[q] = h->h_pin->cnt ? h->h_pin->sum / (double)h->h_pin->cnt : 0.0;
+            if (h->h_pin->err) {
+                h->h_pin->err = 0;
+                BCK(cudaMemsetAsync(h->d_err, 0, sizeof(int), b->stream));
+                return bfail(b, ADI_ERR_TIMEOUT, "a member sweep's bounded wait for its input tiles gave up");
+            }
+        }
+    }
+    for (int q = 0; q < n; q++) diverged |= b->diff_error[q] > 0.01;
+    for (int q = 0; q < n; q++) {
+        adi_handle *h = b->hs[q];
+        h->ta = ta;
+        h->tb = tb;
+        h->diff_error = b->diff_error[q];
+        if (!diverged) {
+            std::swap(h->cur, h->nxt);
+            h->bv_synced = false;
+        }
+    }
+    if (diverged) return bfail(b, ADI_ERR_DIVERGENCE, "a domain's divergence error is above 0.01; no domain advanced");
+    return ADI_OK;
+}
+
 // Mean time of one whole step with the current schedule and chunk lengths,
 // replayed from a graph captured for it; the layer roles are left as they were
 // (the step is not finished: cur keeps the state).
@@ -2363,6 +2460,29 @@ adi_status adi_batch_step(adi_batch *b, double dt, int num_global, int num_local
             return bfail(b, ADI_ERR_STATE, "a batch member was stepped on its own; step members only through the batch");
     if (b->prec == ADI_FP64) return batch_step<double>(b, dt, num_global, num_local, compute_error);
     return batch_step<float>(b, dt, num_global, num_local, compute_error);
+}
+
+adi_status adi_batch_step_io(adi_batch *b, const void *const *in, void *const *out, double dt, int num_global,
+                             int num_local, int compute_error)
+{
+    if (!b || !in || !out) return ADI_ERR_BAD_ARG;
+    if (num_global < 1 || num_local < 1) return bfail(b, ADI_ERR_BAD_ARG, "num_global and num_local must be >= 1");
+    if (!(dt > 0) || !std::isfinite(dt)) return bfail(b, ADI_ERR_BAD_ARG, "dt must be positive and finite");
+    for (size_t i = 0; i < 4 * b->hs.size(); i++)
+        if (!in[i] || !out[i]) return ADI_ERR_BAD_ARG;
+    const adi_handle *h0 = b->hs[0];
+    for (auto *h : b->hs)
+        if (h->cur != h0->cur || h->nxt != h0->nxt || h->ta != h0->ta || h->tb != h0->tb)
+            return bfail(b, ADI_ERR_STATE, "a batch member was stepped on its own; step members only through the batch");
+    if (b->prec == ADI_FP64) return batch_step_io<double>(b, in, out, dt, num_global, num_local, compute_error);
+    return batch_step_io<float>(b, in, out, dt, num_global, num_local, compute_error);
+}
+
+adi_status adi_batch_io_wait(adi_batch *b)
+{
+    if (!b) return ADI_ERR_BAD_ARG;
+    BCK(cudaStreamSynchronize(b->stream));
+    return ADI_OK;
 }
 
 adi_status adi_batch_autotune(adi_batch *b, double dt, int reps)

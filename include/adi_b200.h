@@ -493,6 +493,19 @@ adi_status adi_batch_set_stream(adi_batch *b, void *cuda_stream);
  * ADI_ERR_DIVERGENCE and no member advances. */
 adi_status adi_batch_step(adi_batch *b, double dt, int num_global, int num_local, int compute_error);
 
+/* adi_batch_step with host buffers: member q's state is uploaded from in[4 q + f]
+ * (f = u, v, w, T; the member's precision) and its new state downloaded into
+ * out[4 q + f].  With the member-graph schedule each branch runs, member after
+ * member, the upload, the member's step and the download, so copies overlap other
+ * members' sweeps; with the persistent schedule all uploads precede the step and
+ * all downloads follow it.  Returns once queued (after the divergence check when
+ * compute_error); call adi_batch_io_wait before reading out.  A call may take the
+ * previous call's out as its in.  On ADI_ERR_DIVERGENCE no member advances (out
+ * then holds the rejected step's results). */
+adi_status adi_batch_step_io(adi_batch *b, const void *const *in, void *const *out, double dt, int num_global,
+                             int num_local, int compute_error);
+adi_status adi_batch_io_wait(adi_batch *b);
+
 /* Last computed divergence error of each member (n values). */
 adi_status adi_batch_div_errors(adi_batch *b, double *out);
 

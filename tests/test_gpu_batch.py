@@ -200,3 +200,43 @@ def test_member_graph_divergence_guard_and_autotune(adi_lib):
             assert np.array_equal(members[q].fields(0)[f][fluid], before[q][f][fluid])
     with pytest.raises(_abi.AdiError):
         b.set_schedule(_abi.ADI_BATCH_MEMBER_GRAPHS, 5)
+
+
+@pytest.mark.parametrize("schedule", ["member", "persistent"])
+def test_batch_step_io_time_march_equals_separate_calls(adi_lib, schedule):
+    """adi_batch_step_io chained through host buffers equals, member by member,
+    set_state + the batch step + get_state, in both schedules."""
+    import torch
+    from adi_b200 import _abi
+    ds = _domains(13, n=5)
+    a_m = [_member(adi_lib, d, solver=_abi.ADI_SOLVER_FAST) for d in ds]
+    b_m = [_member(adi_lib, d, solver=_abi.ADI_SOLVER_FAST) for d in ds]
+    for m, s in zip(a_m, b_m):
+        for dr, (K, NL, _) in enumerate(m.fast_shapes()):
+            s.set_fast_shape(dr, K, NL)
+    a, b = adi_lib.AdiBatch(a_m), adi_lib.AdiBatch(b_m)
+    for bb in (a, b):
+        if schedule == "member":
+            bb.set_schedule(_abi.ADI_BATCH_MEMBER_GRAPHS, 2)
+        for dr in range(3):
+            bb.set_chunk(dr, 4)
+    pin = [[[torch.empty(d.shape, dtype=torch.float32, pin_memory=True).numpy() for _ in range(4)]
+            for d in ds] for _ in range(2)]
+    for q, m in enumerate(a_m):
+        for x, y in zip(pin[0][q], m.fields(0)):
+            x[...] = y
+    state = [[x.copy() for x in pin[0][q]] for q in range(len(ds))]
+    src, dst = 0, 1
+    for i in range(3):
+        assert a.step_io(pin[src], pin[dst], 6e-4, 2, 2, i in (0, 2)) == 0, a.last_error()
+        src, dst = dst, src
+    a.io_wait()
+    for i in range(3):
+        for q, m in enumerate(b_m):
+            m.set_state(*state[q])
+        assert b.step(6e-4, 2, 2, i in (0, 2)) == 0, b.last_error()
+        state = [[x.copy() for x in m.fields(0)] for m in b_m]
+    for q in range(len(ds)):
+        for f in range(4):
+            assert np.array_equal(pin[src][q][f], state[q][f]), (q, f)
+    assert np.array_equal(a.div_errors(), b.div_errors())
