@@ -2019,6 +2019,37 @@ void batch_assign_branches(adi_batch *b)
     }
 }
 
+// One member's own step (what adi_step enqueues) on a branch stream, its
+// nonlinear layers starting from the batch's roles (ta0, tb0); ta / tb receive
+// the roles after it.  The batch counts the launches, not the member; per-launch
+// profiling events stay out of batch graphs.
+template <typename R>
+adi_status enqueue_member_step(adi_batch *b, adi_handle *h, cudaStream_t stream, int num_global, int num_local,
+                               int compute_error, int ta0, int tb0, int &ta, int &tb)
+{
+    const cudaStream_t own = h->stream;
+    int64_t l0[ADI_K_NUM], b0[ADI_K_NUM];
+    memcpy(l0, h->launches, sizeof l0);
+    memcpy(b0, h->bytes, sizeof b0);
+    const bool prof = h->prof_on;
+    h->prof_on = false;
+    h->stream = stream;
+    h->ta = ta0;
+    h->tb = tb0;
+    h->bv_synced = true;
+    const adi_status s = enqueue_step<R>(h, (R)b->dt_loaded, num_global, num_local, compute_error, true);
+    h->stream = own;
+    h->prof_on = prof;
+    for (int c = 0; c < ADI_K_NUM; c++) b->launches += h->launches[c] - l0[c];
+    memcpy(h->launches, l0, sizeof l0);
+    memcpy(h->bytes, b0, sizeof b0);
+    ta = h->ta;
+    tb = h->tb;
+    h->ta = ta0;
+    h->tb = tb0;
+    return s == ADI_OK ? ADI_OK : bfail(b, s, std::string("member step: ") + h->err);
+}
+
 // The member-graph schedule: every member's own step (its solver, kernels and
 // shapes, as adi_step enqueues it) on one of `branches` streams forked from and
 // joined back into the batch stream, so one member's launch tails and gaps
@@ -2033,30 +2064,9 @@ adi_status batch_enqueue_members(adi_batch *b, int num_global, int num_local, in
         if (b->branch_members[w].empty()) continue;
         BCK(cudaStreamWaitEvent(b->br[w], b->ev_fork, 0));
         for (int q : b->branch_members[w]) {
-            adi_handle *h = b->hs[q];
-            const cudaStream_t own = h->stream;
-            int64_t l0[ADI_K_NUM], b0[ADI_K_NUM];
-            memcpy(l0, h->launches, sizeof l0);
-            memcpy(b0, h->bytes, sizeof b0);
-            const bool prof = h->prof_on;
-            h->prof_on = false;   // per-launch events do not belong in a batch graph
-            h->stream = b->br[w];
-            h->ta = ta0;
-            h->tb = tb0;
-            h->bv_synced = true;
-            const adi_status s = enqueue_step<R>(h, (R)b->dt_loaded, num_global, num_local, compute_error, true);
-            h->stream = own;
-            h->prof_on = prof;
-            int64_t nl = 0;
-            for (int c = 0; c < ADI_K_NUM; c++) nl += h->launches[c] - l0[c];
-            b->launches += nl;
-            memcpy(h->launches, l0, sizeof l0);   // the batch counts these launches, not the member
-            memcpy(h->bytes, b0, sizeof b0);
-            ta = h->ta;
-            tb = h->tb;
-            h->ta = ta0;
-            h->tb = tb0;
-            if (s != ADI_OK) return bfail(b, s, std::string("member step: ") + h->err);
+            const adi_status s = enqueue_member_step<R>(b, b->hs[q], b->br[w], num_global, num_local, compute_error,
+                                                        ta0, tb0, ta, tb);
+            if (s != ADI_OK) return s;
         }
         BCK(cudaEventRecord(b->ev_join[w], b->br[w]));
         BCK(cudaStreamWaitEvent(b->stream, b->ev_join[w], 0));
@@ -2232,26 +2242,9 @@ adi_status batch_step_io(adi_batch *b, const void *const *in, void *const *out, 
             const size_t fb = (size_t)h->n * sizeof(R);
             for (int f = 0; f < 4; f++)
                 BCK(cudaMemcpyAsync(h->d_L[cur][f], in[4 * q + f], fb, cudaMemcpyHostToDevice, b->br[w]));
-            const cudaStream_t own = h->stream;
-            const bool prof = h->prof_on;
-            int64_t l0[ADI_K_NUM], b0[ADI_K_NUM];
-            memcpy(l0, h->launches, sizeof l0);
-            memcpy(b0, h->bytes, sizeof b0);
-            h->prof_on = false;
-            h->stream = b->br[w];
-            h->ta = ta0;
-            h->tb = tb0;
-            const adi_status st = enqueue_step<R>(h, (R)dt, num_global, num_local, compute_error, true);
-            h->stream = own;
-            h->prof_on = prof;
-            for (int c = 0; c < ADI_K_NUM; c++) b->launches += h->launches[c] - l0[c];
-            memcpy(h->launches, l0, sizeof l0);   // the batch counts these launches, not the member
-            memcpy(h->bytes, b0, sizeof b0);
-            ta = h->ta;
-            tb = h->tb;
-            h->ta = ta0;
-            h->tb = tb0;
-            if (st != ADI_OK) return bfail(b, st, std::string("member step: ") + h->err);
+            const adi_status st = enqueue_member_step<R>(b, h, b->br[w], num_global, num_local, compute_error, ta0,
+                                                         tb0, ta, tb);
+            if (st != ADI_OK) return st;
             for (int f = 0; f < 4; f++)   // the new state: next until the roles swap below
                 BCK(cudaMemcpyAsync(out[4 * q + f], h->d_L[nxt][f], fb, cudaMemcpyDeviceToHost, b->br[w]));
         }
