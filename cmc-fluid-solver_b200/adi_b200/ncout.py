@@ -39,6 +39,8 @@ def write_layer(path: str, vel, T, layer: int, out_vars) -> None:
         raise ValueError("vel must be [x][y][z][3] float32 or float64")
     T = np.ascontiguousarray(T, np.float64)
     nx, ny, nz = vel.shape[:3]
+    if T.shape != (nx, ny, nz):
+        raise ValueError(f"T must be [x][y][z] like vel, got {T.shape} for {vel.shape[:3]}")
     rc = lib.adi_nc_write_layer(path.encode(), vel.ctypes.data, vel.itemsize, T.ctypes.data, layer, nx, ny, nz,
                                 ",".join(out_vars).encode())
     if rc != 0:

@@ -343,6 +343,9 @@ adi_status adi_nc_write_header(const char *path, const adi_bbox3d *bbox, const f
     if (use[4] && (!depth || depth_nx < 1 || depth_ny < 1)) return ADI_ERR_BAD_ARG;
     Layout L;
     L.vars = define_vars(*bbox, time, outdimx, outdimy, outdimz, use, xy_degree_units != 0);
+    // the 64-bit offset format stores a variable's size (one record of it) in 32 bits
+    for (const Var &v : L.vars)
+        if (v.vsize > 0xFFFFFFFCull) return ADI_ERR_BAD_ARG;
     // the time axis is written for time / timestep records (IO.h:260-266)
     const uint32_t count = (uint32_t)(int)(time / timestep);
     place(L, count, outdimx, outdimy, outdimz);

@@ -632,7 +632,9 @@ const char *adi_version(void);
  * records (their data the fill value until written); depth (depth_nx x depth_ny,
  * [x][y]) is point-sampled to the output grid as DepthInfo3D does and needed only
  * when vars names "d"; xy_degree_units: the x / y axes' units are degree_north /
- * degree_east instead of metres.
+ * degree_east instead of metres.  ADI_ERR_BAD_ARG for a file that cannot be written,
+ * a negative time, more than 1e7 records, or one record of a variable above the
+ * format's 4 GiB (outdimx * outdimy * outdimz * 8 bytes).
  * adi_nc_write_layer: writes record `layer` of every data variable vars names
  * (except d) from vel (3 values per cell, float or double: vel_elem_bytes 4 or 8,
  * as Vec3D holds FTYPE) and T (double), cells [x][y][z] as GetLayer gives them;

@@ -89,6 +89,21 @@ def test_layers_past_the_time_axis_and_a_subset_of_variables(adi_lib, tmp_path):
         ncout.write_layer(path, vel[:2], T[:2], 0, ["u", "T"])   # dims differ from the file's
 
 
+def test_header_arguments_the_format_cannot_hold_are_rejected(adi_lib, tmp_path):
+    from adi_b200 import _abi, ncout
+    path = tmp_path / "bad_res.nc"
+    bad = [
+        dict(timestep=0.1, time=-1.0, outdims=(2, 2, 2)),            # negative time
+        dict(timestep=1e-9, time=1.0, outdims=(2, 2, 2)),            # 1e9 records
+        dict(timestep=0.1, time=1.0, outdims=(1024, 1024, 1024)),    # 8 GiB per record of u
+        dict(timestep=0.1, time=1.0, outdims=(0, 2, 2)),
+    ]
+    for kw in bad:
+        with pytest.raises(_abi.AdiError):
+            ncout.write_header(str(path), (0, 0, 0), (1, 1, 1), kw["timestep"], kw["time"], kw["outdims"], ["u"])
+        assert not path.exists()
+
+
 @pytest.mark.gpu
 def test_driver_output_path_getlayer_to_result_file(adi_lib, tmp_path):
     """The reference driver's output path (FluidSolver3D.cpp:206, 248-258): header,
