@@ -440,7 +440,7 @@ std::vector<FastShape> shape_candidates(const adi_handle *h, int dir)
     std::vector<FastShape> out;
     const int len = line_len(h, dir);
     if (dir == 2)
-        for (int K : {4, 5, 8}) {
+        for (int K : {4, 5, 8, 12}) {
             FastShape s{K, 0, (len + K - 1) / K, 1};
             if (shape_ok(h, dir, s)) out.push_back(s);
         }

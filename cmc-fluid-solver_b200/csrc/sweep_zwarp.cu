@@ -18,8 +18,8 @@
 // generic fast sweep (sweep_fast.cu); see the comments there.  The chunk
 // elimination, the cyclic-reduction step and the PCR updates are the shared ones
 // of sweep_common.cuh (packed FP32 in float).  Requirements
-// (checked by the launcher): K in {4, 5, 8}, dimz <= 32*K, 16-byte aligned field
-// arrays.
+// (checked by the launcher): K in {4, 5, 8}, or 12 in FP32 for 256 < dimz <= 384;
+// dimz <= 32*K; 16-byte aligned field arrays.
 #include "adi_internal.cuh"
 #include "sweep_common.cuh"
 
@@ -334,15 +334,17 @@ __global__ void __launch_bounds__(128)
 // Lanes per line: the smallest of 4, 8, 16, 32 whose chunks cover dimz (0: none).
 int zwarp_lanes(int nz, int K)
 {
-    if (K != 4 && K != 5 && K != 8) return 0;
+    if (K != 4 && K != 5 && K != 8 && K != 12) return 0;
     for (int P = 4; P <= 32; P *= 2)
         if (P * K >= nz) return P;
     return 0;
 }
 
+// K = 12 is compiled for lines of 257 to 384 rows only (32 lanes), and only in
+// FP32: in FP64 its rows do not fit in the registers.
 bool zwarp_supported(int nz, int K, int elem_bytes)
 {
-    (void)elem_bytes;
+    if (K == 12 && (elem_bytes != 4 || zwarp_lanes(nz, K) != 32 || nz <= 256)) return false;
     return nz >= 1 && zwarp_lanes(nz, K) > 0;
 }
 
@@ -371,6 +373,9 @@ cudaError_t launch_sweep_zwarp(const DomainView<R> &d, const int *line_lo, const
         return cudaGetLastError();                                                                              \
     }
     ZL(4, 4) ZL(4, 8) ZL(4, 16) ZL(4, 32) ZL(5, 4) ZL(5, 8) ZL(5, 16) ZL(5, 32) ZL(8, 4) ZL(8, 8) ZL(8, 16) ZL(8, 32)
+    if constexpr (sizeof(R) == 4) {
+        ZL(12, 32)
+    }
 #undef ZL
     return cudaErrorInvalidConfiguration;
 }

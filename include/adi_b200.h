@@ -307,8 +307,9 @@ adi_status adi_div_error(adi_handle *h, double *out);
 
 /* Launch shape of the fast sweep for one direction: each thread owns K
  * consecutive rows of a line, a CTA holds NL lines, P = ceil(len/K) chunks per
- * line.  NL = 0 selects the warp-resident Z kernel (Z only; dimz = P*K with P in
- * {4, 8, 16, 32}, K in {4, 8}); NL = -16 and NL = -8 select the TMA-fed X/Y
+ * line.  NL = 0 selects the warp-resident Z kernel (Z only; K in {4, 5, 8}, or
+ * 12 in float for 256 < dimz <= 384; a line in the smallest P in {4, 8, 16, 32}
+ * lanes with P K >= dimz, so dimz <= 32 K); NL = -16 and NL = -8 select the TMA-fed X/Y
  * kernel with 16 or 8 lines per CTA (dimz a multiple of 16, K in {4, 8, 16},
  * line length = P K with P in {4, 8, 16} or P = 32 at K = 4, or, in float with
  * K = 4 and 8 lines, P = 64 or 96 (lines of 256 or 384 rows), tiles within the

@@ -90,10 +90,10 @@ def test_autotuner_picks_supported_shapes(adi_lib):
     s = solver(adi_lib, d, (200.0, 0.72, 1.4))
     shapes = s.fast_shapes()
     for dr, (K, NL, P) in enumerate(shapes):
-        assert K in (4, 8, 12, 16)
+        assert K in (4, 5, 8, 12, 16)
         assert P * K >= d.shape[dr]
         if NL == 0:
-            assert dr == 2 and P * K == d.shape[2]          # warp-resident Z lines
+            assert dr == 2 and P == -(-d.shape[2] // K)      # warp-resident Z lines
         elif NL < 0:
             assert dr < 2 and NL in (-8, -16, -32) and P * K == d.shape[dr]   # TMA-fed X/Y tiles
         else:
@@ -237,6 +237,28 @@ def test_zwarp_any_dimz(adi_lib, nz, zK, precision):
     assert max(errs) < tol, errs
     errs_n = rel_errors(s.fields(1), orc.fields(1), m)
     assert max(errs_n) < tol, errs_n
+
+
+@pytest.mark.parametrize("nz", [384, 300], ids=["nz384-K12-full", "nz300-K12-ragged"])
+def test_zwarp_twelve_row_chunks(adi_lib, nz):
+    """The warp-resident Z sweep with 12-row chunks (float only): lines of up to 384
+    rows in one warp; FP64 rejects the shape."""
+    from adi_b200 import _abi
+    d = G.random_domain(12, 10, nz, seed=90 + nz, shell=True, n_obstacles=6, rmax=4.0)
+    params = (140.0, 0.72, 1.4)
+    s = solver(adi_lib, d, params, precision=_abi.ADI_FP32)
+    s.set_fast_shape(2, 12, 0)
+    assert s.fast_shapes()[2][:2] == (12, 0)
+    orc = O.OracleSolver(d, precision=8, params=fluid_params_tuple(("normalized", params)))
+    m = non_out(d)
+    for _ in range(3):
+        assert s.step(8e-4, 4, 2, True) == 0
+        assert orc.step(8e-4, 4, 2, True) == 0
+    assert max(rel_errors(s.fields(0), orc.fields(0), m)) < 2e-6
+    assert max(rel_errors(s.fields(1), orc.fields(1), m)) < 2e-6
+    s64 = solver(adi_lib, d, params, precision=_abi.ADI_FP64)
+    with pytest.raises(_abi.AdiError):
+        s64.set_fast_shape(2, 12, 0)
 
 
 def _slab_domain(nx, ny, nz, seed):
