@@ -83,6 +83,10 @@ def _spheres64():
     return G.spheres_channel(n=64, n_spheres=10, rmin=3.0, rmax=7.0, seed=0)
 
 
+def _zlines384():
+    return G.spheres_channel(dims=(96, 96, 384), n_spheres=20, rmin=4.0, rmax=12.0, seed=0)
+
+
 def _batched8():
     return G.batch_of_domains(n_domains=8, seed=2, size_lo=64, size_hi=96, spheres=(10, 30), rmin=4.0, rmax=10.0,
                               re=(50.0, 400.0))
@@ -141,6 +145,9 @@ CONFIGS = {
     "spheres64": dict(make=_spheres64, Re=200.0, Pr=0.72, lam=1.4, dt=5e-4, ng=4, nl=2,
                       desc="small case for profiling: 64^3 FP32, 10 spheres, Re=200, dt=5e-4, "
                            "num_global=4, num_local=2"),
+    "zlines384": dict(make=_zlines384, Re=500.0, Pr=0.72, lam=1.4, dt=2e-4, ng=4, nl=2, acc_steps=2,
+                      desc="small case for profiling the sweeps of 384-row Z lines: 96x96x384 FP32, 20 spheres "
+                           "(radii U[4,12], seed 0), Re=500, dt=2e-4, num_global=4, num_local=2"),
 }
 
 
