@@ -160,6 +160,8 @@ __global__ void __launch_bounds__(NLT * P, xy_ctas_per_sm((int)sizeof(R), K, NLT
     using namespace sweep;
     const int p0 = ch * K;
     const R gm = merges == 2 ? R(0.75) : R(0.5);   // share of the correction c in temp_out
+    // the merged nonlinear value (temp + x) / 2, or with the extra merge (temp + 3 x) / 4
+    const R gw_new = gm, gw_old = R(1) - gm;
     // Tile row (i P + c) of row p0 + i, i in [-1, K]: rows -1 and K belong to the
     // neighbouring chunks; outside the line, this chunk's own row stands in.
     auto trow = [&](int i) -> int {
@@ -303,8 +305,7 @@ __global__ void __launch_bounds__(NLT * P, xy_ctas_per_sm((int)sizeof(R), K, NLT
                 R dd = edge ? R(0) : dv[v][i], m = R(0);
                 if (kd == R_IN) {
                     dd += cT[v * fs + tr * NLT];
-                    m = (temp_at(v, tr) + dd) * R(0.5);
-                    if (merges == 2) m = (m + dd) * R(0.5);
+                    m = fma(dd, gw_new, temp_at(v, tr) * gw_old);
                 }
                 dv[v][i] = dd;
                 gv[v][i] = m;
