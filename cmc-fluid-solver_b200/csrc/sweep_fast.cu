@@ -323,6 +323,8 @@ __device__ __forceinline__ void sweep_fast_block(unsigned char *smem_raw, int bu
     if (!active) return;
 
     // ---------------- 4. interior unknowns, write-back, merge ----------------
+    // merged nonlinear value: (temp + x) / 2, or with the extra merge (temp + 3 x) / 4
+    const R gw_new = merges == 2 ? R(0.75) : R(0.5), gw_old = R(1) - gw_new;
 #pragma unroll
     for (int i = 0; i < K; i++) {
         const int kd = kind[i];
@@ -353,12 +355,8 @@ __device__ __forceinline__ void sweep_fast_block(unsigned char *smem_raw, int bu
                 using namespace sweep;
                 const float2 x03 = add2(p2(cu[0][i + 1], cu[3][i + 1]), p2(x[0], x[3]));
                 const float2 x12 = add2(p2(cu[1][i + 1], cu[2][i + 1]), p2(x[1], x[2]));
-                float2 m03 = mul2(add2(p2(tv[0][i + 1], tv[3][i + 1]), x03), bc2(0.5f));
-                float2 m12 = mul2(add2(p2(tv[1][i + 1], tv[2][i + 1]), x12), bc2(0.5f));
-                if (merges == 2) {
-                    m03 = mul2(add2(m03, x03), bc2(0.5f));
-                    m12 = mul2(add2(m12, x12), bc2(0.5f));
-                }
+                const float2 m03 = fma2(x03, bc2(gw_new), mul2(p2(tv[0][i + 1], tv[3][i + 1]), bc2(gw_old)));
+                const float2 m12 = fma2(x12, bc2(gw_new), mul2(p2(tv[1][i + 1], tv[2][i + 1]), bc2(gw_old)));
                 next.f[0][off] = x03.x; next.f[3][off] = x03.y; next.f[1][off] = x12.x; next.f[2][off] = x12.y;
                 tout.f[0][off] = m03.x; tout.f[3][off] = m03.y; tout.f[1][off] = m12.x; tout.f[2][off] = m12.y;
             } else {
@@ -366,9 +364,7 @@ __device__ __forceinline__ void sweep_fast_block(unsigned char *smem_raw, int bu
                 for (int v = 0; v < 4; v++) {
                     const R xv = cu[v][i + 1] + x[v];
                     next.f[v][off] = xv;
-                    R m = (tv[v][i + 1] + xv) * R(0.5);
-                    if (merges == 2) m = (m + xv) * R(0.5);
-                    tout.f[v][off] = m;
+                    tout.f[v][off] = fma(xv, gw_new, tv[v][i + 1] * gw_old);
                 }
             }
         } else {

@@ -281,6 +281,8 @@ __global__ void __launch_bounds__(128)
     if (!has) return;
 
     // ---- write-back ----
+    // merged nonlinear value: (temp + x) / 2, or with the extra merge (temp + 3 x) / 4
+    const R gw_new = merges == 2 ? R(0.75) : R(0.5), gw_old = R(1) - gw_new;
     R xo[4][K], mo[4][K];
     bool all_seg = true, all_in = true;
 #pragma unroll
@@ -293,9 +295,7 @@ __global__ void __launch_bounds__(128)
             R x = i == 0 ? xf[v] : (i == K - 1 ? xl[v] : dv[v][i] - ea[m][i] * xf[v] - ec[m][i] * xl[v]);
             if (kind[i] == Z_IN) x += cu[v][i];
             xo[v][i] = x;
-            R mm = (tv[v][i] + x) * R(0.5);
-            if (merges == 2) mm = (mm + x) * R(0.5);
-            mo[v][i] = mm;
+            mo[v][i] = fma(x, gw_new, tv[v][i] * gw_old);
         }
     }
     // (padding rows are NONE: the row at L-1 is never IN, so the row at L is not a
